@@ -1,0 +1,39 @@
+// Test infrastructure (oracle): argument block shared by the restatement
+// (oracle.cpp) and the host build of the reference's sources (refshim/).
+#pragma once
+
+extern "C" {
+struct or_args {
+  int H, W;
+  const float* ray_o;
+  const float* ray_d;
+  const float* verts;
+  const int* num_points;
+  const int* cumsum;
+  int P;
+  const float* shs;
+  int sh_degree;
+  int M;
+  const float* opacities;
+  const float* sigma;
+  const float* bg;
+  const float* extra;
+  int extra_len;
+  int variant;         // 0 plain, 1 reflect, 2 refract, 3 envlight
+  int tmin_inclusive;  // 1: optixTrace's closed interval
+  int canonical_ties;  // 1: equal-t hits ordered by primitive id
+  int exact_geometry;  // 1: FP64 hit point (FP64 precision only)
+  int nthreads;
+  int row_begin, row_end;  // rows of the image to trace (row_end <= 0: all)
+  // backward inputs (precision of the call)
+  const void* colors;
+  const void* others;
+  const float* dL_dpixels;
+  const float* dL_dothers;
+  // optional per-ray record
+  int max_rec;
+  int* rec_ids;     // [H*W, max_rec]
+  int* rec_count;   // [H*W]
+  float* margin;    // [H*W]
+};
+}
