@@ -1,0 +1,274 @@
+// C ABI (include/tritracer.h): the handle that replaces the reference's
+// OptixTracer class (tritracer/tracer.h:67-126, tracer.cpp, pipeline.cpp).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/tritracer.h"
+#include "bvh.cuh"
+#include "trace.cuh"
+
+struct tt_tracer {
+  tt_config cfg;
+  int device = 0;
+  int num_sms = 148;
+  int fwd_grid = 0, bwd_grid = 0;
+  std::string err;
+  tt::Bvh bvh;
+  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int fail(tt_tracer* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(tt_tracer* h, cudaError_t e, const char* what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? TT_ERR_OOM : TT_ERR_CUDA;
+  return fail(h, code, std::string("CUDA call (") + what + ") failed with error: '" + cudaGetErrorString(e) + "'");
+}
+
+#define TT_CUDA(h, call)                                   \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+  } while (0)
+
+#define TT_REQUIRE(h, cond, msg)                        \
+  do {                                                  \
+    if (!(cond)) return fail(h, TT_ERR_INVALID, (msg)); \
+  } while (0)
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+int accel_step(tt_tracer* h, const float* verts, int num_vertices, const int* cumsum, int P, int mode,
+               cudaStream_t s) {
+  TT_REQUIRE(h, mode == TT_BUILD || mode == TT_REFIT || mode == TT_KEEP, "rebuild_gas must be 0, 1 or 2");
+  TT_REQUIRE(h, P >= 0, "number_of_points must be >= 0");
+  if (mode == TT_KEEP) {
+    if (!h->bvh.built()) return fail(h, TT_ERR_STATE, "rebuild_gas=2 before any acceleration structure was built");
+    if (h->bvh.P() != P) return fail(h, TT_ERR_STATE, "rebuild_gas=2 with a different triangle count than the build");
+    return TT_OK;
+  }
+  if (P > 0) {
+    TT_REQUIRE(h, verts && cumsum, "vertices and cumsum must be device pointers");
+    TT_REQUIRE(h, num_vertices >= 3, "need at least 3 vertices");
+  }
+  TT_REQUIRE(h, P < (1 << 27), "at most 2^27 triangles");
+  cudaError_t e = (mode == TT_BUILD) ? h->bvh.build(verts, cumsum, P, s) : h->bvh.refit(verts, cumsum, P, s);
+  if (e != cudaSuccess) return cuda_fail(h, e, mode == TT_BUILD ? "bvh build" : "bvh refit");
+  return TT_OK;
+}
+
+int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P) {
+  TT_REQUIRE(h, deg >= 0 && deg <= 3, "sh_degree must be in [0, 3]");
+  TT_REQUIRE(h, M >= (deg + 1) * (deg + 1), "shs has fewer coefficients per triangle than sh_degree needs");
+  TT_REQUIRE(h, P == 0 || shs != nullptr,
+             "shs is empty: the reference path evaluates SH only (colors_precomp is never read)");
+  return TT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tt_create(const tt_config* cfg, tt_tracer** out) {
+  if (!out) return TT_ERR_INVALID;
+  *out = nullptr;
+  tt_tracer* h = new (std::nothrow) tt_tracer();
+  if (!h) return TT_ERR_OOM;
+  tt_config def;
+  std::memset(&def, 0, sizeof(def));
+  def.variant = TT_VARIANT_PLAIN;
+  def.tmin_inclusive = 1;
+  h->cfg = cfg ? *cfg : def;
+  if (h->cfg.variant < TT_VARIANT_PLAIN || h->cfg.variant > TT_VARIANT_ENVLIGHT) {
+    delete h;
+    return TT_ERR_INVALID;
+  }
+  cudaError_t e;
+  if ((e = cudaGetDevice(&h->device)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
+      (e = h->scratch.reserve(64)) != cudaSuccess || (e = cudaMemset(h->scratch.p, 0, 64)) != cudaSuccess ||
+      (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+    delete h;
+    return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
+  }
+  h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(0);
+  h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1);
+  *out = h;
+  return TT_OK;
+}
+
+int tt_destroy(tt_tracer* h) {
+  if (!h) return TT_ERR_INVALID;
+  h->bvh.release();
+  h->scratch.release();
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  delete h;
+  return TT_OK;
+}
+
+const char* tt_last_error(const tt_tracer* h) { return h ? h->err.c_str() : "null tracer handle"; }
+
+int tt_build(tt_tracer* h, const float* vertices, int num_vertices, const int* cumsum, int P, int mode,
+             void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  return accel_step(h, vertices, num_vertices, cumsum, P, mode, as_stream(stream));
+}
+
+static tt::TraceParams base_params(tt_tracer* h, int H, int W, const float* ro, const float* rd) {
+  tt::TraceParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.bvh = h->bvh.view();
+  p.H = H;
+  p.W = W;
+  p.ntx = (W + 7) / 8;
+  p.ntiles = p.ntx * ((H + 3) / 4);
+  p.ray_o = ro;
+  p.ray_d = rd;
+  p.tmin_inclusive = h->cfg.tmin_inclusive;
+  p.variant = h->cfg.variant;
+  p.work = h->scratch.as<int>();
+  p.status = h->scratch.as<int>() + 1;
+  return p;
+}
+
+int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+  const cudaStream_t s = as_stream(stream);
+  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
+  TT_REQUIRE(h, (long long)a->H * a->W < (1ll << 31), "too many rays");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->out_color && a->out_others, "null ray or output pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->scaling && a->density_factor && a->max_blending &&
+                              a->num_points),
+             "null per-triangle pointer");
+  TT_REQUIRE(h, a->bg, "null background");
+  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  if (rc != TT_OK) return rc;
+  if (h->cfg.variant != TT_VARIANT_PLAIN) {
+    TT_REQUIRE(h, a->extra && a->extra_len >= (h->cfg.variant == TT_VARIANT_ENVLIGHT ? 5 : 4),
+               "variant needs extra = [r, cx, cy, cz(, samples)]");
+    return fail(h, TT_ERR_INVALID, "secondary-ray variants are not available in this build");
+  }
+  rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
+  if (rc != TT_OK) return rc;
+  tt::TraceParams p = base_params(h, a->H, a->W, a->ray_o, a->ray_d);
+  p.verts = a->vertices;
+  p.cumsum = a->cumsum;
+  p.num_points = a->num_points;
+  p.shs = a->shs;
+  p.sh_degree = a->sh_degree;
+  p.M = a->M;
+  p.opac = a->opacities;
+  p.sigma = a->sigma;
+  p.bg = a->bg;
+  p.scaling = a->scaling;
+  p.density = a->density_factor;
+  p.max_blending = a->max_blending;
+  p.out_color = a->out_color;
+  p.out_others = a->out_others;
+  if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
+  TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+  if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  TT_CUDA(h, tt::launch_forward(p, h->fwd_grid, s));
+  if (a->debug) {
+    TT_CUDA(h, cudaEventRecord(h->ev1, s));
+    TT_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (a->gpu_time_ms) *a->gpu_time_ms = ms;
+  }
+  return TT_OK;
+}
+
+int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+  const cudaStream_t s = as_stream(stream);
+  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->colors && a->others && a->dL_dpixels && a->dL_dothers,
+             "null ray, forward-output or upstream-gradient pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->cumsum && a->vertices), "null per-triangle pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->dL_dtriangle && a->dL_dsigma && a->dL_dopacity && a->dL_dsh),
+             "null gradient output");
+  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  if (rc != TT_OK) return rc;
+  if (!h->bvh.built()) return fail(h, TT_ERR_STATE, "backward before any forward/build");
+  if (h->bvh.P() != a->P) return fail(h, TT_ERR_STATE, "backward with a different triangle count than the forward");
+  if (a->P > 0) {
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dtriangle, 0, (size_t)a->num_vertices * 3 * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dsigma, 0, (size_t)a->P * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dopacity, 0, (size_t)a->P * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dsh, 0, (size_t)a->P * a->M * 3 * sizeof(float), s));
+  }
+  tt::TraceParams p = base_params(h, a->H, a->W, a->ray_o, a->ray_d);
+  p.verts = a->vertices;
+  p.cumsum = a->cumsum;
+  p.num_points = a->num_points;
+  p.shs = a->shs;
+  p.sh_degree = a->sh_degree;
+  p.M = a->M;
+  p.opac = a->opacities;
+  p.sigma = a->sigma;
+  p.bg = a->bg;
+  p.colors = a->colors;
+  p.others = a->others;
+  p.dL_dpix = a->dL_dpixels;
+  p.dL_doth = a->dL_dothers;
+  p.d_tri = a->dL_dtriangle;
+  p.d_sigma = a->dL_dsigma;
+  p.d_opac = a->dL_dopacity;
+  p.d_sh = a->dL_dsh;
+  TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+  if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  TT_CUDA(h, tt::launch_backward(p, h->bwd_grid, s));
+  if (a->debug) {
+    TT_CUDA(h, cudaEventRecord(h->ev1, s));
+    TT_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (a->gpu_time_ms) *a->gpu_time_ms = ms;
+  }
+  return TT_OK;
+}
+
+int tt_device_status(tt_tracer* h, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  const cudaStream_t s = as_stream(stream);
+  int st = 0;
+  TT_CUDA(h, cudaMemcpyAsync(&st, h->scratch.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(h, cudaStreamSynchronize(s));
+  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<int>() + 1, 0, sizeof(int), s));
+  if (st & tt::kStatusStack) return fail(h, TT_ERR_STACK, "traversal stack overflow made no progress on some ray");
+  if (st & tt::kStatusTimeout) return fail(h, TT_ERR_TIMEOUT, "a bounded device loop gave up");
+  return TT_OK;
+}
+
+int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
+                  float* ts, int* counts, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, R >= 0 && max_hits >= 0, "R and max_hits must be >= 0");
+  TT_REQUIRE(h, R == 0 || (ray_o && ray_d && counts && (max_hits == 0 || (ids && ts))), "null pointer");
+  if (!h->bvh.built()) return fail(h, TT_ERR_STATE, "hit stream before any build");
+  tt::HitStreamParams p;
+  p.bvh = h->bvh.view();
+  p.R = R;
+  p.ray_o = ray_o;
+  p.ray_d = ray_d;
+  p.max_hits = max_hits;
+  p.ids = ids;
+  p.ts = ts;
+  p.counts = counts;
+  p.status = h->scratch.as<int>() + 1;
+  TT_CUDA(h, tt::launch_hit_stream(p, as_stream(stream)));
+  return TT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,605 @@
+// LBVH builder: replaces the OptiX GAS build/update of the reference
+// (tritracer/pipeline.cpp:206-265, driven from tracer.cpp:53-69).
+//
+//   prep       triangle records (primitive order) + centroid bounds
+//   morton     30-bit Morton codes of the centroids
+//   sort       4-pass LSD radix sort (8-bit digits), stable, hand-written
+//   records    triangle records in Morton order (traversal reads these)
+//   karras     binary radix tree over (code, position) keys (Karras, HPG 2012)
+//   bottom-up  node boxes, second arrival at each node merges its children
+//   collapse   one launch per level: greedily open the largest child until a
+//              node has 8 children; subtrees of <= kLeafMax triangles become
+//              leaves (a contiguous run of Morton-ordered records)
+//   boxes      each wide node's 8 child boxes from the binary boxes
+// A refit re-runs prep/records/bottom-up/boxes over the same topology.
+#include <cstdio>
+
+#include "bvh.cuh"
+
+namespace tt {
+
+cudaError_t DevBuf::reserve(size_t n) {
+  if (n <= bytes && p) return cudaSuccess;
+  release();
+  cudaError_t e = cudaMalloc(&p, n ? n : 16);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return e;
+  }
+  bytes = n;
+  return cudaSuccess;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kBlock * kSortItems;
+
+struct alignas(16) BinNode {
+  float4 lo, hi;
+  int left, right, first, last;
+};
+
+__device__ __forceinline__ int f2o(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : (i ^ 0x7FFFFFFF);
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : (i ^ 0x7FFFFFFF)); }
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_bounds_init(int* b) {
+  if (threadIdx.x < 3) b[threadIdx.x] = 0x7FFFFFFF;
+  else if (threadIdx.x < 6) b[threadIdx.x] = (int)0x80000000;
+}
+
+// Triangle records in primitive order (and, when `cen` is set, centroids and
+// their bounds for the Morton quantisation).
+__global__ void k_prep(const float* __restrict__ verts, const int* __restrict__ cumsum, int P,
+                       float4* __restrict__ tri_prim, float4* __restrict__ cen, int* __restrict__ bounds) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  float c[3] = {0.f, 0.f, 0.f};
+  const bool ok = p < P;
+  if (ok) {
+    const float* v = verts + 3 * (size_t)cumsum[p];
+    float x[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) x[k] = v[k];
+    tri_prim[3 * (size_t)p + 0] = make_float4(x[0], x[1], x[2], __int_as_float(p));
+    tri_prim[3 * (size_t)p + 1] = make_float4(x[3], x[4], x[5], 0.f);
+    tri_prim[3 * (size_t)p + 2] = make_float4(x[6], x[7], x[8], 0.f);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float lo = fminf(x[a], fminf(x[3 + a], x[6 + a]));
+      const float hi = fmaxf(x[a], fmaxf(x[3 + a], x[6 + a]));
+      c[a] = 0.5f * (lo + hi);
+    }
+    if (cen) cen[p] = make_float4(c[0], c[1], c[2], 0.f);
+  }
+  if (!cen) return;
+  // block reduction of the centroid bounds, then one atomic per block
+  __shared__ int s_lo[3][kBlock / 32], s_hi[3][kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int lo = ok ? f2o(c[a]) : 0x7FFFFFFF;
+    int hi = ok ? f2o(c[a]) : (int)0x80000000;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+    }
+    if (lane == 0) {
+      s_lo[a][warp] = lo;
+      s_hi[a][warp] = hi;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int a = threadIdx.x;
+    int lo = s_lo[a][0], hi = s_hi[a][0];
+    for (int w = 1; w < kBlock / 32; ++w) {
+      lo = min(lo, s_lo[a][w]);
+      hi = max(hi, s_hi[a][w]);
+    }
+    atomicMin(&bounds[a], lo);
+    atomicMax(&bounds[3 + a], hi);
+  }
+}
+
+__global__ void k_morton(const float4* __restrict__ cen, const int* __restrict__ bounds, int P,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const float4 c = cen[p];
+  const float cc[3] = {c.x, c.y, c.z};
+  uint32_t q[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = o2f(bounds[a]), hi = o2f(bounds[3 + a]);
+    const float ext = hi - lo;
+    float u = ext > 0.f ? (cc[a] - lo) / ext : 0.5f;
+    u = fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f);
+    q[a] = (uint32_t)u;
+  }
+  keys[p] = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+  vals[p] = (uint32_t)p;
+}
+
+// ------------------------------------------------------------- radix sort
+__global__ void k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift, uint32_t* __restrict__ hist,
+                            int tiles) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int i = 0; i < kSortItems; ++i) {
+    const int idx = base + i * kBlock + threadIdx.x;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of n counters in one block (digit-major histogram).
+__global__ void k_scan_excl(uint32_t* __restrict__ a, int n) {
+  constexpr int T = 1024, K = 8;
+  __shared__ uint32_t warp_sum[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < n; base += T * K) {
+    uint32_t v[K];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int idx = base + threadIdx.x * K + k;
+      v[k] = idx < n ? a[idx] : 0u;
+      s += v[k];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = warp_sum[lane];
+      uint32_t wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      warp_sum[lane] = wi - w;  // exclusive prefix of warp totals
+    }
+    __syncthreads();
+    uint32_t run = carry + warp_sum[warp] + (incl - s);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int idx = base + threadIdx.x * K + k;
+      if (idx < n) a[idx] = run;
+      run += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == T - 1) carry = run;
+    __syncthreads();
+  }
+}
+
+// Stable scatter of one tile: keys are visited in index order (16 rounds of
+// 256), ranked within each warp with __match_any_sync and across warps with a
+// per-digit prefix in shared memory.
+__global__ void k_sort_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                               uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int n, int shift,
+                               const uint32_t* __restrict__ offsets, int tiles) {
+  __shared__ uint32_t run[256];
+  __shared__ uint32_t wcnt[kBlock / 32][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  run[threadIdx.x] = offsets[threadIdx.x * tiles + blockIdx.x];
+  const unsigned lt = (1u << lane) - 1u;
+  const int base = blockIdx.x * kSortTile;
+  for (int it = 0; it < kSortItems; ++it) {
+    const int idx = base + it * kBlock + threadIdx.x;
+    const bool valid = idx < n;
+    const uint32_t k = valid ? kin[idx] : 0u;
+    const uint32_t v = valid ? vin[idx] : 0u;
+    const uint32_t digit = valid ? ((k >> shift) & 255u) : 256u;
+    for (int j = lane; j < 256; j += 32) wcnt[warp][j] = 0u;
+    __syncwarp();
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, digit);
+    const uint32_t rank = __popc(peers & lt);
+    if (valid && rank == 0) wcnt[warp][digit] = __popc(peers);
+    __syncthreads();
+    {
+      const int d = threadIdx.x;
+      uint32_t acc = run[d];
+#pragma unroll
+      for (int w = 0; w < kBlock / 32; ++w) {
+        const uint32_t c = wcnt[w][d];
+        wcnt[w][d] = acc;
+        acc += c;
+      }
+      run[d] = acc;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t pos = wcnt[warp][digit] + rank;
+      kout[pos] = k;
+      vout[pos] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_records(const uint32_t* __restrict__ order, const float4* __restrict__ tri_prim, int P,
+                          float4* __restrict__ tri_sorted) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const uint32_t p = order[i];
+  tri_sorted[3 * (size_t)i + 0] = tri_prim[3 * (size_t)p + 0];  // w = primitive index
+  tri_sorted[3 * (size_t)i + 1] = tri_prim[3 * (size_t)p + 1];
+  tri_sorted[3 * (size_t)i + 2] = tri_prim[3 * (size_t)p + 2];
+}
+
+// ------------------------------------------------------------- hierarchy
+__device__ __forceinline__ int delta(const uint32_t* __restrict__ keys, int P, int i, int j) {
+  if (j < 0 || j >= P) return -1;
+  const unsigned long long a = ((unsigned long long)keys[i] << 32) | (uint32_t)i;
+  const unsigned long long b = ((unsigned long long)keys[j] << 32) | (uint32_t)j;
+  return __clzll(a ^ b);
+}
+
+__global__ void k_karras(const uint32_t* __restrict__ keys, int P, BinNode* __restrict__ bn, int* __restrict__ bparent,
+                         int* __restrict__ lparent) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P - 1) return;
+  const int d = (delta(keys, P, i, i + 1) - delta(keys, P, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = delta(keys, P, i, i - d);
+  int lmax = 2;
+  while (delta(keys, P, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (delta(keys, P, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = delta(keys, P, i, j);
+  int s = 0, t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (delta(keys, P, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  const int gamma = i + s * d + min(d, 0);
+  const int first = min(i, j), last = max(i, j);
+  const int left = (first == gamma) ? ~gamma : gamma;
+  const int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+  bn[i].left = left;
+  bn[i].right = right;
+  bn[i].first = first;
+  bn[i].last = last;
+  if (left >= 0) bparent[left] = i; else lparent[~left] = i;
+  if (right >= 0) bparent[right] = i; else lparent[~right] = i;
+  if (i == 0) bparent[0] = -1;
+}
+
+__device__ __forceinline__ void tri_box(const float4* __restrict__ tri, int pos, float4& lo, float4& hi) {
+  const float4 a = tri[3 * (size_t)pos], b = tri[3 * (size_t)pos + 1], c = tri[3 * (size_t)pos + 2];
+  lo = make_float4(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)), 0.f);
+  hi = make_float4(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), 0.f);
+}
+
+__device__ __forceinline__ void child_box(const BinNode* bn, const float4* tri, int ref, float4& lo, float4& hi) {
+  if (ref >= 0) {
+    lo = __ldcg(&bn[ref].lo);
+    hi = __ldcg(&bn[ref].hi);
+  } else {
+    tri_box(tri, ~ref, lo, hi);
+  }
+}
+
+__global__ void k_bottom_up(const float4* __restrict__ tri, int P, BinNode* bn, const int* __restrict__ bparent,
+                            const int* __restrict__ lparent, int* flags) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P || P < 2) return;
+  int node = lparent[p];
+  while (node >= 0) {
+    __threadfence();
+    if (atomicAdd(&flags[node], 1) == 0) return;
+    __threadfence();
+    float4 l0, h0, l1, h1;
+    const int left = __ldcg(&bn[node].left), right = __ldcg(&bn[node].right);
+    child_box(bn, tri, left, l0, h0);
+    child_box(bn, tri, right, l1, h1);
+    const float4 lo = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+    const float4 hi = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+    __stcg(&bn[node].lo, lo);
+    __stcg(&bn[node].hi, hi);
+    node = bparent[node];
+  }
+}
+
+// ------------------------------------------------------------- collapse
+__global__ void k_collapse_init(int P, int* levels, int* wbin, int* counters) {
+  const int i = threadIdx.x;
+  if (i < kMaxWideLevels + 1) levels[i] = (i == 0) ? 1 : 0;
+  if (i == 0) {
+    wbin[0] = (P >= 2) ? 0 : ~0;  // root: binary node 0, or the single leaf
+    counters[0] = 0;
+    counters[1] = 0;
+  }
+}
+
+__device__ __forceinline__ float half_area(const BinNode* bn, int r) {
+  const float4 lo = bn[r].lo, hi = bn[r].hi;
+  const float x = hi.x - lo.x, y = hi.y - lo.y, z = hi.z - lo.z;
+  return x * y + y * z + z * x;
+}
+
+__global__ void k_collapse_level(int level, const BinNode* __restrict__ bn, int* levels, int* wbin,
+                                 int* __restrict__ wsrc, float4* __restrict__ wnodes, int* counters) {
+  int base = 0;
+  for (int l = 0; l < level; ++l) base += levels[l];
+  const int cnt = levels[level];
+  const int next_base = base + cnt;
+  if (level == kMaxWideLevels - 1 && cnt > 0 && blockIdx.x == 0 && threadIdx.x == 0) counters[1] = 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+    const int w = base + k;
+    const int b = wbin[w];
+    int slot[kWide];
+    int n;
+    if (b < 0) {
+      slot[0] = b;
+      n = 1;
+    } else {
+      slot[0] = bn[b].left;
+      slot[1] = bn[b].right;
+      n = 2;
+    }
+    while (n < kWide) {
+      int best = -1;
+      float best_a = -1.f;
+      for (int i = 0; i < n; ++i) {
+        const int r = slot[i];
+        if (r >= 0) {
+          const float a = half_area(bn, r);
+          if (a > best_a) {
+            best_a = a;
+            best = i;
+          }
+        }
+      }
+      if (best < 0) break;
+      const int r = slot[best];
+      slot[best] = bn[r].left;
+      slot[n++] = bn[r].right;
+    }
+    uint32_t refs[kWide];
+#pragma unroll
+    for (int i = 0; i < kWide; ++i) {
+      uint32_t ref = kEmptyRef;
+      int src = (int)0x80000000;
+      if (i < n) {
+        const int r = slot[i];
+        src = r;
+        if (r < 0) {
+          ref = leaf_ref((uint32_t)~r, 1u);
+        } else {
+          const int first = bn[r].first, size = bn[r].last - first + 1;
+          if (size <= kLeafMax) {
+            ref = leaf_ref((uint32_t)first, (uint32_t)size);
+          } else {
+            const int idx = next_base + atomicAdd(&levels[level + 1], 1);
+            wbin[idx] = r;
+            ref = (uint32_t)idx;
+          }
+        }
+      }
+      refs[i] = ref;
+      wsrc[(size_t)w * kWide + i] = src;
+    }
+    float4* nd = wnodes + (size_t)w * kNodeF4;
+    nd[12] = make_float4(__uint_as_float(refs[0]), __uint_as_float(refs[1]), __uint_as_float(refs[2]),
+                         __uint_as_float(refs[3]));
+    nd[13] = make_float4(__uint_as_float(refs[4]), __uint_as_float(refs[5]), __uint_as_float(refs[6]),
+                         __uint_as_float(refs[7]));
+  }
+}
+
+__global__ void k_collapse_total(const int* levels, int* counters) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int s = 0;
+    for (int l = 0; l < kMaxWideLevels; ++l) s += levels[l];
+    counters[0] = s;
+  }
+}
+
+// Child boxes of every wide node (SoA across the 8 slots).
+__global__ void k_wide_boxes(const int* __restrict__ wsrc, const BinNode* __restrict__ bn,
+                             const float4* __restrict__ tri, const int* __restrict__ counters, int cap,
+                             float4* __restrict__ wnodes) {
+  const int total = counters[0];
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < total && w < cap; w += gridDim.x * blockDim.x) {
+    float lo[3][kWide], hi[3][kWide];
+#pragma unroll
+    for (int i = 0; i < kWide; ++i) {
+      const int r = wsrc[(size_t)w * kWide + i];
+      float4 l, h;
+      if (r == (int)0x80000000) {
+        l = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        h = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+      } else if (r >= 0) {
+        l = bn[r].lo;
+        h = bn[r].hi;
+      } else {
+        tri_box(tri, ~r, l, h);
+      }
+      lo[0][i] = l.x; lo[1][i] = l.y; lo[2][i] = l.z;
+      hi[0][i] = h.x; hi[1][i] = h.y; hi[2][i] = h.z;
+    }
+    float4* nd = wnodes + (size_t)w * kNodeF4;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      nd[4 * a + 0] = make_float4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+      nd[4 * a + 1] = make_float4(lo[a][4], lo[a][5], lo[a][6], lo[a][7]);
+      nd[4 * a + 2] = make_float4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+      nd[4 * a + 3] = make_float4(hi[a][4], hi[a][5], hi[a][6], hi[a][7]);
+    }
+  }
+}
+
+inline int blocks_for(long long n) { return (int)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+cudaError_t Bvh::reserve(int P) {
+  if (P <= cap_) return cudaSuccess;
+  const size_t n = (size_t)P;
+  const size_t tiles = (n + kSortTile - 1) / kSortTile;
+  const size_t wcap = n > 1 ? n - 1 : 1;
+  cudaError_t e;
+#define TT_RES(buf, bytes)            \
+  if ((e = buf.reserve(bytes)) != cudaSuccess) return e;
+  TT_RES(tri_prim_, n * 3 * sizeof(float4));
+  TT_RES(tri_sorted_, n * 3 * sizeof(float4));
+  TT_RES(centroid_, n * sizeof(float4));
+  TT_RES(bounds_, 8 * sizeof(int));
+  TT_RES(keys_, n * 4);
+  TT_RES(vals_, n * 4);
+  TT_RES(keys2_, n * 4);
+  TT_RES(vals2_, n * 4);
+  TT_RES(hist_, 256 * tiles * 4);
+  TT_RES(bnode_, (n > 1 ? n - 1 : 1) * sizeof(BinNode));
+  TT_RES(bparent_, (n > 1 ? n - 1 : 1) * 4);
+  TT_RES(lparent_, n * 4);
+  TT_RES(flags_, (n > 1 ? n - 1 : 1) * 4);
+  TT_RES(wnodes_, wcap * kNodeF4 * sizeof(float4));
+  TT_RES(wsrc_, wcap * kWide * 4);
+  TT_RES(wbin_, wcap * 4);
+  TT_RES(levels_, (kMaxWideLevels + 1) * 4);
+  TT_RES(counters_, 4 * 4);
+#undef TT_RES
+  cap_ = P;
+  return cudaSuccess;
+}
+
+cudaError_t Bvh::prep(const float* verts, const int* cumsum, int P, bool with_centroids, cudaStream_t s) {
+  if (with_centroids) k_bounds_init<<<1, 32, 0, s>>>(bounds_.as<int>());
+  k_prep<<<blocks_for(P), kBlock, 0, s>>>(verts, cumsum, P, tri_prim_.as<float4>(),
+                                          with_centroids ? centroid_.as<float4>() : nullptr, bounds_.as<int>());
+  return cudaGetLastError();
+}
+
+cudaError_t Bvh::boxes(cudaStream_t s) {
+  const int P = P_;
+  cudaError_t e;
+  if (P >= 2) {
+    if ((e = cudaMemsetAsync(flags_.p, 0, (size_t)(P - 1) * 4, s)) != cudaSuccess) return e;
+    k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(tri_sorted_.as<float4>(), P, bnode_.as<BinNode>(),
+                                                 bparent_.as<int>(), lparent_.as<int>(), flags_.as<int>());
+  }
+  const int wcap = P > 1 ? P - 1 : 1;
+  const int grid = blocks_for(wcap) < 148 * 8 ? blocks_for(wcap) : 148 * 8;
+  k_wide_boxes<<<grid, kBlock, 0, s>>>(wsrc_.as<int>(), bnode_.as<BinNode>(), tri_sorted_.as<float4>(),
+                                       counters_.as<int>(), wcap, wnodes_.as<float4>());
+  return cudaGetLastError();
+}
+
+cudaError_t Bvh::build(const float* verts, const int* cumsum, int P, cudaStream_t s) {
+  built_ = false;
+  P_ = P;
+  if (P <= 0) {
+    built_ = true;
+    return cudaSuccess;
+  }
+  cudaError_t e = reserve(P);
+  if (e != cudaSuccess) return e;
+  if ((e = prep(verts, cumsum, P, true, s)) != cudaSuccess) return e;
+  k_morton<<<blocks_for(P), kBlock, 0, s>>>(centroid_.as<float4>(), bounds_.as<int>(), P, keys_.as<uint32_t>(),
+                                            vals_.as<uint32_t>());
+  // 30-bit keys: four 8-bit passes, ending back in keys_/vals_
+  const int tiles = (P + kSortTile - 1) / kSortTile;
+  uint32_t *ka = keys_.as<uint32_t>(), *va = vals_.as<uint32_t>();
+  uint32_t *kb = keys2_.as<uint32_t>(), *vb = vals2_.as<uint32_t>();
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 8 * pass;
+    k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, P, shift, hist_.as<uint32_t>(), tiles);
+    k_scan_excl<<<1, 1024, 0, s>>>(hist_.as<uint32_t>(), 256 * tiles);
+    k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, P, shift, hist_.as<uint32_t>(), tiles);
+    uint32_t* t;
+    t = ka; ka = kb; kb = t;
+    t = va; va = vb; vb = t;
+  }
+  // after an even number of passes the sorted data is back in keys_/vals_
+  k_records<<<blocks_for(P), kBlock, 0, s>>>(vals_.as<uint32_t>(), tri_prim_.as<float4>(), P,
+                                             tri_sorted_.as<float4>());
+  if (P >= 2)
+    k_karras<<<blocks_for(P - 1), kBlock, 0, s>>>(keys_.as<uint32_t>(), P, bnode_.as<BinNode>(), bparent_.as<int>(),
+                                                  lparent_.as<int>());
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // binary boxes are needed by the collapse's area heuristic
+  if (P >= 2) {
+    if ((e = cudaMemsetAsync(flags_.p, 0, (size_t)(P - 1) * 4, s)) != cudaSuccess) return e;
+    k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(tri_sorted_.as<float4>(), P, bnode_.as<BinNode>(),
+                                                 bparent_.as<int>(), lparent_.as<int>(), flags_.as<int>());
+  }
+  k_collapse_init<<<1, 128, 0, s>>>(P, levels_.as<int>(), wbin_.as<int>(), counters_.as<int>());
+  const int wcap = P > 1 ? P - 1 : 1;
+  const int cgrid = blocks_for(wcap) < 148 * 4 ? blocks_for(wcap) : 148 * 4;
+  for (int level = 0; level < kMaxWideLevels; ++level)
+    k_collapse_level<<<cgrid, kBlock, 0, s>>>(level, bnode_.as<BinNode>(), levels_.as<int>(), wbin_.as<int>(),
+                                              wsrc_.as<int>(), wnodes_.as<float4>(), counters_.as<int>());
+  k_collapse_total<<<1, 32, 0, s>>>(levels_.as<int>(), counters_.as<int>());
+  const int grid = blocks_for(wcap) < 148 * 8 ? blocks_for(wcap) : 148 * 8;
+  k_wide_boxes<<<grid, kBlock, 0, s>>>(wsrc_.as<int>(), bnode_.as<BinNode>(), tri_sorted_.as<float4>(),
+                                       counters_.as<int>(), wcap, wnodes_.as<float4>());
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  built_ = true;
+  return cudaSuccess;
+}
+
+cudaError_t Bvh::refit(const float* verts, const int* cumsum, int P, cudaStream_t s) {
+  if (!built_ || P != P_) return build(verts, cumsum, P, s);
+  if (P <= 0) return cudaSuccess;
+  cudaError_t e;
+  if ((e = prep(verts, cumsum, P, false, s)) != cudaSuccess) return e;
+  k_records<<<blocks_for(P), kBlock, 0, s>>>(vals_.as<uint32_t>(), tri_prim_.as<float4>(), P,
+                                             tri_sorted_.as<float4>());
+  return boxes(s);
+}
+
+void Bvh::release() {
+  DevBuf* all[] = {&tri_prim_, &tri_sorted_, &centroid_, &bounds_, &keys_,  &vals_,  &keys2_, &vals2_, &hist_,
+                   &bnode_,    &bparent_,   &lparent_,  &flags_,  &wnodes_, &wsrc_, &wbin_,  &levels_, &counters_};
+  for (DevBuf* b : all) b->release();
+  cap_ = 0;
+  built_ = false;
+}
+
+BvhView Bvh::view() const {
+  BvhView v;
+  v.nodes = wnodes_.as<float4>();
+  v.tris = tri_sorted_.as<float4>();
+  v.tri_prim = tri_prim_.as<float4>();
+  v.P = P_;
+  v.has_root = (built_ && P_ > 0) ? 1 : 0;
+  return v;
+}
+
+}  // namespace tt

@@ -1,0 +1,59 @@
+// Host-side interface of the LBVH builder (bvh.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "tt_device.cuh"
+
+namespace tt {
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t n);
+  void release();
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Replaces OptiX's GAS build/update (tritracer/pipeline.cpp:206-265): a
+// Morton-ordered linear BVH (Karras 2012) collapsed to 8-wide nodes. All
+// steps are kernels on the caller's stream; nothing synchronises.
+class Bvh {
+ public:
+  // Full build from vertices (float[num_vertices][3]) through cumsum[P].
+  cudaError_t build(const float* verts, const int* cumsum, int P, cudaStream_t s);
+  // Same topology, boxes and triangle records recomputed from moved vertices.
+  cudaError_t refit(const float* verts, const int* cumsum, int P, cudaStream_t s);
+  void release();
+
+  BvhView view() const;
+  bool built() const { return built_; }
+  int P() const { return P_; }
+  // device scalars: [0] number of wide nodes, [1] error flag of the collapse
+  const int* counters() const { return counters_.as<int>(); }
+
+ private:
+  cudaError_t reserve(int P);
+  cudaError_t prep(const float* verts, const int* cumsum, int P, bool sorted_only, cudaStream_t s);
+  cudaError_t boxes(cudaStream_t s);
+
+  int P_ = 0;
+  int cap_ = 0;
+  bool built_ = false;
+  DevBuf tri_prim_, tri_sorted_;       // 3 float4 per triangle
+  DevBuf centroid_, bounds_;           // float4 per prim; 6 ints (ordered-float bounds)
+  DevBuf keys_, vals_, keys2_, vals2_; // radix sort ping-pong
+  DevBuf hist_;                        // 256 x tiles
+  DevBuf bnode_;                       // binary internal nodes (BinNode)
+  DevBuf bparent_, lparent_, flags_;   // parents of internal nodes / leaves, arrival flags
+  DevBuf wnodes_, wsrc_, wbin_;        // wide nodes, per-slot binary source, per-node binary source
+  DevBuf levels_;                      // per-level wide node counts
+  DevBuf counters_;
+};
+
+}  // namespace tt

@@ -1,0 +1,226 @@
+"""Host-side mirror of the reference's pybind11 module ``_C`` (ext.cpp:11-27):
+``OptixTracer`` with ``build_tri_accel``, ``trace_forward`` and
+``trace_backward``, returning objects with a ``.data`` tuple, over the C ABI of
+libtritracer.so. Tensors are handed over as raw device pointers on the
+current torch stream; no OptiX is involved.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import lib, check
+
+# the PTX names the reference loads select a raygen program here
+_VARIANTS = {
+    "forward.ptx": _lib.TT_VARIANT_PLAIN,
+    "reflect.ptx": _lib.TT_VARIANT_REFLECT,
+    "refract.ptx": _lib.TT_VARIANT_REFRACT,
+    "envlight.ptx": _lib.TT_VARIANT_ENVLIGHT,
+}
+
+
+class FwdTraceResult:
+    """tracer.h:59-61: data = (color, others, gpu_time, scaling, density_factor, max_blending)."""
+
+    def __init__(self, data):
+        self.data = data
+
+
+class BwdTraceResult:
+    """tracer.h:63-65: data = (dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh)."""
+
+    def __init__(self, data):
+        self.data = data
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+def _f32(t, name, device):
+    if not isinstance(t, torch.Tensor):
+        raise RuntimeError(f"{name} must be a tensor")
+    if t.dtype != torch.float32:
+        raise RuntimeError(f"{name} must be float32, got {t.dtype}")
+    if t.device != device:
+        raise RuntimeError(f"{name} must be on {device}, got {t.device}")
+    return t.contiguous()
+
+
+def _i32(t, name, device):
+    if not isinstance(t, torch.Tensor):
+        raise RuntimeError(f"{name} must be a tensor")
+    if t.dtype != torch.int32:
+        raise RuntimeError(f"{name} must be int32, got {t.dtype}")
+    if t.device != device:
+        raise RuntimeError(f"{name} must be on {device}, got {t.device}")
+    return t.contiguous()
+
+
+class OptixTracer:
+    """Drop-in for the reference's ``_C.OptixTracer(pkgDir[, forward, backward])``
+    (tracer.h:67-126). ``pkgDir`` is accepted for signature compatibility and
+    unused; the two names select the program (forward.ptx, reflect.ptx,
+    refract.ptx, envlight.ptx / backward.ptx)."""
+
+    def __init__(self, pkg_dir: str = "", forward: str = "forward.ptx", backward: str = "backward.ptx",
+                 tmin_inclusive: bool = True):
+        if forward not in _VARIANTS:
+            raise RuntimeError(f"unknown forward program {forward!r}; expected one of {sorted(_VARIANTS)}")
+        if backward != "backward.ptx":
+            raise RuntimeError(f"unknown backward program {backward!r}; expected 'backward.ptx'")
+        if not torch.cuda.is_available():
+            raise RuntimeError("OptixTracer needs a CUDA device")
+        self.variant = _VARIANTS[forward]
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        cfg = _lib.TtConfig()
+        cfg.variant = self.variant
+        cfg.tmin_inclusive = 1 if tmin_inclusive else 0
+        h = ctypes.c_void_p(0)
+        rc = lib.tt_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != _lib.TT_OK:
+            raise _lib.TracerError(rc, f"OptixTracer construction failed (tt_create returned {rc})")
+        self._h = h
+        self._keep = ()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.tt_destroy(h)
+            self._h = None
+
+    # ------------------------------------------------------------------
+    def build_tri_accel(self, triangles_points, cumsum_of_points_per_triangle, number_of_points, rebuild=True):
+        """pipeline.cpp:206-265 (BUILD when `rebuild`, UPDATE otherwise)."""
+        dev = self.device
+        verts = _f32(triangles_points, "triangles_points", dev)
+        cumsum = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        mode = 0 if rebuild else 1
+        check(self._h, lib.tt_build(self._h, _ptr(verts), verts.numel() // 3, _ptr(cumsum), int(number_of_points),
+                                    mode, _stream()))
+
+    def trace_forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
+                      cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, colors_precomp, opacities,
+                      scaling, density_factor, bg_color, extra, rebuild_gas_opt, debug):
+        """tracer.cpp:16-142: returns FwdTraceResult((color [3,H,W], others [7,H,W],
+        gpu_time [1], scaling, density_factor, max_blending [P]))."""
+        dev = self.device
+        P = int(number_of_points)
+        ro = _f32(ray_o, "ray_o", dev)
+        rd = _f32(ray_d, "ray_d", dev)
+        if ro.dim() < 2 or ro.shape != rd.shape or ro.shape[-1] != 3:
+            raise RuntimeError("ray_o / ray_d must both be [H, W, 3]")
+        H, W = int(ro.shape[0]), int(ro.shape[1])
+        verts = _f32(triangles_points, "triangles_points", dev)
+        sig = _f32(sigma, "sigma", dev)
+        npts = _i32(num_points_per_triangle, "num_points_per_triangle", dev)
+        cums = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        sh = _f32(shs, "shs", dev)
+        M = int(sh.shape[1]) if sh.dim() >= 2 and sh.shape[0] != 0 else 0
+        opac = _f32(opacities, "opacities", dev)
+        bg = _f32(bg_color, "bg_color", dev)
+        ex = extra.to(device=dev, dtype=torch.float32).contiguous() if isinstance(extra, torch.Tensor) else None
+        if ex is not None and ex.numel() == 0:
+            ex = None
+        # scaling / density_factor are updated in place and returned
+        sc = _f32(scaling, "scaling", dev)
+        de = _f32(density_factor, "density_factor", dev)
+        out_color = torch.empty((3, H, W), dtype=torch.float32, device=dev)
+        out_others = torch.empty((7, H, W), dtype=torch.float32, device=dev)
+        max_blending = torch.empty((P,), dtype=torch.float32, device=dev)
+        ms = ctypes.c_float(0.0)
+        a = _lib.TtFwdArgs()
+        a.H, a.W = H, W
+        a.ray_o, a.ray_d = _ptr(ro), _ptr(rd)
+        a.vertices, a.num_vertices = _ptr(verts), verts.numel() // 3
+        a.num_points, a.cumsum, a.P = _ptr(npts), _ptr(cums), P
+        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
+        a.colors_precomp = ctypes.c_void_p(0)
+        a.opacities, a.sigma = _ptr(opac), _ptr(sig)
+        a.scaling, a.density_factor = _ptr(sc), _ptr(de)
+        a.bg = _ptr(bg)
+        a.extra, a.extra_len = (_ptr(ex), ex.numel()) if ex is not None else (ctypes.c_void_p(0), 0)
+        a.rebuild_gas, a.debug = int(rebuild_gas_opt), 1 if debug else 0
+        a.out_color, a.out_others, a.max_blending = _ptr(out_color), _ptr(out_others), _ptr(max_blending)
+        a.gpu_time_ms = ctypes.pointer(ms)
+        check(self._h, lib.tt_forward(self._h, ctypes.byref(a), _stream()))
+        if sc.data_ptr() != scaling.data_ptr():
+            scaling.copy_(sc.view_as(scaling))
+        if de.data_ptr() != density_factor.data_ptr():
+            density_factor.copy_(de.view_as(density_factor))
+        gpu_time = torch.zeros((1,), dtype=torch.float32, device=dev)
+        if debug:
+            gpu_time.fill_(ms.value)
+        # the arrays the kernels read must outlive the asynchronous launch
+        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de)
+        return FwdTraceResult((out_color, out_others, gpu_time, scaling, density_factor, max_blending))
+
+    def trace_backward(self, ray_o, ray_d, background, triangles_points, sigma, num_points_per_triangle,
+                       cumsum_of_points_per_triangle, colors, others, number_of_points, shs, sh_degree, opacities,
+                       dL_dpixels, dL_dothers, scaling, debug):
+        """tracer.cpp:144-228: returns BwdTraceResult((dL_dtriangle [V,3],
+        dL_dsigma like sigma, dL_dopacity like opacities, dL_dsh [P,M,3]))."""
+        dev = self.device
+        P = int(number_of_points)
+        ro = _f32(ray_o, "ray_o", dev)
+        rd = _f32(ray_d, "ray_d", dev)
+        H, W = int(ro.shape[0]), int(ro.shape[1])
+        verts = _f32(triangles_points, "triangles_points", dev)
+        sig = _f32(sigma, "sigma", dev)
+        npts = _i32(num_points_per_triangle, "num_points_per_triangle", dev)
+        cums = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        col = _f32(colors, "colors", dev)
+        oth = _f32(others, "others", dev)
+        sh = _f32(shs, "shs", dev)
+        M = int(sh.shape[1]) if sh.dim() >= 2 and sh.shape[0] != 0 else 0
+        opac = _f32(opacities, "opacities", dev)
+        g = _f32(dL_dpixels, "dL_dpixels", dev)
+        go = _f32(dL_dothers, "dL_dothers", dev)
+        bg = _f32(background, "background", dev)
+        V = verts.numel() // 3
+        dL_dtriangle = torch.empty((V, 3), dtype=torch.float32, device=dev)
+        dL_dsigma = torch.empty_like(sigma, memory_format=torch.contiguous_format)
+        dL_dopacity = torch.empty_like(opacities, memory_format=torch.contiguous_format)
+        dL_dsh = torch.empty((P, M, 3), dtype=torch.float32, device=dev)
+        a = _lib.TtBwdArgs()
+        a.H, a.W = H, W
+        a.ray_o, a.ray_d, a.bg = _ptr(ro), _ptr(rd), _ptr(bg)
+        a.vertices, a.num_vertices = _ptr(verts), V
+        a.sigma, a.num_points, a.cumsum = _ptr(sig), _ptr(npts), _ptr(cums)
+        a.colors, a.others, a.P = _ptr(col), _ptr(oth), P
+        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
+        a.opacities, a.dL_dpixels, a.dL_dothers = _ptr(opac), _ptr(g), _ptr(go)
+        a.scaling = ctypes.c_void_p(0)
+        a.debug = 1 if debug else 0
+        a.dL_dtriangle, a.dL_dsigma = _ptr(dL_dtriangle), _ptr(dL_dsigma)
+        a.dL_dopacity, a.dL_dsh = _ptr(dL_dopacity), _ptr(dL_dsh)
+        a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        check(self._h, lib.tt_backward(self._h, ctypes.byref(a), _stream()))
+        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg)
+        return BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
+
+    # ------------------------------------------------------------------
+    def device_status(self):
+        """Synchronises and raises if a bounded device loop gave up since the
+        last check (no reference counterpart)."""
+        check(self._h, lib.tt_device_status(self._h, _stream()))
+
+    def hit_stream(self, ray_o, ray_d, max_hits=64):
+        """Test hook: first `max_hits` hits per ray ordered by (t, primitive)."""
+        ro = _f32(ray_o, "ray_o", self.device).reshape(-1, 3)
+        rd = _f32(ray_d, "ray_d", self.device).reshape(-1, 3)
+        R = ro.shape[0]
+        ids = torch.full((R, max_hits), -1, dtype=torch.int32, device=self.device)
+        ts = torch.full((R, max_hits), float("inf"), dtype=torch.float32, device=self.device)
+        counts = torch.zeros((R,), dtype=torch.int32, device=self.device)
+        check(self._h, lib.tt_hit_stream(self._h, _ptr(ro), _ptr(rd), R, max_hits, _ptr(ids), _ptr(ts),
+                                         _ptr(counts), _stream()))
+        return ids, ts, counts

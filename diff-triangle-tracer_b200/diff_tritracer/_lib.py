@@ -1,0 +1,109 @@
+"""ctypes binding of libtritracer.so, the C ABI declared in include/tritracer.h.
+
+The library is built in-tree (``make -C diff-triangle-tracer_b200``). There is
+no fallback: importing this module without the built library raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtritracer.so")
+
+TT_OK = 0
+TT_ERR_INVALID = 1
+TT_ERR_OOM = 2
+TT_ERR_TIMEOUT = 3
+TT_ERR_STACK = 4
+TT_ERR_CUDA = 5
+TT_ERR_STATE = 6
+
+TT_VARIANT_PLAIN = 0
+TT_VARIANT_REFLECT = 1
+TT_VARIANT_REFRACT = 2
+TT_VARIANT_ENVLIGHT = 3
+
+_f = ctypes.POINTER(ctypes.c_float)
+_i = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+
+class TtConfig(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int), ("tmin_inclusive", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+class TtFwdArgs(ctypes.Structure):
+    _fields_ = [
+        ("H", ctypes.c_int), ("W", ctypes.c_int),
+        ("ray_o", _vp), ("ray_d", _vp),
+        ("vertices", _vp), ("num_vertices", ctypes.c_int),
+        ("num_points", _vp), ("cumsum", _vp), ("P", ctypes.c_int),
+        ("shs", _vp), ("sh_degree", ctypes.c_int), ("M", ctypes.c_int),
+        ("colors_precomp", _vp), ("opacities", _vp), ("sigma", _vp),
+        ("scaling", _vp), ("density_factor", _vp),
+        ("bg", _vp), ("extra", _vp), ("extra_len", ctypes.c_int),
+        ("rebuild_gas", ctypes.c_int), ("debug", ctypes.c_int),
+        ("out_color", _vp), ("out_others", _vp), ("max_blending", _vp),
+        ("gpu_time_ms", _f),
+    ]
+
+
+class TtBwdArgs(ctypes.Structure):
+    _fields_ = [
+        ("H", ctypes.c_int), ("W", ctypes.c_int),
+        ("ray_o", _vp), ("ray_d", _vp), ("bg", _vp),
+        ("vertices", _vp), ("num_vertices", ctypes.c_int),
+        ("sigma", _vp), ("num_points", _vp), ("cumsum", _vp),
+        ("colors", _vp), ("others", _vp), ("P", ctypes.c_int),
+        ("shs", _vp), ("sh_degree", ctypes.c_int), ("M", ctypes.c_int),
+        ("opacities", _vp), ("dL_dpixels", _vp), ("dL_dothers", _vp), ("scaling", _vp),
+        ("debug", ctypes.c_int),
+        ("dL_dtriangle", _vp), ("dL_dsigma", _vp), ("dL_dopacity", _vp), ("dL_dsh", _vp),
+        ("gpu_time_ms", _f),
+    ]
+
+
+EXPORTS = (
+    "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
+    "tt_device_status", "tt_hit_stream",
+)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"diff_tritracer: {LIB_PATH} is missing; build it with `make -C {os.path.dirname(_HERE)}` "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.tt_create.argtypes = [ctypes.POINTER(TtConfig), ctypes.POINTER(_vp)]
+    lib.tt_destroy.argtypes = [_vp]
+    lib.tt_build.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, _vp]
+    lib.tt_forward.argtypes = [_vp, ctypes.POINTER(TtFwdArgs), _vp]
+    lib.tt_backward.argtypes = [_vp, ctypes.POINTER(TtBwdArgs), _vp]
+    lib.tt_last_error.argtypes = [_vp]
+    lib.tt_last_error.restype = ctypes.c_char_p
+    lib.tt_device_status.argtypes = [_vp, _vp]
+    lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+    for name in EXPORTS:
+        getattr(lib, name).restype = getattr(lib, name).restype if name == "tt_last_error" else ctypes.c_int
+    return lib
+
+
+lib = _load()
+
+
+class TracerError(RuntimeError):
+    """Raised for a failed C-ABI call (RuntimeError, like the reference's
+    exceptions through pybind11)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def check(handle, rc: int):
+    if rc != TT_OK:
+        msg = lib.tt_last_error(handle).decode(errors="replace") if handle else f"tritracer error {rc}"
+        raise TracerError(rc, msg)

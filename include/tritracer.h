@@ -1,0 +1,166 @@
+/*
+ * tritracer.h - C ABI of the B200 differentiable k-closest-hit triangle tracer.
+ *
+ * Drop-in for the reference's host tracer class `OptixTracer`
+ * (tritracer/tracer.h:67-126, bound to Python in ext.cpp:11-27). Every entry
+ * point takes plain device pointers and sizes, never framework types, and
+ * returns a status code (TT_OK = 0). Work is enqueued on the caller's CUDA
+ * stream (`stream`, a cudaStream_t; NULL = legacy default stream) and nothing
+ * synchronises unless stated.
+ *
+ * Data layout (the reference's per-triangle layout, tritracer/params.h:15-62):
+ *   vertices   float[num_vertices][3]; triangle i uses vertices cumsum[i],
+ *              cumsum[i]+1, cumsum[i]+2
+ *   num_points int[P] (3 for every triangle), cumsum int[P] (exclusive prefix sum)
+ *   shs        float[P][M][3], coefficient-major, RGB innermost
+ *   opacities, sigma, scaling, density_factor, max_blending   float[P]
+ *   rays       ray_o, ray_d float[H][W][3]
+ *   out_color  float[3][H][W];  out_others float[7][H][W] with channels
+ *              0 depth, 1 alpha = 1-T, 2..4 normal, 5 middepth, 6 distortion
+ *              (tritracer/config.h:16-20)
+ */
+#ifndef TRITRACER_H
+#define TRITRACER_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference reports failures as C++ exceptions
+ * (tritracer/exception.h:16-51); here each call returns one of these and
+ * tt_last_error() holds the message. */
+#define TT_OK 0
+#define TT_ERR_INVALID 1 /* bad argument (shape, pointer, degree, size) */
+#define TT_ERR_OOM 2     /* device allocation failed */
+#define TT_ERR_TIMEOUT 3 /* a bounded device loop gave up (see tt_device_status) */
+#define TT_ERR_STACK 4   /* traversal stack could not make progress */
+#define TT_ERR_CUDA 5    /* CUDA runtime error */
+#define TT_ERR_STATE 6   /* call order (e.g. trace before any BVH build) */
+
+/* Which raygen program the forward pass runs: the reference selects one by
+ * the PTX file handed to OptixTracer (tritracer/pipeline.cpp:289-296). */
+#define TT_VARIANT_PLAIN 0    /* forward.cu */
+#define TT_VARIANT_REFLECT 1  /* reflect.cu: mirror sphere from extra[0..3] */
+#define TT_VARIANT_REFRACT 2  /* refract.cu: glass sphere from extra[0..3] */
+#define TT_VARIANT_ENVLIGHT 3 /* envlight.cu: extra[4] cosine samples off the sphere */
+
+/* Acceleration-structure step taken by a forward call (`rebuild_gas` of
+ * TracerSettings, diff_tritracer/__init__.py:42; tracer.cpp:56-69). */
+#define TT_BUILD 0 /* full rebuild from the vertices */
+#define TT_REFIT 1 /* keep the topology, refit boxes to moved vertices */
+#define TT_KEEP 2  /* use the structure as is */
+
+typedef struct tt_tracer tt_tracer;
+
+typedef struct tt_config {
+  int variant;        /* TT_VARIANT_* (default PLAIN) */
+  int tmin_inclusive; /* 1 (default): each re-trace starts AT the last hit's t,
+                         the closed interval of optixTrace; 0: strictly after */
+  int reserved[6];    /* zero */
+} tt_config;
+
+/* Arguments of the forward trace: OptixTracer::trace_fwd
+ * (tritracer/tracer.h:78-95, tracer.cpp:16-142). All pointers are device
+ * pointers except gpu_time_ms. */
+typedef struct tt_fwd_args {
+  int H, W;
+  const float* ray_o;
+  const float* ray_d;
+  const float* vertices;
+  int num_vertices;
+  const int* num_points;
+  const int* cumsum;
+  int P; /* number_of_points: the triangle count (tracer.cpp:43) */
+  const float* shs;
+  int sh_degree; /* 0..3 */
+  int M;         /* coefficients per triangle, >= (sh_degree+1)^2 */
+  const float* colors_precomp; /* accepted and ignored, as in the reference */
+  const float* opacities;      /* already activated */
+  const float* sigma;
+  float* scaling;        /* in/out */
+  float* density_factor; /* in/out */
+  const float* bg;       /* [3] */
+  const float* extra;    /* variant parameters [r, cx, cy, cz, samples] */
+  int extra_len;         /* floats in extra */
+  int rebuild_gas;       /* TT_BUILD / TT_REFIT / TT_KEEP */
+  int debug;             /* 1: time the trace with events into *gpu_time_ms (syncs) */
+  float* out_color;      /* [3,H,W], fully written */
+  float* out_others;     /* [7,H,W], fully written */
+  float* max_blending;   /* [P], zeroed then written */
+  float* gpu_time_ms;    /* host pointer, may be NULL */
+} tt_fwd_args;
+
+/* Arguments of the adjoint: OptixTracer::trace_bwd (tritracer/tracer.h:97-114,
+ * tracer.cpp:144-228). Gradient outputs are zeroed, then accumulated. */
+typedef struct tt_bwd_args {
+  int H, W;
+  const float* ray_o;
+  const float* ray_d;
+  const float* bg;
+  const float* vertices;
+  int num_vertices;
+  const float* sigma;
+  const int* num_points;
+  const int* cumsum;
+  const float* colors; /* forward out_color */
+  const float* others; /* forward out_others */
+  int P;
+  const float* shs;
+  int sh_degree;
+  int M;
+  const float* opacities;
+  const float* dL_dpixels; /* [3,H,W] */
+  const float* dL_dothers; /* [7,H,W]; channels 0 and 2..4 are read */
+  const float* scaling;    /* unused by the adjoint, as in the reference */
+  int debug;
+  float* dL_dtriangle; /* [num_vertices,3] */
+  float* dL_dsigma;    /* [P] */
+  float* dL_dopacity;  /* [P] */
+  float* dL_dsh;       /* [P,M,3] */
+  float* gpu_time_ms;  /* host pointer, may be NULL */
+} tt_bwd_args;
+
+/* OptixTracer::OptixTracer (tritracer/pipeline.cpp:267-302). `cfg` may be
+ * NULL for the defaults. Uses the CUDA device current at the call. */
+int tt_create(const tt_config* cfg, tt_tracer** out);
+
+/* OptixTracer::~OptixTracer (tritracer/pipeline.cpp:322-326). */
+int tt_destroy(tt_tracer* h);
+
+/* OptixTracer::build_tri_accel (tritracer/pipeline.cpp:206-265) together with
+ * the index-buffer set-up of tracer.cpp:53-69: mode TT_BUILD builds, TT_REFIT
+ * refits the existing structure to moved vertices, TT_KEEP does nothing. */
+int tt_build(tt_tracer* h, const float* vertices, int num_vertices, const int* cumsum, int P, int mode,
+             void* stream);
+
+/* OptixTracer::trace_fwd (tritracer/tracer.cpp:16-142). Runs the
+ * acceleration-structure step `a->rebuild_gas` first. */
+int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream);
+
+/* OptixTracer::trace_bwd (tritracer/tracer.cpp:144-228). Re-traces with the
+ * structure of the last forward/build call. */
+int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream);
+
+/* Message of the last failed call on this handle (never NULL). */
+const char* tt_last_error(const tt_tracer* h);
+
+/* Synchronises `stream` and returns the device-side status word of the
+ * handle's kernels since the last call (TT_OK, TT_ERR_TIMEOUT or
+ * TT_ERR_STACK), then clears it. No reference counterpart: the reference's
+ * device code has no bounded loops to report on. */
+int tt_device_status(tt_tracer* h, void* stream);
+
+/* Test hook, no reference counterpart: the first `max_hits` triangle hits of
+ * each of R rays in [0, 1000], ordered by (t, primitive index), found by the
+ * same chunked traversal the trace kernels use. ids/ts are [R][max_hits]
+ * device arrays, counts [R] receives each ray's total hit count. */
+int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
+                  float* ts, int* counts, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRITRACER_H */

@@ -1,0 +1,200 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+* Hit streams: the traversal's (t, primitive) sequence per ray must equal the
+  oracle's BIT FOR BIT (same FP32 watertight intersector, every triangle hit in
+  [0, 1000], ordered by (t, id)).
+* Forward: against the FP64 oracle with exact geometry, per pixel
+  |gpu - oracle| <= 1e-5 |oracle| + 1e-6 (north_star: images within 1e-5
+  relative), on every ray whose threshold decisions are not within 1e-5
+  (relative) of flipping.
+* Adjoint: each gradient tensor within 1e-4 relative (L2) of the FP64 oracle
+  (north_star: gradients within 1e-4 relative), with the upstream gradient of
+  excluded rays set to zero so their decisions cannot matter.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # collected on CPU hosts, skipped there
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import diff_tritracer  # noqa: E402
+from diff_tritracer import _C, scenes  # noqa: E402
+from gpu_helpers import (MARGIN, DEV, T, flagged_prims, gpu_backward, gpu_forward, rel_norm,  # noqa: E402
+                         settings)
+from scenes_for_tests import dense_scene, dense_view  # noqa: E402
+
+RTOL, ATOL = 1e-5, 1e-6
+GRAD_RTOL = 1e-4
+
+
+def cases():
+    yield "dense", dense_scene(seed=1, P=3000), dense_view(H=48, W=64)
+    sc = scenes.make_scene(20000, seed=5)
+    cam = scenes.sphere_cameras(1, 56, 72, seed=5)[0]
+    yield "random20k", sc, scenes.camera_rays(cam)
+
+
+CASES = list(cases())
+
+
+@pytest.fixture(scope="module")
+def tracer():
+    return _C.OptixTracer("", "forward.ptx", "backward.ptx")
+
+
+@pytest.mark.parametrize("name,sc,rays", CASES, ids=[c[0] for c in CASES])
+def test_hit_stream_bitwise(oracle, tracer, name, sc, rays):
+    ro, rd = rays
+    tracer.build_tri_accel(T(sc.verts), T(sc.cumsum), sc.P, True)
+    ids_g, ts_g, cnt_g = [x.cpu().numpy() for x in tracer.hit_stream(T(ro), T(rd), max_hits=64)]
+    tracer.device_status()
+    ids_o, ts_o, cnt_o = oracle.hit_stream(sc, ro, rd, max_hits=64, nthreads=8)
+    assert cnt_o.sum() > 0
+    np.testing.assert_array_equal(cnt_g, cnt_o)
+    n = np.minimum(cnt_o, 64)
+    mask = np.arange(64)[None, :] < n[:, None]
+    np.testing.assert_array_equal(ids_g[mask].astype(np.uint32), ids_o[mask])
+    np.testing.assert_array_equal(ts_g[mask].view(np.uint32), ts_o[mask].view(np.uint32))
+
+
+@pytest.mark.parametrize("incl", [True, False], ids=["closed", "open"])
+@pytest.mark.parametrize("name,sc,rays", CASES, ids=[c[0] for c in CASES])
+def test_forward_vs_fp64_oracle(oracle, name, sc, rays, incl):
+    ro, rd = rays
+    H, W = ro.shape[:2]
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", tmin_inclusive=incl)
+    bg = np.array([0.1, 0.2, 0.3], np.float32)
+    st = settings(bg=bg)
+    out = gpu_forward(tr, sc, ro, rd, st)
+    tr.device_status()
+    ref = oracle.forward(sc, ro, rd, bg=bg, precision=64, exact=True, canonical=True, tmin_inclusive=incl,
+                         record=256, nthreads=8)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    assert ok.mean() > 0.97, ok.mean()
+    for key in ("color", "others"):
+        a, b = out[key][:, ok], getattr(ref, key)[:, ok]
+        err = np.abs(a - b)
+        worst = float((err / (RTOL * np.abs(b) + ATOL)).max())
+        print(f"{name} {key}: max abs {err.max():.2e}, worst/tol {worst:.3f}")
+        assert np.all(err <= RTOL * np.abs(b) + ATOL), (key, worst)
+    skip = np.zeros(sc.P, bool)
+    skip[flagged_prims(ref, H, W, ok)] = True
+    np.testing.assert_array_equal(out["density"][~skip], ref.density[~skip])
+    np.testing.assert_allclose(out["max_blending"][~skip], ref.max_blending[~skip], rtol=RTOL, atol=ATOL)
+    np.testing.assert_allclose(out["scaling"][~skip], ref.scaling[~skip], rtol=1e-6, atol=1e-9)
+    assert (out["density"] > 0).sum() > 100
+
+
+@pytest.mark.parametrize("incl", [True, False], ids=["closed", "open"])
+@pytest.mark.parametrize("name,sc,rays", CASES, ids=[c[0] for c in CASES])
+def test_backward_vs_fp64_oracle(oracle, name, sc, rays, incl):
+    ro, rd = rays
+    H, W = ro.shape[:2]
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", tmin_inclusive=incl)
+    st = settings()
+    ref = oracle.forward(sc, ro, rd, precision=64, exact=True, canonical=True, tmin_inclusive=incl, record=256,
+                         nthreads=8)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    g, go = scenes.upstream_grads(H, W, seed=11, others_std=1.0)
+    g = g * ok[None]
+    go = go * ok[None]
+    out = gpu_forward(tr, sc, ro, rd, st)
+    grads = gpu_backward(tr, sc, ro, rd, st, out["color"], out["others"], g, go)
+    tr.device_status()
+    rb = oracle.backward(sc, ro, rd, ref.color, ref.others, g, go, precision=64, exact=True, canonical=True,
+                         tmin_inclusive=incl, nthreads=8)
+    for key in ("dtri", "dsigma", "dopac", "dsh"):
+        e = rel_norm(grads[key], getattr(rb, key))
+        print(f"{name} {key}: rel L2 {e:.2e}")
+        assert np.linalg.norm(getattr(rb, key)) > 0
+        assert e < GRAD_RTOL, (key, e)
+
+
+def test_autograd_module(oracle):
+    sc = dense_scene(seed=4, P=2000)
+    ro, rd = dense_view(H=32, W=40)
+    tr = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
+    verts = T(sc.verts.reshape(-1)).requires_grad_(True)  # flat [9P], as the reference's callers pass it
+    sigma = T(sc.sigma).requires_grad_(True)
+    opac = T(sc.opacities).requires_grad_(True)
+    shs = T(sc.shs).requires_grad_(True)
+    color, gpu_time, scaling, density, others, maxb = tr(
+        T(ro), T(rd), verts, sigma, T(sc.num_points), T(sc.cumsum), sc.P, opac, torch.zeros(sc.P, device=DEV),
+        torch.zeros(sc.P, device=DEV), shs, None, settings(debug=True))
+    assert color.shape == (3, 32, 40) and others.shape == (7, 32, 40) and maxb.shape == (sc.P,)
+    assert gpu_time.shape == (1,) and float(gpu_time) > 0
+    g = torch.randn_like(color)
+    (color * g).sum().backward()
+    assert verts.grad.shape == verts.shape and sigma.grad.shape == sigma.shape
+    assert opac.grad.shape == opac.shape and shs.grad.shape == shs.shape
+    ref = oracle.forward(sc, ro, rd, precision=64, exact=True, canonical=True, record=128)
+    np.testing.assert_allclose(color.detach().cpu().numpy(), ref.color, rtol=1e-4, atol=1e-5)
+
+
+def test_refit_follows_moved_vertices(oracle):
+    sc = dense_scene(seed=2, P=2500)
+    ro, rd = dense_view(H=40, W=48)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    gpu_forward(tr, sc, ro, rd, settings(rebuild=0))
+    rng = np.random.default_rng(0)
+    moved = sc.__class__(**{**sc.__dict__})
+    moved.verts = (sc.verts + rng.normal(0, 0.01, sc.verts.shape)).astype(np.float32)
+    out = gpu_forward(tr, moved, ro, rd, settings(rebuild=1))  # refit
+    tr.device_status()
+    ids_g, ts_g, cnt_g = [x.cpu().numpy() for x in tr.hit_stream(T(ro), T(rd), max_hits=32)]
+    ids_o, ts_o, cnt_o = oracle.hit_stream(moved, ro, rd, max_hits=32, nthreads=8)
+    np.testing.assert_array_equal(cnt_g, cnt_o)
+    ref = oracle.forward(moved, ro, rd, precision=64, exact=True, canonical=True, record=128)
+    ok = ref.margin > MARGIN
+    a, b = out["color"].reshape(3, -1)[:, ok], ref.color.reshape(3, -1)[:, ok]
+    assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + ATOL)
+    # keep: same structure again
+    out2 = gpu_forward(tr, moved, ro, rd, settings(rebuild=2))
+    np.testing.assert_array_equal(out2["color"], out["color"])
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 5, 17])
+def test_tiny_scenes(oracle, P):
+    sc = scenes.make_scene(P, seed=P, center_std=0.02, edge_range=(0.3, 0.5))
+    cam = scenes.look_at_camera([0.0, 0.2, 3.0], 24, 24, fov_deg=20.0)
+    ro, rd = scenes.camera_rays(cam)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    out = gpu_forward(tr, sc, ro, rd, settings())
+    tr.device_status()
+    ref = oracle.forward(sc, ro, rd, precision=64, exact=True, canonical=True, record=64)
+    ok = ref.margin > MARGIN
+    a, b = out["color"].reshape(3, -1)[:, ok], ref.color.reshape(3, -1)[:, ok]
+    assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + ATOL)
+
+
+def test_rays_missing_everything(oracle):
+    sc = dense_scene(seed=1, P=500)
+    cam = scenes.look_at_camera([0.0, 0.0, 3.0], 16, 16, fov_deg=10.0, target=(0.0, 0.0, 10.0))
+    ro, rd = scenes.camera_rays(cam)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    bg = np.array([0.25, 0.5, 0.75], np.float32)
+    out = gpu_forward(tr, sc, ro, rd, settings(bg=bg))
+    np.testing.assert_array_equal(out["color"], np.broadcast_to(bg[:, None, None], (3, 16, 16)))
+    assert np.all(out["others"] == 0)
+    assert np.all(out["max_blending"] == 0)
+
+
+def test_invalid_arguments_raise():
+    sc = dense_scene(seed=1, P=100)
+    ro, rd = dense_view(H=8, W=8)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    with pytest.raises(RuntimeError, match="sh_degree"):
+        gpu_forward(tr, sc, ro, rd, settings(sh_degree=4))
+    with pytest.raises(RuntimeError, match="rebuild_gas=2 before"):
+        gpu_forward(_C.OptixTracer(), sc, ro, rd, settings(rebuild=2))
+    with pytest.raises(RuntimeError, match="float32"):
+        tr.trace_forward(T(ro).double(), T(rd), T(sc.verts), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P,
+                         T(sc.shs), 3, torch.empty(0, device=DEV), T(sc.opacities), torch.zeros(sc.P, device=DEV),
+                         torch.zeros(sc.P, device=DEV), torch.zeros(3, device=DEV), torch.zeros(5, device=DEV), 0,
+                         False)
+    with pytest.raises(Exception, match="excatly one"):
+        diff_tritracer.Tracer()(T(ro), T(rd), T(sc.verts), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P,
+                                T(sc.opacities), None, None, None, None, settings())
