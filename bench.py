@@ -1,0 +1,401 @@
+"""Benchmark: forward+backward Mrays/s of the differentiable k-closest-hit
+triangle tracer on one node.
+
+Workload (default): 1M triangles from the seeded synthetic generator, 4 views
+of 800x800 on a radius-3 sphere, stacked into one [3200, 800] ray array, fp32,
+forward + backward with upstream dL/dcolor ~ N(0, 1). One step = BVH refit +
+forward trace + adjoint trace (what one optimiser step of the caller runs).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line (rank 0). Multi-GPU runs are independent replicas (the
+tracer does not shard; each rank traces its own copy of the workload) and
+report the aggregate with the max time over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "diff-triangle-tracer_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "fwd+bwd Mrays/s, proposal vs plain on B200 at RMSE≤1e-3; vs OptiX ref"
+WORKLOADS = {
+    # name: (triangles, views, H, W)
+    "c2_1M_4x800": (1_000_000, 4, 800, 800),
+    "c1_100k_1x400": (100_000, 1, 400, 400),
+    # one view of the 1M scene: the profiling case (inputs still larger than L2)
+    "c2_1M_1x800": (1_000_000, 1, 800, 800),
+}
+
+
+def make_workload(name, seed=0):
+    from diff_tritracer import scenes
+
+    P, views, H, W = WORKLOADS[name]
+    sc = scenes.make_scene(P, seed=seed)
+    cams = scenes.sphere_cameras(views, H, W, seed=seed)
+    rays = [scenes.camera_rays(c) for c in cams]
+    ro = np.ascontiguousarray(np.concatenate([r[0] for r in rays], 0))
+    rd = np.ascontiguousarray(np.concatenate([r[1] for r in rays], 0))
+    g, go = scenes.upstream_grads(ro.shape[0], ro.shape[1], seed=seed)
+    return sc, ro, rd, g, go
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        time.sleep(0.05)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_run(runner, sc, ro, rd, g, go, rows, nthreads):
+    """One forward + backward of the CPU implementation over `rows` of the image."""
+    H, W = ro.shape[:2]
+    f = runner.forward(sc, ro, rd, nthreads=nthreads, rows=rows)
+    runner.backward(sc, ro, rd, f.color, f.others, g, go, nthreads=nthreads, rows=rows)
+
+
+def cpu_baseline(name, sc, ro, rd, g, go, budget_s=12.0):
+    """Times the reference's own per-ray code built for the host (oracle/_ref)
+    if it was built, else the oracle's FP32 port, on all host cores, over a
+    bounded band of rows of the first view."""
+    from oracle import pyoracle
+
+    if pyoracle.reference_available():
+        runner, kind = pyoracle.Reference(), "reference"
+    else:
+        runner, kind = pyoracle.Oracle(), "port"
+    nthreads = os.cpu_count() or 1
+    H, W = ro.shape[:2]
+    view_h = WORKLOADS[name][2]
+    mid = view_h // 2
+    t0 = time.time()
+    runner._scene(sc)  # CPU BVH over the same triangles (not timed)
+    build_s = time.time() - t0
+    rows = (mid, mid + 2)
+    t0 = time.time()
+    cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+    probe = max(time.time() - t0, 1e-3)
+    nrows = int(max(2, min(view_h // 2, 2 * budget_s / probe)))
+    rows = (mid - nrows // 2, mid - nrows // 2 + nrows)
+    t0 = time.time()
+    cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+    dt = time.time() - t0
+    nrays = (rows[1] - rows[0]) * W
+    runner.close()
+    return {"value": nrays / dt / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": kind,
+            "sample": f"rows {rows[0]}..{rows[1] - 1} of view 0 ({nrays} rays, fwd+bwd), {dt:.1f} s; "
+                      f"CPU BVH build {build_s:.1f} s untimed"}, runner, kind, nthreads, rows
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    name = args.workload
+    sc, ro, rd, g, go = make_workload(name)
+    base, runner, kind, nthreads, rows = cpu_baseline(name, sc, ro, rd, g, go, budget_s=args.ref_budget)
+    from oracle import pyoracle
+
+    runner = pyoracle.Reference() if kind == "reference" else pyoracle.Oracle()
+    runner._scene(sc)
+    for _ in range(args.warmup):
+        cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+        times.append(time.time() - t0)
+    nrays = (rows[1] - rows[0]) * ro.shape[1]
+    total = sum(times)
+    value = nrays * args.steps / total / 1e6
+    P, views, H, W = WORKLOADS[name]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "triangles": P, "views": views, "H": H, "W": W,
+                   "sample_rays_per_step": nrays},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": nthreads, "kind": kind,
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def algorithmic_bytes(rays, evals, blends):
+    """Per launch, from the per-ray figures: forward 24 + 40 + 48 h_e + 204 h_b;
+    adjoint 24 + 40 + 28 + 48 h_e + (192 + 2*236) h_b (h_e/h_b = evaluated /
+    blended hits, counted by the forward kernel)."""
+    fwd = rays * (24 + 40) + 48 * evals + 204 * blends
+    bwd = rays * (24 + 40 + 28) + 48 * evals + (192 + 2 * 236) * blends
+    return fwd, bwd
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2_1M_4x800", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ref-budget", type=float, default=3.0, help="seconds of CPU work per reference step")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import diff_tritracer
+    from diff_tritracer import _C
+
+    name = args.workload
+    P, views, H, W = WORKLOADS[name]
+    sc, ro_np, rd_np, g_np, go_np = make_workload(name)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ro, rd, g, go = T(ro_np), T(rd_np), T(g_np), T(go_np)
+    verts, sig, npts, cums = T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum)
+    shs, opac = T(sc.shs), T(sc.opacities)
+    bg = torch.zeros(3, device=dev)
+    extra = torch.zeros(5, device=dev)
+    scaling = torch.zeros(P, device=dev)
+    density = torch.zeros(P, device=dev)
+    empty = torch.empty(0, device=dev)
+    HH, WW = ro.shape[0], ro.shape[1]
+    R = HH * WW
+
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.build_tri_accel(verts, cums, P, True)
+    def step():
+        out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg, extra,
+                               1, False).data
+        tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling, False)
+
+    # kernel-level timing: forward and adjoint each bracketed by events
+    def timed_kernels(n):
+        fwd_ms, bwd_ms = [], []
+        for _ in range(n):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            tr.build_tri_accel(verts, cums, P, False)
+            e[0].record()
+            out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg,
+                                   extra, 2, False).data
+            e[1].record()
+            tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling,
+                              False)
+            e[2].record()
+            torch.cuda.synchronize()
+            fwd_ms.append(e[0].elapsed_time(e[1]))
+            bwd_ms.append(e[1].elapsed_time(e[2]))
+        return float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    tr.device_status()
+
+    # ---------------- timed region: exactly K steps
+    sampler = ClockSampler(local)
+    tr.reset_stats()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        step()
+    t1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    elapsed_ms = t0.elapsed_time(t1)
+    st = tr.stats()
+    tr.device_status()
+    if world > 1:
+        tt = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * R * args.steps / (elapsed_ms / 1e3) / 1e6
+
+    # ---------------- roofline of the dominant kernel (adjoint)
+    fwd_ms, bwd_ms = timed_kernels(3)
+    rays_step = st["rays"] / args.steps
+    evals = st["evaluated_hits"] / args.steps
+    blends = st["blended_hits"] / args.steps
+    fwd_b, bwd_b = algorithmic_bytes(rays_step, evals, blends)
+    peak, peak_kind = peaks()
+    dominant = "adjoint" if bwd_ms >= fwd_ms else "forward"
+    dom_bytes, dom_ms = (bwd_b, bwd_ms) if dominant == "adjoint" else (fwd_b, fwd_ms)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"traffic_{name}.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(dominant)
+        except Exception:
+            traffic = None
+
+    # ---------------- end to end through the public API (host buffers)
+    tracer_mod = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
+    tracer_mod.tracer = tr
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    ro_h, rd_h, g_h = pin(ro_np), pin(rd_np), pin(g_np)
+    color_h = torch.empty((3, HH, WW), dtype=torch.float32).pin_memory()
+    verts_p = verts.clone().requires_grad_(True)
+    sig_p, opac_p, shs_p = sig.clone().requires_grad_(True), opac.clone().requires_grad_(True), \
+        shs.clone().requires_grad_(True)
+    settings = diff_tritracer.TracerSettings(bg=bg, scale_modifier=1.0, sh_degree=3, debug=False, rebuild_gas=1,
+                                             extra_params=extra)
+
+    def e2e_step():
+        ro_d = ro_h.to(dev, non_blocking=True)
+        rd_d = rd_h.to(dev, non_blocking=True)
+        g_d = g_h.to(dev, non_blocking=True)
+        color, _, _, _, _, _ = tracer_mod(ro_d, rd_d, verts_p, sig_p, npts, cums, P, opac_p, scaling, density,
+                                          shs_p, None, settings)
+        color.backward(g_d)
+        color_h.copy_(color.detach(), non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = world * R * args.e2e_steps / (e2e_ms / 1e3) / 1e6
+    h2d = ro_h.numel() * 4 + rd_h.numel() * 4 + g_h.numel() * 4
+    d2h = color_h.numel() * 4
+
+    # ---------------- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(name, sc, ro_np, rd_np, g_np, go_np)[0]
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    launches_per_step = st["kernel_launches"] / args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "triangles": P, "views": views, "H": H, "W": W, "rays_per_step": R,
+                   "step": "BVH refit + forward trace + adjoint trace",
+                   "l2": "inputs larger than L2 (scene + BVH + rays ~0.5 GB per step)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "hits_per_ray": {"evaluated": evals / max(rays_step, 1), "blended": blends / max(rays_step, 1)}},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "path": "diff_tritracer.Tracer autograd forward+backward, pinned host rays/grads in, image out"},
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
+                     "forward_ms": fwd_ms, "adjoint_ms": bwd_ms,
+                     "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -16,8 +16,11 @@ struct tt_tracer {
   int fwd_grid = 0, bwd_grid = 0;
   std::string err;
   tt::Bvh bvh;
-  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word
+  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64[2..4] stats
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  unsigned long long trace_launches = 0;  // trace kernels enqueued
+  unsigned long long launch_base = 0;     // launch count at the last stats reset
+  unsigned long long launches() const { return trace_launches + bvh.launches(); }
 };
 
 namespace {
@@ -136,6 +139,7 @@ static tt::TraceParams base_params(tt_tracer* h, int H, int W, const float* ro, 
   p.variant = h->cfg.variant;
   p.work = h->scratch.as<int>();
   p.status = h->scratch.as<int>() + 1;
+  p.stats = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 16);
   return p;
 }
 
@@ -178,6 +182,7 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
   TT_CUDA(h, tt::launch_forward(p, h->fwd_grid, s));
+  ++h->trace_launches;
   if (a->debug) {
     TT_CUDA(h, cudaEventRecord(h->ev1, s));
     TT_CUDA(h, cudaEventSynchronize(h->ev1));
@@ -229,6 +234,7 @@ int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
   TT_CUDA(h, tt::launch_backward(p, h->bwd_grid, s));
+  ++h->trace_launches;
   if (a->debug) {
     TT_CUDA(h, cudaEventRecord(h->ev1, s));
     TT_CUDA(h, cudaEventSynchronize(h->ev1));
@@ -251,6 +257,27 @@ int tt_device_status(tt_tracer* h, void* stream) {
   return TT_OK;
 }
 
+int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!out) return fail(h, TT_ERR_INVALID, "null stats pointer");
+  const cudaStream_t s = as_stream(stream);
+  unsigned long long v[3] = {0, 0, 0};
+  TT_CUDA(h, cudaMemcpyAsync(v, h->scratch.as<char>() + 16, sizeof(v), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(h, cudaStreamSynchronize(s));
+  out->rays = v[0];
+  out->evaluated_hits = v[1];
+  out->blended_hits = v[2];
+  out->kernel_launches = h->launches() - h->launch_base;
+  return TT_OK;
+}
+
+int tt_reset_stats(tt_tracer* h, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 24, as_stream(stream)));
+  h->launch_base = h->launches();
+  return TT_OK;
+}
+
 int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
                   float* ts, int* counts, void* stream) {
   if (!h) return TT_ERR_INVALID;
@@ -268,6 +295,7 @@ int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, i
   p.counts = counts;
   p.status = h->scratch.as<int>() + 1;
   TT_CUDA(h, tt::launch_hit_stream(p, as_stream(stream)));
+  if (R > 0) ++h->trace_launches;
   return TT_OK;
 }
 

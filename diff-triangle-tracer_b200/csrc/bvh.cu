@@ -500,7 +500,11 @@ cudaError_t Bvh::reserve(int P) {
 }
 
 cudaError_t Bvh::prep(const float* verts, const int* cumsum, int P, bool with_centroids, cudaStream_t s) {
-  if (with_centroids) k_bounds_init<<<1, 32, 0, s>>>(bounds_.as<int>());
+  if (with_centroids) {
+    k_bounds_init<<<1, 32, 0, s>>>(bounds_.as<int>());
+    ++launches_;
+  }
+  ++launches_;
   k_prep<<<blocks_for(P), kBlock, 0, s>>>(verts, cumsum, P, tri_prim_.as<float4>(),
                                           with_centroids ? centroid_.as<float4>() : nullptr, bounds_.as<int>());
   return cudaGetLastError();
@@ -513,7 +517,9 @@ cudaError_t Bvh::boxes(cudaStream_t s) {
     if ((e = cudaMemsetAsync(flags_.p, 0, (size_t)(P - 1) * 4, s)) != cudaSuccess) return e;
     k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(tri_sorted_.as<float4>(), P, bnode_.as<BinNode>(),
                                                  bparent_.as<int>(), lparent_.as<int>(), flags_.as<int>());
+    ++launches_;
   }
+  ++launches_;
   const int wcap = P > 1 ? P - 1 : 1;
   const int grid = blocks_for(wcap) < 148 * 8 ? blocks_for(wcap) : 148 * 8;
   k_wide_boxes<<<grid, kBlock, 0, s>>>(wsrc_.as<int>(), bnode_.as<BinNode>(), tri_sorted_.as<float4>(),
@@ -531,6 +537,8 @@ cudaError_t Bvh::build(const float* verts, const int* cumsum, int P, cudaStream_
   cudaError_t e = reserve(P);
   if (e != cudaSuccess) return e;
   if ((e = prep(verts, cumsum, P, true, s)) != cudaSuccess) return e;
+  // morton + 4 x (hist, scan, scatter) + records + karras + bottom-up + collapse init/levels/total + boxes
+  launches_ += 1 + 12 + 1 + (P >= 2 ? 2 : 0) + 1 + kMaxWideLevels + 1 + 1;
   k_morton<<<blocks_for(P), kBlock, 0, s>>>(centroid_.as<float4>(), bounds_.as<int>(), P, keys_.as<uint32_t>(),
                                             vals_.as<uint32_t>());
   // 30-bit keys: four 8-bit passes, ending back in keys_/vals_
@@ -579,6 +587,7 @@ cudaError_t Bvh::refit(const float* verts, const int* cumsum, int P, cudaStream_
   if (P <= 0) return cudaSuccess;
   cudaError_t e;
   if ((e = prep(verts, cumsum, P, false, s)) != cudaSuccess) return e;
+  ++launches_;
   k_records<<<blocks_for(P), kBlock, 0, s>>>(vals_.as<uint32_t>(), tri_prim_.as<float4>(), P,
                                              tri_sorted_.as<float4>());
   return boxes(s);

@@ -36,12 +36,15 @@ class Bvh {
   int P() const { return P_; }
   // device scalars: [0] number of wide nodes, [1] error flag of the collapse
   const int* counters() const { return counters_.as<int>(); }
+  // kernels enqueued by build/refit so far
+  unsigned long long launches() const { return launches_; }
 
  private:
   cudaError_t reserve(int P);
   cudaError_t prep(const float* verts, const int* cumsum, int P, bool sorted_only, cudaStream_t s);
   cudaError_t boxes(cudaStream_t s);
 
+  unsigned long long launches_ = 0;
   int P_ = 0;
   int cap_ = 0;
   bool built_ = false;

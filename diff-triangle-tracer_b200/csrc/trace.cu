@@ -376,12 +376,25 @@ __device__ __forceinline__ RayW load_ray(const float* ro, const float* rd, int p
 }
 
 // ---------------------------------------------------------------- forward
+__device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends) {
+  rays = __reduce_add_sync(0xFFFFFFFFu, rays);
+  evals = __reduce_add_sync(0xFFFFFFFFu, evals);
+  blends = __reduce_add_sync(0xFFFFFFFFu, blends);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(stats, (unsigned long long)rays);
+    atomicAdd(stats + 1, (unsigned long long)evals);
+    atomicAdd(stats + 2, (unsigned long long)blends);
+  }
+}
+
 __global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
   const Stack st = thread_stack();
   const int HW = p.H * p.W;
+  unsigned n_rays = 0, n_eval = 0, n_blend = 0;
   int px, py;
   while (next_tile(p, px, py)) {
     if (px >= p.W || py >= p.H) continue;
+    ++n_rays;
     const int pix = py * p.W + px;
     const RayW r = load_ray(p.ray_o, p.ray_d, pix);
     const float3 u = unit_dir(r);
@@ -391,10 +404,12 @@ __global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
     march(p.bvh, r, p.tmin_inclusive, st, p.status, [&](uint32_t prim, float) -> bool {
       const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
       const Geom g = window_fp64(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), r, __ldg(p.sigma + prim));
+      ++n_eval;
       const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
       if (alpha < kAlphaMin) return false;
       const float test_T = T * (1.0f - alpha);
       if (test_T < kTMin) return true;
+      ++n_blend;
       p.density[prim] = 1.0f;
       compute_scaling(p, (int)prim, r);
       const float w = alpha * T;
@@ -420,6 +435,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
     p.out_others[kMidDepthCh * HW + pix] = 0.0f;
     p.out_others[kDistortionCh * HW + pix] = 0.0f;
   }
+  add_stats(p.stats, n_rays, n_eval, n_blend);
 }
 
 // ---------------------------------------------------------------- adjoint

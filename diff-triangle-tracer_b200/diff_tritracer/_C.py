@@ -213,6 +213,16 @@ class OptixTracer:
         last check (no reference counterpart)."""
         check(self._h, lib.tt_device_status(self._h, _stream()))
 
+    def stats(self):
+        """Synchronises; returns the handle's counters since reset_stats()."""
+        s = _lib.TtStats()
+        check(self._h, lib.tt_get_stats(self._h, ctypes.byref(s), _stream()))
+        return dict(rays=s.rays, evaluated_hits=s.evaluated_hits, blended_hits=s.blended_hits,
+                    kernel_launches=s.kernel_launches)
+
+    def reset_stats(self):
+        check(self._h, lib.tt_reset_stats(self._h, _stream()))
+
     def hit_stream(self, ray_o, ray_d, max_hits=64):
         """Test hook: first `max_hits` hits per ray ordered by (t, primitive)."""
         ro = _f32(ray_o, "ray_o", self.device).reshape(-1, 3)

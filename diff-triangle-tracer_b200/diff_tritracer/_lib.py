@@ -65,9 +65,14 @@ class TtBwdArgs(ctypes.Structure):
     ]
 
 
+class TtStats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
+                ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong)]
+
+
 EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
-    "tt_device_status", "tt_hit_stream",
+    "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats",
 )
 
 
@@ -85,6 +90,8 @@ def _load():
     lib.tt_last_error.argtypes = [_vp]
     lib.tt_last_error.restype = ctypes.c_char_p
     lib.tt_device_status.argtypes = [_vp, _vp]
+    lib.tt_get_stats.argtypes = [_vp, ctypes.POINTER(TtStats), _vp]
+    lib.tt_reset_stats.argtypes = [_vp, _vp]
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype if name == "tt_last_error" else ctypes.c_int

@@ -152,6 +152,24 @@ const char* tt_last_error(const tt_tracer* h);
  * device code has no bounded loops to report on. */
 int tt_device_status(tt_tracer* h, void* stream);
 
+/* Counters of the handle's trace kernels since the last tt_reset_stats (no
+ * reference counterpart; the reference reports only gpu_time). Evaluated hits
+ * are hits at or beyond the near plane whose window function was computed;
+ * blended hits are those composited. kernel_launches counts every kernel this
+ * handle enqueued (BVH steps included). */
+typedef struct tt_stats {
+  unsigned long long rays;
+  unsigned long long evaluated_hits;
+  unsigned long long blended_hits;
+  unsigned long long kernel_launches;
+} tt_stats;
+
+/* Synchronises `stream`, then fills *out. */
+int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream);
+
+/* Zeroes the counters (asynchronously on `stream`). */
+int tt_reset_stats(tt_tracer* h, void* stream);
+
 /* Test hook, no reference counterpart: the first `max_hits` triangle hits of
  * each of R rays in [0, 1000], ordered by (t, primitive index), found by the
  * same chunked traversal the trace kernels use. ids/ts are [R][max_hits]
