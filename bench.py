@@ -315,12 +315,12 @@ def main():
     dom_bytes, dom_ms = (bwd_b, bwd_ms) if dominant == "adjoint" else (fwd_b, fwd_ms)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", f"traffic_{name}.json")
+    tfile = os.path.join(ROOT, "profiles", f"traffic_{name}.txt")
     if os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(dominant)
-        except Exception:
-            traffic = None
+        for ln in open(tfile):
+            parts = ln.split()
+            if len(parts) == 2 and parts[0] == dominant:
+                traffic = float(parts[1])
 
     # ---------------- end to end through the public API (host buffers)
     tracer_mod = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
