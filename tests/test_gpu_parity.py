@@ -4,11 +4,11 @@
   oracle's BIT FOR BIT (same FP32 watertight intersector, every triangle hit in
   [0, 1000], ordered by (t, id)).
 * Forward: against the FP64 oracle with exact geometry, per pixel
-  |gpu - oracle| <= 1e-5 |oracle| + 1e-6 (north_star: images within 1e-5
-  relative), on every ray whose threshold decisions are not within 1e-5
-  (relative) of flipping.
+  |gpu - oracle| <= 1e-5 |oracle| + 1e-6 (images within 1e-5 relative), on
+  every ray whose threshold decisions are not within 1e-5 (relative) of
+  flipping.
 * Adjoint: each gradient tensor within 1e-4 relative (L2) of the FP64 oracle
-  (north_star: gradients within 1e-4 relative), with the upstream gradient of
+  (gradients within 1e-4 relative), with the upstream gradient of
   excluded rays set to zero so their decisions cannot matter.
 """
 import numpy as np
