@@ -611,4 +611,100 @@ BvhView Bvh::view() const {
   return v;
 }
 
+// ------------------------------------------------------------- carved storage
+namespace {
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+BvhStorage carve(char* base, int P, size_t* total) {
+  const size_t n = (size_t)(P > 0 ? P : 1);
+  const size_t tiles = (n + kSortTile - 1) / kSortTile;
+  const size_t inner = n > 1 ? n - 1 : 1;
+  Carver c{base};
+  BvhStorage st;
+  st.tri_prim = c.take<float4>(3 * n);
+  st.tri_sorted = c.take<float4>(3 * n);
+  st.centroid = c.take<float4>(n);
+  st.bounds = c.take<int>(8);
+  st.keys = c.take<uint32_t>(n);
+  st.vals = c.take<uint32_t>(n);
+  st.keys2 = c.take<uint32_t>(n);
+  st.vals2 = c.take<uint32_t>(n);
+  st.hist = c.take<uint32_t>(256 * tiles);
+  st.bnode = c.take<BinNode>(inner);
+  st.bparent = c.take<int>(inner);
+  st.lparent = c.take<int>(n);
+  st.flags = c.take<int>(inner);
+  st.wnodes = c.take<float4>(inner * kNodeF4);
+  st.wsrc = c.take<int>(inner * kWide);
+  st.wbin = c.take<int>(inner);
+  st.levels = c.take<int>(kMaxWideLevels + 1);
+  st.counters = c.take<int>(4);
+  if (total) *total = (c.off + 255) & ~size_t(255);
+  return st;
+}
+
+}  // namespace
+
+size_t bvh_storage_bytes(int P) {
+  size_t total = 0;
+  carve(nullptr, P, &total);
+  return total;
+}
+
+BvhStorage bvh_storage_carve(void* base, int P) { return carve(static_cast<char*>(base), P, nullptr); }
+
+cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* cumsum, int P, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  BinNode* bn = static_cast<BinNode*>(st.bnode);
+  k_bounds_init<<<1, 32, 0, s>>>(st.bounds);
+  k_prep<<<blocks_for(P), kBlock, 0, s>>>(verts, cumsum, P, st.tri_prim, st.centroid, st.bounds);
+  k_morton<<<blocks_for(P), kBlock, 0, s>>>(st.centroid, st.bounds, P, st.keys, st.vals);
+  const int tiles = (P + kSortTile - 1) / kSortTile;
+  uint32_t *ka = st.keys, *va = st.vals, *kb = st.keys2, *vb = st.vals2;
+  for (int pass = 0; pass < 4; ++pass) {
+    k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, P, 8 * pass, st.hist, tiles);
+    k_scan_excl<<<1, 1024, 0, s>>>(st.hist, 256 * tiles);
+    k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, P, 8 * pass, st.hist, tiles);
+    uint32_t* t;
+    t = ka; ka = kb; kb = t;
+    t = va; va = vb; vb = t;
+  }
+  k_records<<<blocks_for(P), kBlock, 0, s>>>(st.vals, st.tri_prim, P, st.tri_sorted);
+  cudaError_t e;
+  if (P >= 2) {
+    k_karras<<<blocks_for(P - 1), kBlock, 0, s>>>(st.keys, P, bn, st.bparent, st.lparent);
+    if ((e = cudaMemsetAsync(st.flags, 0, (size_t)(P - 1) * 4, s)) != cudaSuccess) return e;
+    k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(st.tri_sorted, P, bn, st.bparent, st.lparent, st.flags);
+  }
+  k_collapse_init<<<1, 128, 0, s>>>(P, st.levels, st.wbin, st.counters);
+  const int wcap = P > 1 ? P - 1 : 1;
+  const int grid = blocks_for(wcap) < 148 * 4 ? blocks_for(wcap) : 148 * 4;
+  for (int level = 0; level < kMaxWideLevels; ++level)
+    k_collapse_level<<<grid, kBlock, 0, s>>>(level, bn, st.levels, st.wbin, st.wsrc, st.wnodes, st.counters);
+  k_collapse_total<<<1, 32, 0, s>>>(st.levels, st.counters);
+  k_wide_boxes<<<grid, kBlock, 0, s>>>(st.wsrc, bn, st.tri_sorted, st.counters, wcap, st.wnodes);
+  return cudaGetLastError();
+}
+
+BvhView bvh_storage_view(const BvhStorage& st, int P) {
+  BvhView v;
+  v.nodes = st.wnodes;
+  v.tris = st.tri_sorted;
+  v.tri_prim = st.tri_prim;
+  v.P = P;
+  v.has_root = P > 0 ? 1 : 0;
+  return v;
+}
+
 }  // namespace tt

@@ -59,4 +59,24 @@ class Bvh {
   DevBuf counters_;
 };
 
+// Device buffers of one BVH carved out of caller-provided memory: the same
+// build kernels as Bvh::build, for callers that may not allocate.
+struct BvhStorage {
+  float4* tri_prim;
+  float4* tri_sorted;
+  float4* centroid;
+  int* bounds;
+  uint32_t *keys, *vals, *keys2, *vals2, *hist;
+  void* bnode;
+  int *bparent, *lparent, *flags;
+  float4* wnodes;
+  int *wsrc, *wbin, *levels, *counters;
+};
+
+// Bytes needed for P triangles (every array 256-byte aligned).
+size_t bvh_storage_bytes(int P);
+BvhStorage bvh_storage_carve(void* base, int P);
+cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* cumsum, int P, cudaStream_t s);
+BvhView bvh_storage_view(const BvhStorage& st, int P);
+
 }  // namespace tt

@@ -38,6 +38,7 @@ extern "C" {
 #define TT_ERR_STACK 4   /* traversal stack could not make progress */
 #define TT_ERR_CUDA 5    /* CUDA runtime error */
 #define TT_ERR_STATE 6   /* call order (e.g. trace before any BVH build) */
+#define TT_ERR_TOO_LARGE 7 /* more triangles than tt_forward_noalloc's fixed capacity */
 
 /* Which raygen program the forward pass runs: the reference selects one by
  * the PTX file handed to OptixTracer (tritracer/pipeline.cpp:289-296). */
@@ -176,6 +177,27 @@ int tt_reset_stats(tt_tracer* h, void* stream);
  * device arrays, counts [R] receives each ray's total hit count. */
 int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
                   float* ts, int* counts, void* stream);
+
+/* Forward trace that allocates nothing. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: an operator plugin that only
+ * receives the input and output buffers of each call from its host framework
+ * (a TensorRT plugin, an XLA custom call), or a frame loop held to a fixed
+ * device-memory budget. It needs no handle: every call builds the BVH over
+ * the given triangles and runs the plain forward trace using one fixed,
+ * file-scope device array (4 MiB on every GPU that loads this library, for
+ * the life of the process) instead of allocated memory. The caller passes the
+ * inputs and outputs as in tt_forward; the results match tt_forward's.
+ *
+ * Limits: at most TT_NOALLOC_MAX_TRIANGLES triangles (else TT_ERR_TOO_LARGE,
+ * nothing enqueued); plain variant only (cfg may be NULL for the defaults);
+ * rebuild_gas is ignored (nothing persists between calls); debug timing is
+ * not available (*gpu_time_ms is set to 0). All calls share the one array:
+ * calls that overlap on the GPU race and must not be issued. The first call
+ * on each device looks the array's address up once (host-side set-up, with
+ * that device current); make it before any stream capture. */
+#define TT_NOALLOC_MAX_TRIANGLES 8192
+int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, void* stream);
 
 #ifdef __cplusplus
 }
