@@ -16,7 +16,7 @@ struct tt_tracer {
   int fwd_grid = 0, bwd_grid = 0;
   std::string err;
   tt::Bvh bvh;
-  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64[2..4] stats
+  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[6] from byte 16
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
@@ -96,7 +96,7 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
   cudaError_t e;
   if ((e = cudaGetDevice(&h->device)) != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
-      (e = h->scratch.reserve(64)) != cudaSuccess || (e = cudaMemset(h->scratch.p, 0, 64)) != cudaSuccess ||
+      (e = h->scratch.reserve(128)) != cudaSuccess || (e = cudaMemset(h->scratch.p, 0, 128)) != cudaSuccess ||
       (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
@@ -261,19 +261,22 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   if (!h) return TT_ERR_INVALID;
   if (!out) return fail(h, TT_ERR_INVALID, "null stats pointer");
   const cudaStream_t s = as_stream(stream);
-  unsigned long long v[3] = {0, 0, 0};
+  unsigned long long v[6] = {0, 0, 0, 0, 0, 0};
   TT_CUDA(h, cudaMemcpyAsync(v, h->scratch.as<char>() + 16, sizeof(v), cudaMemcpyDeviceToHost, s));
   TT_CUDA(h, cudaStreamSynchronize(s));
   out->rays = v[0];
   out->evaluated_hits = v[1];
   out->blended_hits = v[2];
   out->kernel_launches = h->launches() - h->launch_base;
+  out->node_visits = v[3];
+  out->triangle_tests = v[4];
+  out->queries = v[5];
   return TT_OK;
 }
 
 int tt_reset_stats(tt_tracer* h, void* stream) {
   if (!h) return TT_ERR_INVALID;
-  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 24, as_stream(stream)));
+  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 48, as_stream(stream)));
   h->launch_base = h->launches();
   return TT_OK;
 }

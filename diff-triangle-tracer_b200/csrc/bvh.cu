@@ -430,7 +430,12 @@ __global__ void k_collapse_total(const int* levels, int* counters) {
   }
 }
 
-// Child boxes of every wide node (SoA across the 8 slots).
+// (infinite planes of empty slots pass through unchanged)
+__device__ __forceinline__ float pad_lo(float v) { return isinf(v) ? v : v - (fabsf(v) * 4e-6f + 1e-12f); }
+__device__ __forceinline__ float pad_hi(float v) { return isinf(v) ? v : v + (fabsf(v) * 4e-6f + 1e-12f); }
+
+// Child boxes of every wide node (SoA across the 8 slots); empty slots get
+// inverted boxes (lo = +inf, hi = -inf), which no slab test accepts.
 __global__ void k_wide_boxes(const int* __restrict__ wsrc, const BinNode* __restrict__ bn,
                              const float4* __restrict__ tri, const int* __restrict__ counters, int cap,
                              float4* __restrict__ wnodes) {
@@ -450,8 +455,10 @@ __global__ void k_wide_boxes(const int* __restrict__ wsrc, const BinNode* __rest
       } else {
         tri_box(tri, ~r, l, h);
       }
-      lo[0][i] = l.x; lo[1][i] = l.y; lo[2][i] = l.z;
-      hi[0][i] = h.x; hi[1][i] = h.y; hi[2][i] = h.z;
+      // padded outward by a few ulps (relative) plus a tiny absolute margin, so
+      // a slab test rounded in FP32 never culls a hit the triangle test reports
+      lo[0][i] = pad_lo(l.x); lo[1][i] = pad_lo(l.y); lo[2][i] = pad_lo(l.z);
+      hi[0][i] = pad_hi(h.x); hi[1][i] = pad_hi(h.y); hi[2][i] = pad_hi(h.z);
     }
     float4* nd = wnodes + (size_t)w * kNodeF4;
 #pragma unroll

@@ -27,6 +27,7 @@ namespace {
 
 constexpr int kMaxChunks = 1 << 20;   // bound on re-traces per ray
 constexpr int kMaxSteps = 1 << 24;    // bound on stack pops per query
+constexpr int kMinBlocks = 4;         // resident blocks per SM the register budget must allow
 
 struct Stack {
   uint32_t* ref;
@@ -48,17 +49,33 @@ __device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsi
   }
 }
 
+struct Counters {
+  unsigned nodes = 0, tris = 0, queries = 0;
+};
+
 // The kChunk smallest hit keys >= key_min (t <= far) along the ray, in
 // ascending order, EMPTY-padded. If the stack overflowed, subtrees were
 // dropped and t_drop is the smallest entry distance among them: only keys with
 // t < t_drop are then guaranteed.
+//
+// Node visit: the near and far slab planes of each axis are picked per ray by
+// the sign of the direction, so each child costs 6 FMAs and 6 min/max; child
+// boxes are padded outward when written (k_wide_boxes) so the rounded test
+// never culls a reported hit, and empty slots hold inverted boxes that never
+// pass. Hit children are pushed in slot order with the nearest one on top.
 __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min,
-                                      unsigned long long (&kb)[kChunk], Stack st, float& t_drop, int* status) {
+                                      unsigned long long (&kb)[kChunk], Stack st, float& t_drop, int* status,
+                                      Counters& cnt) {
+  ++cnt.queries;
 #pragma unroll
   for (int i = 0; i < kChunk; ++i) kb[i] = kEmptyKey;
   t_drop = INFINITY;
   if (!bvh.has_root) return;
   const float t_lo = key_t(key_min);
+  float tmax = kFar;
+  // word offsets of the near / far planes (lo at +0, hi at +2 within each axis)
+  const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
+  const int fx = nx ^ 2, fy = ny ^ 2, fz = nz ^ 2;
   int sp = 0;
   st.put(sp++, 0u, t_lo);
   int steps = 0;
@@ -69,125 +86,143 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
     }
     --sp;
     const uint32_t ref = st.ref[sp * st.stride];
-    const float tn = st.tn[sp * st.stride];
-    const float tmax = (kb[kChunk - 1] != kEmptyKey) ? key_t(kb[kChunk - 1]) : kFar;
-    if (tn > tmax) continue;
+    if (st.tn[sp * st.stride] > tmax) continue;
     if (ref_is_leaf(ref)) {
-      const uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
-      for (uint32_t j = 0; j < cnt; ++j) {
+      const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
+      cnt.tris += ntri;
+      for (uint32_t j = 0; j < ntri; ++j) {
         const float4* tr = bvh.tris + 3 * (size_t)(first + j);
         const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
         float t;
         if (!isect_tri(r, a, b, c, t)) continue;
-        const float tm = (kb[kChunk - 1] != kEmptyKey) ? key_t(kb[kChunk - 1]) : kFar;
-        if (!(t >= t_lo) || !(t <= tm)) continue;
+        if (!(t >= t_lo) || !(t <= tmax)) continue;
         const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-        if (key >= key_min && key < kb[kChunk - 1]) kb_insert(kb, key);
+        if (key >= key_min && key < kb[kChunk - 1]) {
+          kb_insert(kb, key);
+          if (kb[kChunk - 1] != kEmptyKey) tmax = key_t(kb[kChunk - 1]);
+        }
       }
       continue;
     }
+    ++cnt.nodes;
     const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
-    float lox[8], hix[8], loy[8], hiy[8], loz[8], hiz[8];
-    uint32_t cref[8];
-    {
-      float4 v;
-#define TT_LD8(arr, word)                                                           \
-  v = __ldg(nd + (word));                                                           \
-  arr[0] = v.x; arr[1] = v.y; arr[2] = v.z; arr[3] = v.w;                           \
-  v = __ldg(nd + (word) + 1);                                                       \
-  arr[4] = v.x; arr[5] = v.y; arr[6] = v.z; arr[7] = v.w;
-      TT_LD8(lox, 0) TT_LD8(hix, 2) TT_LD8(loy, 4) TT_LD8(hiy, 6) TT_LD8(loz, 8) TT_LD8(hiz, 10)
-#undef TT_LD8
-      v = __ldg(nd + 12);
-      cref[0] = __float_as_uint(v.x); cref[1] = __float_as_uint(v.y);
-      cref[2] = __float_as_uint(v.z); cref[3] = __float_as_uint(v.w);
-      v = __ldg(nd + 13);
-      cref[4] = __float_as_uint(v.x); cref[5] = __float_as_uint(v.y);
-      cref[6] = __float_as_uint(v.z); cref[7] = __float_as_uint(v.w);
-    }
-    float tnear[8];
+    float tn[8], tf[8];
     bool hit[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const float x0 = fmaf(lox[c], r.ix, -r.oix), x1 = fmaf(hix[c], r.ix, -r.oix);
-      const float y0 = fmaf(loy[c], r.iy, -r.oiy), y1 = fmaf(hiy[c], r.iy, -r.oiy);
-      const float z0 = fmaf(loz[c], r.iz, -r.oiz), z1 = fmaf(hiz[c], r.iz, -r.oiz);
-      const float tn0 = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), t_lo));
-      const float tf0 = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-      // padded by a few ulps so a rounded slab test never culls a reported hit
-      tnear[c] = tn0 * 0.9999990f;
-      hit[c] = (cref[c] != kEmptyRef) && (tnear[c] <= tf0 * 1.0000010f);
+    // one axis at a time: near/far planes of the 8 children, then the slab test
+#define TT_AXIS(NEAR, FAR, INV, OI, FIRST)                                                       \
+    {                                                                                            \
+      const float4 n0 = __ldg(nd + (NEAR)), n1 = __ldg(nd + (NEAR) + 1);                          \
+      const float4 f0 = __ldg(nd + (FAR)), f1 = __ldg(nd + (FAR) + 1);                            \
+      const float N8[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};                        \
+      const float F8[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};                        \
+      _Pragma("unroll") for (int c = 0; c < 8; ++c) {                                            \
+        const float a = fmaf(N8[c], (INV), -(OI)), b = fmaf(F8[c], (INV), -(OI));                  \
+        tn[c] = (FIRST) ? fmaxf(a, t_lo) : fmaxf(tn[c], a);                                       \
+        tf[c] = (FIRST) ? fminf(b, tmax) : fminf(tf[c], b);                                       \
+      }                                                                                          \
     }
-    int nhit = 0;
+    TT_AXIS(nx, fx, r.ix, r.oix, true)
+    TT_AXIS(ny, fy, r.iy, r.oiy, false)
+    TT_AXIS(nz, fz, r.iz, r.oiz, false)
+#undef TT_AXIS
 #pragma unroll
-    for (int c = 0; c < 8; ++c) nhit += hit[c] ? 1 : 0;
-    const int avail = kStackDepth - sp;
-    const int npush = nhit < avail ? nhit : avail;
+    for (int c = 0; c < 8; ++c) hit[c] = tn[c] <= tf[c];
+    int nhit = 0, best = -1;
+    float best_t = INFINITY;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      if (!hit[c]) continue;
-      int rank = 0;
-#pragma unroll
-      for (int c2 = 0; c2 < 8; ++c2) {
-        if (c2 == c) continue;
-        const bool before = hit[c2] && (tnear[c2] < tnear[c] || (tnear[c2] == tnear[c] && c2 < c));
-        rank += before ? 1 : 0;
+      if (hit[c]) {
+        ++nhit;
+        if (tn[c] < best_t) {
+          best_t = tn[c];
+          best = c;
+        }
       }
-      if (rank < npush)
-        st.put(sp + npush - 1 - rank, cref[c], tnear[c]);  // nearest on top
-      else
-        t_drop = fminf(t_drop, tnear[c]);
     }
-    sp += npush;
+    if (nhit == 0) continue;
+    const float4 r0 = __ldg(nd + 12), r1 = __ldg(nd + 13);
+    const uint32_t cref[8] = {__float_as_uint(r0.x), __float_as_uint(r0.y), __float_as_uint(r0.z),
+                              __float_as_uint(r0.w), __float_as_uint(r1.x), __float_as_uint(r1.y),
+                              __float_as_uint(r1.z), __float_as_uint(r1.w)};
+    // nearest child last (top of the stack); on overflow drop the others and
+    // remember the smallest distance dropped
+    const int avail = kStackDepth - sp;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (!hit[c] || c == best) continue;
+      if (sp < kStackDepth - 1) {
+        st.put(sp++, cref[c], tn[c]);
+      } else {
+        t_drop = fminf(t_drop, tn[c]);
+      }
+    }
+    (void)avail;
+    st.put(sp++, cref[best], best_t);
   }
 }
 
 // ---------------------------------------------------------------- shading
+// Per-hit geometry. The ray/plane intersection (t and the hit point relative
+// to vertex A) is solved in FP64; everything after that works in FP32 on
+// triangle-sized, A-relative coordinates, where FP32 keeps ~7 digits of the
+// inradius (an FP32 hit point o + t d at distance ~3 keeps only ~3).
 struct Geom {
   float Cx;
-  float3 n;
-  double phi_final, phi_max;
-  double d[3];
-  d3 hp;
-  double t;
+  float3 n;          // unit face normal
+  float phi_final, phi_max;
+  float d[3];        // signed edge distances of the hit point
+  float3 q;          // hit point - A
+  float3 e1, e2;     // B - A, C - A
+  float t;           // hit distance from the FP64 solve
 };
 
-// Window function of tritracer/common.h:57-114 in FP64, evaluated at the
-// exact ray/plane intersection.
-__device__ __forceinline__ Geom window_fp64(float4 a, float4 b, float4 c, const RayW& r, float sigma) {
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float fdot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 fcross(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float flen(float3 v) { return sqrtf(fdot(v, v)); }
+__device__ __forceinline__ float3 fnormalize(float3 v) { return v * rsqrtf(fdot(v, v)); }
+
+// Window function of tritracer/common.h:57-114: edge normals
+// normalize(edge_cross x (p_i - p_{i+1})), edge 0 oriented by the incenter,
+// phi = max edge distance, phi_final = phi / dist(incenter, edge 0),
+// Cx = max(0, phi_final^sigma) with a negative base giving 0.
+__device__ __forceinline__ Geom window_fn(float4 a, float4 b, float4 c, float3 o, float3 d, float sigma) {
   Geom g;
-  const d3 A = tod(a), B = tod(b), C = tod(c);
-  const d3 o = mkd(r.ox, r.oy, r.oz), d = mkd(r.dx, r.dy, r.dz);
-  const d3 ec = cross(B - A, C - A);
-  g.t = dot(A - o, ec) / dot(d, ec);
-  g.hp = o + g.t * d;
-  const double la = len(B - C), lb = len(A - C), lc = len(A - B);
-  const d3 inc = (la * A + lb * B + lc * C) * (1.0 / (la + lb + lc));
-  const d3 fn = normalize(ec);
-  g.n = make_float3((float)fn.x, (float)fn.y, (float)fn.z);
-  const d3 P3[3] = {A, B, C};
-  double dist = 0.0, phi = -INFINITY;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const d3 p1 = P3[i], p2 = P3[(i + 1) % 3];
-    d3 en = normalize(cross(ec, p1 - p2));
-    double off = -dot(en, p1);
-    if (i == 0) {
-      dist = dot(en, inc) + off;
-      if (dist > 0.0) {
-        en = -en;
-        off = -off;
-        dist = -dist;
-      }
-    }
-    const double ed = dot(en, g.hp) + off;
-    phi = fmax(phi, ed);
-    g.d[i] = ed;
+  const double e1x = (double)b.x - a.x, e1y = (double)b.y - a.y, e1z = (double)b.z - a.z;
+  const double e2x = (double)c.x - a.x, e2y = (double)c.y - a.y, e2z = (double)c.z - a.z;
+  const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+  const double ox = (double)o.x - a.x, oy = (double)o.y - a.y, oz = (double)o.z - a.z;  // o - A
+  const double t = -(ox * nx + oy * ny + oz * nz) / ((double)d.x * nx + (double)d.y * ny + (double)d.z * nz);
+  g.t = (float)t;
+  g.q = make_float3((float)(ox + t * d.x), (float)(oy + t * d.y), (float)(oz + t * d.z));
+  g.e1 = make_float3((float)e1x, (float)e1y, (float)e1z);
+  g.e2 = make_float3((float)e2x, (float)e2y, (float)e2z);
+  const float3 e1 = g.e1, e2 = g.e2;
+  const float la = flen(e1 - e2), lb = flen(e2), lc = flen(e1);
+  const float3 inc = (lb * e1 + lc * e2) * (1.0f / (la + lb + lc));  // A is the origin
+  const float3 ec = fcross(e1, e2);
+  g.n = fnormalize(ec);
+  float3 en0 = fnormalize(fcross(ec, -e1));
+  float dist = fdot(en0, inc);
+  if (dist > 0.0f) {
+    en0 = -en0;
+    dist = -dist;
   }
-  g.phi_max = phi;
-  g.phi_final = phi / dist;
+  const float3 en1 = fnormalize(fcross(ec, e1 - e2));
+  const float3 en2 = fnormalize(fcross(ec, e2));
+  g.d[0] = fdot(en0, g.q);
+  g.d[1] = fdot(en1, g.q - e1);
+  g.d[2] = fdot(en2, g.q - e2);
+  g.phi_max = fmaxf(fmaxf(g.d[0], g.d[1]), g.d[2]);
+  g.phi_final = g.phi_max / dist;
   // __powf of the reference is NaN for a negative base and then clamped to 0
-  g.Cx = (g.phi_final >= 0.0) ? (float)pow(g.phi_final, (double)sigma) : 0.0f;
+  g.Cx = (g.phi_final >= 0.0f) ? powf(g.phi_final, sigma) : 0.0f;
   return g;
 }
 
@@ -200,7 +235,8 @@ constexpr float kSH0 = 0.28209479177387814f;
 constexpr float kSH1 = 0.4886025119029199f;
 
 // Degree-<=3 SH basis (tritracer/common.h:16-55, auxiliary.h:13-30).
-__device__ __forceinline__ void sh_basis(float x, float y, float z, int deg, float (&B)[16]) {
+__device__ __forceinline__ void sh_basis(float3 u, int deg, float (&B)[16]) {
+  const float x = u.x, y = u.y, z = u.z;
   B[0] = kSH0;
   if (deg > 0) {
     B[1] = -kSH1 * y;
@@ -233,84 +269,113 @@ __device__ __forceinline__ float3 sh_raw(const float* __restrict__ shs, int M, i
   const float* base = shs + (size_t)prim * M * 3;
   float r = 0.f, g = 0.f, b = 0.f;
   if (M == 16 && deg == 3) {
-    const float4* q = reinterpret_cast<const float4*>(base);  // 192-byte aligned rows
-    float v[48];
+    const float4* q = reinterpret_cast<const float4*>(base);  // 192-byte rows, 16-byte aligned
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
       const float4 w = __ldg(q + i);
-      v[4 * i] = w.x; v[4 * i + 1] = w.y; v[4 * i + 2] = w.z; v[4 * i + 3] = w.w;
-    }
+      const float v[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      r = fmaf(B[k], v[3 * k], r);
-      g = fmaf(B[k], v[3 * k + 1], g);
-      b = fmaf(B[k], v[3 * k + 2], b);
+      for (int j = 0; j < 4; ++j) {
+        const int idx = 4 * i + j, k = idx / 3, ch = idx % 3;
+        if (ch == 0) r = fmaf(B[k], v[j], r);
+        else if (ch == 1) g = fmaf(B[k], v[j], g);
+        else b = fmaf(B[k], v[j], b);
+      }
     }
   } else {
     const int n = sh_count(deg);
-#pragma unroll 4
-    for (int k = 0; k < n; ++k) {
-      r = fmaf(B[k], __ldg(base + 3 * k), r);
-      g = fmaf(B[k], __ldg(base + 3 * k + 1), g);
-      b = fmaf(B[k], __ldg(base + 3 * k + 2), b);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      if (k < n) {
+        r = fmaf(B[k], __ldg(base + 3 * k), r);
+        g = fmaf(B[k], __ldg(base + 3 * k + 1), g);
+        b = fmaf(B[k], __ldg(base + 3 * k + 2), b);
+      }
     }
   }
   return make_float3(r + 0.5f, g + 0.5f, b + 0.5f);
 }
 
-__device__ __forceinline__ float3 unit_dir(const RayW& r) {
-  const float inv = 1.0f / sqrtf(r.dx * r.dx + r.dy * r.dy + r.dz * r.dz);
-  return make_float3(r.dx * inv, r.dy * inv, r.dz * inv);
+__device__ __forceinline__ float3 unit(float3 d) {
+  const float inv = 1.0f / sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+  return make_float3(d.x * inv, d.y * inv, d.z * inv);
 }
 
 // computeScaling of tritracer/forward.cu:25-74 (first blending ray records the
 // largest angle the vertices subtend around the centroid direction), in FP64.
-__device__ __forceinline__ void compute_scaling(const TraceParams& p, int prim, const RayW& r) {
-  if (p.scaling[prim] > 0.0f) return;
-  const int off = p.cumsum[prim], np = p.num_points[prim];
-  const d3 o = mkd(r.ox, r.oy, r.oz);
+__device__ __noinline__ void compute_scaling(float* __restrict__ scaling, const float* __restrict__ verts,
+                                             const int* __restrict__ cumsum, const int* __restrict__ num_points,
+                                             int prim, float3 of) {
+  if (scaling[prim] > 0.0f) return;
+  const int off = cumsum[prim], np = num_points[prim];
+  const d3 o = mkd(of.x, of.y, of.z);
   d3 cen = mkd(0, 0, 0);
   for (int i = 0; i < np; ++i) {
-    const float* v = p.verts + 3 * (size_t)(off + i);
+    const float* v = verts + 3 * (size_t)(off + i);
     cen = cen + mkd(v[0], v[1], v[2]);
   }
   cen = cen * (1.0 / (double)np);
   const d3 t2o = cen - o;
   double best = 0.0;
   for (int i = 0; i < np; ++i) {
-    const float* v = p.verts + 3 * (size_t)(off + i);
+    const float* v = verts + 3 * (size_t)(off + i);
     const d3 a = mkd(v[0], v[1], v[2]) - o;
     const double lab = len(a) * len(t2o);
     double ang = 0.0;
     if (!(lab < 1e-12)) ang = acos(fmax(-1.0, fmin(1.0, dot(a, t2o) / lab)));
     best = fmax(ang, best);
   }
-  p.scaling[prim] = (float)best;
+  scaling[prim] = (float)best;
 }
 
 // ---------------------------------------------------------------- the march
+// Per-thread shared memory: the traversal stack and the 16 keys of the
+// current chunk (staged out of registers before shading starts).
+struct Smem {
+  Stack st;
+  unsigned long long* keys;
+  int stride;
+};
+
+__device__ __forceinline__ Smem thread_smem() {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem s;
+  const int nt = blockDim.x;
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw);
+  uint32_t* refs = reinterpret_cast<uint32_t*>(smem_raw + (size_t)kChunk * nt * 8);
+  float* tns = reinterpret_cast<float*>(refs + (size_t)kStackDepth * nt);
+  s.keys = keys + threadIdx.x;
+  s.stride = nt;
+  s.st.ref = refs + threadIdx.x;
+  s.st.tn = tns + threadIdx.x;
+  s.st.stride = nt;
+  return s;
+}
+
 // Visits the hit stream of one ray in the reference's chunk order and calls
 // visit(prim, t) for each hit at or beyond the near plane; visit returns true
 // to end the ray (transmittance cut-off).
 template <class Visit>
-__device__ __forceinline__ void march(const BvhView& bvh, const RayW& r, int tmin_inclusive, Stack st, int* status,
-                                      Visit&& visit) {
+__device__ __forceinline__ void march(const BvhView& bvh, float3 o, float3 d, int tmin_inclusive, Smem sm,
+                                      int* status, Counters& cnt, Visit&& visit) {
   unsigned long long key_min = tmin_inclusive ? 0ull : (1ull << 32);
   float last_hit_t = 0.f;
   int ref_pos = 0;
-  unsigned long long kb[kChunk];
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
-    query(bvh, r, key_min, kb, st, t_drop, status);
+    {
+      const RayW r = make_ray(o, d);
+      unsigned long long kb[kChunk];
+      query(bvh, r, key_min, kb, sm.st, t_drop, status, cnt);
+#pragma unroll
+      for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+    }
     const bool truncated = t_drop < INFINITY;
     int consumed = 0;
     unsigned long long last_key = 0;
     bool boundary = false, done = false;
     for (int i = 0; i < kChunk; ++i) {
-      const unsigned long long key = kb[0];
-#pragma unroll
-      for (int j = 0; j < kChunk - 1; ++j) kb[j] = kb[j + 1];
-      kb[kChunk - 1] = kEmptyKey;
+      const unsigned long long key = sm.keys[i * sm.stride];
       if (key == kEmptyKey || (truncated && key_t(key) >= t_drop)) break;
       ++consumed;
       last_key = key;
@@ -360,50 +425,38 @@ __device__ __forceinline__ bool next_tile(const TraceParams& p, int& px, int& py
   return true;
 }
 
-__device__ __forceinline__ Stack thread_stack() {
-  extern __shared__ uint32_t smem[];
-  Stack st;
-  st.stride = blockDim.x;
-  st.ref = smem + threadIdx.x;
-  st.tn = reinterpret_cast<float*>(smem + kStackDepth * blockDim.x) + threadIdx.x;
-  return st;
-}
-
-__device__ __forceinline__ RayW load_ray(const float* ro, const float* rd, int pix) {
-  const float3 o = make_float3(ro[3 * pix], ro[3 * pix + 1], ro[3 * pix + 2]);
-  const float3 d = make_float3(rd[3 * pix], rd[3 * pix + 1], rd[3 * pix + 2]);
-  return make_ray(o, d);
+__device__ __forceinline__ void load_ray(const float* ro, const float* rd, int pix, float3& o, float3& d) {
+  o = make_float3(ro[3 * pix], ro[3 * pix + 1], ro[3 * pix + 2]);
+  d = make_float3(rd[3 * pix], rd[3 * pix + 1], rd[3 * pix + 2]);
 }
 
 // ---------------------------------------------------------------- forward
-__device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends) {
-  rays = __reduce_add_sync(0xFFFFFFFFu, rays);
-  evals = __reduce_add_sync(0xFFFFFFFFu, evals);
-  blends = __reduce_add_sync(0xFFFFFFFFu, blends);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(stats, (unsigned long long)rays);
-    atomicAdd(stats + 1, (unsigned long long)evals);
-    atomicAdd(stats + 2, (unsigned long long)blends);
+__device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends,
+                                          const Counters& c) {
+  const unsigned v[6] = {rays, evals, blends, c.nodes, c.tris, c.queries};
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[i]);
+    if ((threadIdx.x & 31) == 0) atomicAdd(stats + i, (unsigned long long)s);
   }
 }
 
-__global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
-  const Stack st = thread_stack();
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TraceParams p) {
+  const Smem sm = thread_smem();
   const int HW = p.H * p.W;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
+  Counters cnt;
   int px, py;
   while (next_tile(p, px, py)) {
     if (px >= p.W || py >= p.H) continue;
     ++n_rays;
     const int pix = py * p.W + px;
-    const RayW r = load_ray(p.ray_o, p.ray_d, pix);
-    const float3 u = unit_dir(r);
-    float B[16];
-    sh_basis(u.x, u.y, u.z, p.sh_degree, B);
+    float3 o, d;
+    load_ray(p.ray_o, p.ray_d, pix, o, d);
     float C0 = 0.f, C1 = 0.f, C2 = 0.f, N0 = 0.f, N1 = 0.f, N2 = 0.f, T = 1.0f;
-    march(p.bvh, r, p.tmin_inclusive, st, p.status, [&](uint32_t prim, float) -> bool {
+    march(p.bvh, o, d, p.tmin_inclusive, sm, p.status, cnt, [&](uint32_t prim, float) -> bool {
       const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-      const Geom g = window_fp64(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), r, __ldg(p.sigma + prim));
+      const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
       ++n_eval;
       const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
       if (alpha < kAlphaMin) return false;
@@ -411,12 +464,14 @@ __global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
       if (test_T < kTMin) return true;
       ++n_blend;
       p.density[prim] = 1.0f;
-      compute_scaling(p, (int)prim, r);
+      compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
       const float w = alpha * T;
       atomicMax(reinterpret_cast<int*>(p.max_blending) + prim, __float_as_int(w));
       N0 += g.n.x * w;
       N1 += g.n.y * w;
       N2 += g.n.z * w;
+      float B[16];
+      sh_basis(unit(d), p.sh_degree, B);
       const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
       C0 += fmaxf(c.x, 0.f) * w;
       C1 += fmaxf(c.y, 0.f) * w;
@@ -435,68 +490,60 @@ __global__ void __launch_bounds__(kTraceThreads) k_forward(TraceParams p) {
     p.out_others[kMidDepthCh * HW + pix] = 0.0f;
     p.out_others[kDistortionCh * HW + pix] = 0.0f;
   }
-  add_stats(p.stats, n_rays, n_eval, n_blend);
+  add_stats(p.stats, n_rays, n_eval, n_blend, cnt);
 }
 
 // ---------------------------------------------------------------- adjoint
-// Gradient of phi_max through the unit edge normals at the maximum and of the
-// face normal (tritracer/backward.cu:104-189), in FP64; returns the 9 vertex
-// gradients summed over both terms.
-__device__ __forceinline__ void window_bwd_fp64(float4 a, float4 b, float4 c, const Geom& g, double dL_dphi,
-                                                d3 dL_dn3, d3 (&gv)[3]) {
-  const d3 V[3] = {tod(a), tod(b), tod(c)};
-  gv[0] = gv[1] = gv[2] = mkd(0, 0, 0);
+// Gradient of phi_max through the unit edge normal of each edge at the maximum
+// (|d_k - phi_max| <= 1e-6) and of the face normal, as in
+// tritracer/backward.cu:104-189, in A-relative FP32 coordinates. Returns the
+// 9 vertex gradients summed over both terms.
+__device__ __forceinline__ void window_bwd(const Geom& g, float dL_dphi, float3 dL_dn3, float3 (&gv)[3]) {
+  const float3 V[3] = {make_float3(0.f, 0.f, 0.f), g.e1, g.e2};
+  gv[0] = gv[1] = gv[2] = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    if (fabs(g.d[k] - g.phi_max) > 1e-6) continue;
-    const d3 p1 = V[k], p2 = V[(k + 1) % 3], p3 = V[(k + 2) % 3];
-    const d3 n = cross(p1 - p3, p2 - p3);
-    const d3 ne = cross(n, p1 - p2);
-    const double inv = 1.0 / len(ne);
-    const d3 Ne = ne * inv;
+    if (fabsf(g.d[k] - g.phi_max) > 1e-6f) continue;
+    const float3 p1 = V[k], p2 = V[(k + 1) % 3], p3 = V[(k + 2) % 3];
+    const float3 aa = p1 - p3, bb = p2 - p3, cc = p1 - p2;
+    const float3 n = fcross(aa, bb);
+    const float3 ne = fcross(n, cc);
+    const float inv = 1.0f / flen(ne);
+    const float3 Ne = ne * inv;
     // dL/dne = (I - Ne Ne^T) dL/dNe / |ne|
-    const d3 dL_dNe = dL_dphi * (g.hp - p1);
-    const d3 dL_dne = (dL_dNe - Ne * dot(Ne, dL_dNe)) * inv;
-    // ne = ((p1-p3) x (p2-p3)) x (p1-p2), Jacobians in the form of
-    // vecmath.h:2808-2859; v^T [u]x = v x u for the skew terms
-    const d3 bb = p2 - p3, cc = p1 - p2, aa = p1 - p3;
-    const d3 axb = cross(aa, bb);
-    // v^T (b c^T - (b.c) I + [axb]x)
-    const d3 g1 = mkd(dot(dL_dne, bb) * cc.x, dot(dL_dne, bb) * cc.y, dot(dL_dne, bb) * cc.z) -
-                  dot(bb, cc) * dL_dne + cross(dL_dne, axb);
-    // v^T ((a.c) I - a c^T - [axb]x)
-    const d3 g2 = dot(aa, cc) * dL_dne - mkd(dot(dL_dne, aa) * cc.x, dot(dL_dne, aa) * cc.y, dot(dL_dne, aa) * cc.z) -
-                  cross(dL_dne, axb);
-    // v^T (c c^T - (c.c) I)
-    const d3 g3 = mkd(dot(dL_dne, cc) * cc.x, dot(dL_dne, cc) * cc.y, dot(dL_dne, cc) * cc.z) - dot(cc, cc) * dL_dne;
+    const float3 dL_dNe = dL_dphi * (g.q - p1);
+    const float3 v = (dL_dNe - Ne * fdot(Ne, dL_dNe)) * inv;
+    // ne = ((p1-p3) x (p2-p3)) x (p1-p2); Jacobians in the form of
+    // vecmath.h:2808-2859, with v^T [u]x = v x u for the skew terms
+    const float3 axb = n;
+    const float3 g1 = fdot(v, bb) * cc - fdot(bb, cc) * v + fcross(v, axb);
+    const float3 g2 = fdot(aa, cc) * v - fdot(v, aa) * cc - fcross(v, axb);
+    const float3 g3 = fdot(v, cc) * cc - fdot(cc, cc) * v;
     gv[k] = gv[k] + g1 - dL_dphi * Ne;
     gv[(k + 1) % 3] = gv[(k + 1) % 3] + g2;
     gv[(k + 2) % 3] = gv[(k + 2) % 3] + g3;
   }
   {
-    const d3 p1 = V[0], p2 = V[1], p3 = V[2];
-    const d3 n = cross(p1 - p3, p2 - p3);
-    const double inv = 1.0 / len(n);
-    const d3 Nn = n * inv;
-    const d3 dL_dn = (dL_dn3 - Nn * dot(Nn, dL_dn3)) * inv;
     // n = (p1-p3) x (p2-p3): dn/dp1 = [p3-p2]x etc.; v^T [u]x = v x u
-    gv[0] = gv[0] + cross(p3 - p2, dL_dn) * -1.0;
-    gv[1] = gv[1] + cross(p1 - p3, dL_dn) * -1.0;
-    gv[2] = gv[2] + cross(p2 - p1, dL_dn) * -1.0;
+    const float3 n = fcross(V[0] - V[2], V[1] - V[2]);
+    const float inv = 1.0f / flen(n);
+    const float3 Nn = n * inv;
+    const float3 v = (dL_dn3 - Nn * fdot(Nn, dL_dn3)) * inv;
+    gv[0] = gv[0] + fcross(v, V[2] - V[1]);
+    gv[1] = gv[1] + fcross(v, V[0] - V[2]);
+    gv[2] = gv[2] + fcross(v, V[1] - V[0]);
   }
 }
 
-__global__ void __launch_bounds__(kTraceThreads) k_backward(TraceParams p) {
-  const Stack st = thread_stack();
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(TraceParams p) {
+  const Smem sm = thread_smem();
   const int HW = p.H * p.W;
   int px, py;
   while (next_tile(p, px, py)) {
     if (px >= p.W || py >= p.H) continue;
     const int pix = py * p.W + px;
-    const RayW r = load_ray(p.ray_o, p.ray_d, pix);
-    const float3 u = unit_dir(r);
-    float B[16];
-    sh_basis(u.x, u.y, u.z, p.sh_degree, B);
+    float3 o, d;
+    load_ray(p.ray_o, p.ray_d, pix, o, d);
     const float Cf0 = p.colors[pix], Cf1 = p.colors[HW + pix], Cf2 = p.colors[2 * HW + pix];
     const float Df = p.others[kDepthCh * HW + pix];
     const float Nf0 = p.others[(kNormalCh + 0) * HW + pix], Nf1 = p.others[(kNormalCh + 1) * HW + pix],
@@ -506,17 +553,19 @@ __global__ void __launch_bounds__(kTraceThreads) k_backward(TraceParams p) {
     const float gN0 = p.dL_doth[(kNormalCh + 0) * HW + pix], gN1 = p.dL_doth[(kNormalCh + 1) * HW + pix],
                 gN2 = p.dL_doth[(kNormalCh + 2) * HW + pix];
     float C0 = 0.f, C1 = 0.f, C2 = 0.f, N0 = 0.f, N1 = 0.f, N2 = 0.f, D = 0.f, T = 1.0f;
-    march(p.bvh, r, p.tmin_inclusive, st, p.status, [&](uint32_t prim, float) -> bool {
+    Counters cnt;
+    march(p.bvh, o, d, p.tmin_inclusive, sm, p.status, cnt, [&](uint32_t prim, float) -> bool {
       const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-      const float4 va = __ldg(tr), vb = __ldg(tr + 1), vc = __ldg(tr + 2);
       const float sig = __ldg(p.sigma + prim);
-      const Geom g = window_fp64(va, vb, vc, r, sig);
+      const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
       const float opacity = __ldg(p.opac + prim);
       const float alpha = fminf(kAlphaMax, opacity * g.Cx);
       if (alpha < kAlphaMin) return false;
       const float test_T = T * (1.0f - alpha);
       if (test_T < kTMin) return true;
       const float w = alpha * T;
+      float B[16];
+      sh_basis(unit(d), p.sh_degree, B);
       const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
       const float c0 = fmaxf(raw.x, 0.f), c1 = fmaxf(raw.y, 0.f), c2 = fmaxf(raw.z, 0.f);
       C0 += c0 * w;
@@ -525,27 +574,26 @@ __global__ void __launch_bounds__(kTraceThreads) k_backward(TraceParams p) {
       N0 += g.n.x * w;
       N1 += g.n.y * w;
       N2 += g.n.z * w;
-      const float ht = (float)g.t;
-      D += w * ht;
+      D += w * g.t;
       // backward.cu:296-312; C/N/D already include this hit
       const float inv1a = 1.0f / (1.0f - alpha);
       float dL_dalpha = g0 * (T * c0 - (Cf0 - C0) * inv1a) + g1 * (T * c1 - (Cf1 - C1) * inv1a) +
                         g2 * (T * c2 - (Cf2 - C2) * inv1a);
-      dL_dalpha += gD * (T * ht - (Df - D) * inv1a);
+      dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
       dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
                    gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
       red_add(p.d_opac + prim, dL_dalpha * g.Cx);
       const float dL_dC = opacity * dL_dalpha;
-      if (g.phi_final > 0.0) red_add(p.d_sigma + prim, (float)((double)(dL_dC * g.Cx) * log(g.phi_final)));
-      const double dL_dphi = (double)sig / g.phi_max * (double)dL_dC * (double)g.Cx;
-      d3 gv[3];
-      window_bwd_fp64(va, vb, vc, g, dL_dphi, mkd((double)gN0 * w, (double)gN1 * w, (double)gN2 * w), gv);
+      if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
+      const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
+      float3 gv[3];
+      window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
       float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        red_add(dt + 3 * k + 0, (float)gv[k].x);
-        red_add(dt + 3 * k + 1, (float)gv[k].y);
-        red_add(dt + 3 * k + 2, (float)gv[k].z);
+        red_add(dt + 3 * k + 0, gv[k].x);
+        red_add(dt + 3 * k + 1, gv[k].y);
+        red_add(dt + 3 * k + 2, gv[k].z);
       }
       // SH: dRGB/dsh_k = B_k, masked where the colour was clamped at 0
       const float e0 = raw.x < 0.f ? 0.f : g0 * w, e1 = raw.y < 0.f ? 0.f : g1 * w, e2 = raw.z < 0.f ? 0.f : g2 * w;
@@ -563,10 +611,13 @@ __global__ void __launch_bounds__(kTraceThreads) k_backward(TraceParams p) {
           red_add4(dsh + 4 * q, v4[0], v4[1], v4[2], v4[3]);
         }
       } else {
-        for (int k = 0; k < n; ++k) {
-          red_add(dsh + 3 * k + 0, B[k] * e0);
-          red_add(dsh + 3 * k + 1, B[k] * e1);
-          red_add(dsh + 3 * k + 2, B[k] * e2);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          if (k < n) {
+            red_add(dsh + 3 * k + 0, B[k] * e0);
+            red_add(dsh + 3 * k + 1, B[k] * e1);
+            red_add(dsh + 3 * k + 2, B[k] * e2);
+          }
         }
       }
       T = test_T;
@@ -577,16 +628,19 @@ __global__ void __launch_bounds__(kTraceThreads) k_backward(TraceParams p) {
 
 // ---------------------------------------------------------------- hit stream
 __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p) {
-  const Stack st = thread_stack();
+  const Stack st = thread_smem().st;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.R) return;
-  const RayW r = load_ray(p.ray_o, p.ray_d, i);
+  float3 o, d;
+  load_ray(p.ray_o, p.ray_d, i, o, d);
+  const RayW r = make_ray(o, d);
   unsigned long long key_min = 0ull;
   unsigned long long kb[kChunk];
   int count = 0;
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
-    query(p.bvh, r, key_min, kb, st, t_drop, p.status);
+    Counters cnt;
+    query(p.bvh, r, key_min, kb, st, t_drop, p.status, cnt);
     int consumed = 0;
     unsigned long long last = 0;
 #pragma unroll
@@ -613,7 +667,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
 
 }  // namespace
 
-size_t trace_smem_bytes() { return (size_t)kStackDepth * kTraceThreads * 8; }
+size_t trace_smem_bytes() { return (size_t)kTraceThreads * (kStackDepth * 8 + kChunk * 8); }
 
 int trace_blocks_per_sm(int which) {
   int n = 0;

@@ -42,7 +42,7 @@ struct TraceParams {
   int tmin_inclusive;
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
-  unsigned long long* stats;  // [0] rays, [1] evaluated hits, [2] blended hits (forward)
+  unsigned long long* stats;  // forward: rays, evaluated hits, blended hits, node visits, triangle tests, queries
 };
 
 struct HitStreamParams {

@@ -217,8 +217,7 @@ class OptixTracer:
         """Synchronises; returns the handle's counters since reset_stats()."""
         s = _lib.TtStats()
         check(self._h, lib.tt_get_stats(self._h, ctypes.byref(s), _stream()))
-        return dict(rays=s.rays, evaluated_hits=s.evaluated_hits, blended_hits=s.blended_hits,
-                    kernel_launches=s.kernel_launches)
+        return {name: getattr(s, name) for name, _ in s._fields_}
 
     def reset_stats(self):
         check(self._h, lib.tt_reset_stats(self._h, _stream()))

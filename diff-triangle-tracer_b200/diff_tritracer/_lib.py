@@ -67,7 +67,9 @@ class TtBwdArgs(ctypes.Structure):
 
 class TtStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
-                ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong)]
+                ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
+                ("node_visits", ctypes.c_ulonglong), ("triangle_tests", ctypes.c_ulonglong),
+                ("queries", ctypes.c_ulonglong)]
 
 
 EXPORTS = (

@@ -153,16 +153,20 @@ const char* tt_last_error(const tt_tracer* h);
  * device code has no bounded loops to report on. */
 int tt_device_status(tt_tracer* h, void* stream);
 
-/* Counters of the handle's trace kernels since the last tt_reset_stats (no
+/* Counters of the handle's forward kernels since the last tt_reset_stats (no
  * reference counterpart; the reference reports only gpu_time). Evaluated hits
  * are hits at or beyond the near plane whose window function was computed;
- * blended hits are those composited. kernel_launches counts every kernel this
- * handle enqueued (BVH steps included). */
+ * blended hits are those composited; node visits, triangle tests and queries
+ * (k-closest traversals) describe the traversal work. kernel_launches counts
+ * every kernel this handle enqueued (BVH steps included). */
 typedef struct tt_stats {
   unsigned long long rays;
   unsigned long long evaluated_hits;
   unsigned long long blended_hits;
   unsigned long long kernel_launches;
+  unsigned long long node_visits;
+  unsigned long long triangle_tests;
+  unsigned long long queries;
 } tt_stats;
 
 /* Synchronises `stream`, then fills *out. */
