@@ -384,7 +384,8 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "hits_per_ray": {"evaluated": evals / max(rays_step, 1), "blended": blends / max(rays_step, 1)},
                    "traversal_per_ray": {k: st[k] / max(st["rays"], 1)
-                                         for k in ("queries", "node_visits", "triangle_tests")}},
+                                         for k in ("queries", "node_visits", "triangle_tests",
+                                                   "packet_node_visits")}},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "path": "diff_tritracer.Tracer autograd forward+backward, pinned host rays/grads in, image out"},
         "gpu_launches": int(round(launches_per_step * args.steps)),

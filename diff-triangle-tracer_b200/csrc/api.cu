@@ -14,6 +14,7 @@ struct tt_tracer {
   int device = 0;
   int num_sms = 148;
   int fwd_grid = 0, bwd_grid = 0;
+  int packets = 1;
   std::string err;
   tt::Bvh bvh;
   tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[6] from byte 16
@@ -101,8 +102,13 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
   }
-  h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(0);
-  h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1);
+  if (h->cfg.traversal < TT_TRAVERSAL_AUTO || h->cfg.traversal > TT_TRAVERSAL_LANES) {
+    delete h;
+    return TT_ERR_INVALID;
+  }
+  h->packets = h->cfg.traversal != TT_TRAVERSAL_LANES ? 1 : 0;
+  h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(0, h->packets);
+  h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1, h->packets);
   *out = h;
   return TT_OK;
 }
@@ -137,6 +143,7 @@ static tt::TraceParams base_params(tt_tracer* h, int H, int W, const float* ro, 
   p.ray_d = rd;
   p.tmin_inclusive = h->cfg.tmin_inclusive;
   p.variant = h->cfg.variant;
+  p.packets = h->packets;
   p.work = h->scratch.as<int>();
   p.status = h->scratch.as<int>() + 1;
   p.stats = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 16);
@@ -261,7 +268,7 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   if (!h) return TT_ERR_INVALID;
   if (!out) return fail(h, TT_ERR_INVALID, "null stats pointer");
   const cudaStream_t s = as_stream(stream);
-  unsigned long long v[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long v[7] = {0, 0, 0, 0, 0, 0, 0};
   TT_CUDA(h, cudaMemcpyAsync(v, h->scratch.as<char>() + 16, sizeof(v), cudaMemcpyDeviceToHost, s));
   TT_CUDA(h, cudaStreamSynchronize(s));
   out->rays = v[0];
@@ -271,12 +278,13 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   out->node_visits = v[3];
   out->triangle_tests = v[4];
   out->queries = v[5];
+  out->packet_node_visits = v[6];
   return TT_OK;
 }
 
 int tt_reset_stats(tt_tracer* h, void* stream) {
   if (!h) return TT_ERR_INVALID;
-  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 48, as_stream(stream)));
+  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 56, as_stream(stream)));
   h->launch_base = h->launches();
   return TT_OK;
 }

@@ -64,7 +64,7 @@ int setup_current_device(DeviceSetup** out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TT_ERR_CUDA;
     s.base = static_cast<unsigned char*>(p);
-    s.grid = sms * tt::trace_blocks_per_sm(0);
+    s.grid = sms * tt::trace_blocks_per_sm(0, 1);
     s.done = true;
   }
   *out = &s;
@@ -126,6 +126,7 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   p.out_others = a->out_others;
   p.variant = TT_VARIANT_PLAIN;
   p.tmin_inclusive = tmin_inclusive;
+  p.packets = 1;
   p.work = reinterpret_cast<int*>(counters);
   p.status = reinterpret_cast<int*>(counters) + 1;
   p.stats = reinterpret_cast<unsigned long long*>(counters + 16);

@@ -50,7 +50,7 @@ __device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsi
 }
 
 struct Counters {
-  unsigned nodes = 0, tris = 0, queries = 0;
+  unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
 };
 
 // The kChunk smallest hit keys >= key_min (t <= far) along the ray, in
@@ -158,6 +158,148 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
     }
     (void)avail;
     st.put(sp++, cref[best], best_t);
+  }
+}
+
+// ---------------------------------------------------------------- packets
+// Warp packet traversal for coherent rays (a warp = an 8x4-pixel tile of a
+// pinhole camera, whose rays all cross nearly the same BVH nodes). The warp
+// shares ONE stack in shared memory; an entry carries the node, the mask of
+// lanes whose ray hit its box and the smallest entry distance among them.
+// Every active lane tests its own ray (its own [t_lo, tmax] interval and
+// k-buffer) against the 8 children; ballots give each child's lane mask and
+// __reduce_min_sync its nearest entry distance; hit children are ranked
+// lane-parallel (lane c ranks child c) and pushed far-to-near. Control flow
+// is warp-uniform, so SIMT efficiency equals the fraction of lanes whose ray
+// still needs the node, and every node/triangle record is read once per warp.
+constexpr int kWarpStack = 96;
+
+struct WarpStack {
+  uint32_t* ref;
+  unsigned* mask;
+  float* tmin;
+};
+
+__device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
+                                             unsigned long long key_min, unsigned long long (&kb)[kChunk],
+                                             WarpStack ws, float& t_drop, int* status, Counters& cnt) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < kChunk; ++i) kb[i] = kEmptyKey;
+  t_drop = INFINITY;
+  const unsigned act = __ballot_sync(full, want);
+  if (act == 0 || !bvh.has_root) return;
+  if (want) ++cnt.queries;
+  const float t_lo = want ? key_t(key_min) : 0.f;
+  float tmax = want ? kFar : -1.0f;  // a lane without a query never passes a test
+  const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
+  const int fx = nx ^ 2, fy = ny ^ 2, fz = nz ^ 2;
+  if (lane == 0) {
+    ws.ref[0] = 0u;
+    ws.mask[0] = act;
+    ws.tmin[0] = 0.f;
+  }
+  __syncwarp();
+  int sp = 1;
+  for (int steps = 0; sp > 0; ++steps) {
+    if (steps > kMaxSteps) {
+      if (lane == 0) atomicOr(status, kStatusTimeout);
+      break;
+    }
+    --sp;
+    const uint32_t ref = ws.ref[sp];
+    const float emin = ws.tmin[sp];
+    // lanes whose interval now ends before the entry's nearest distance drop out
+    const unsigned m = ws.mask[sp] & __ballot_sync(full, tmax >= emin);
+    __syncwarp();
+    if (m == 0) continue;
+    const bool on = (m >> lane) & 1u;
+    if (ref_is_leaf(ref)) {
+      const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
+      if (on) cnt.tris += ntri;
+      for (uint32_t j = 0; j < ntri; ++j) {
+        const float4* tr = bvh.tris + 3 * (size_t)(first + j);
+        const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+        float t;
+        if (!on || !isect_tri(r, a, b, c, t)) continue;
+        if (!(t >= t_lo) || !(t <= tmax)) continue;
+        const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
+        if (key >= key_min && key < kb[kChunk - 1]) {
+          kb_insert(kb, key);
+          if (kb[kChunk - 1] != kEmptyKey) tmax = key_t(kb[kChunk - 1]);
+        }
+      }
+      continue;
+    }
+    if (on) ++cnt.nodes;
+    if (lane == 0) ++cnt.warp_nodes;
+    const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
+    float tn[8], tf[8];
+#define TT_AXIS(NEAR, FAR, INV, OI, FIRST)                                                       \
+    {                                                                                            \
+      const float4 n0 = __ldg(nd + (NEAR)), n1 = __ldg(nd + (NEAR) + 1);                          \
+      const float4 f0 = __ldg(nd + (FAR)), f1 = __ldg(nd + (FAR) + 1);                            \
+      const float N8[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};                        \
+      const float F8[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};                        \
+      _Pragma("unroll") for (int c = 0; c < 8; ++c) {                                            \
+        const float a = fmaf(N8[c], (INV), -(OI)), b = fmaf(F8[c], (INV), -(OI));                  \
+        tn[c] = (FIRST) ? fmaxf(a, t_lo) : fmaxf(tn[c], a);                                       \
+        tf[c] = (FIRST) ? fminf(b, tmax) : fminf(tf[c], b);                                       \
+      }                                                                                          \
+    }
+    TT_AXIS(nx, fx, r.ix, r.oix, true)
+    TT_AXIS(ny, fy, r.iy, r.oiy, false)
+    TT_AXIS(nz, fz, r.iz, r.oiz, false)
+#undef TT_AXIS
+    unsigned cm[8];
+    float cmin[8];
+    int nh = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const bool hit = on && tn[c] <= tf[c];
+      cm[c] = __ballot_sync(full, hit);
+      cmin[c] = __uint_as_float(__reduce_min_sync(full, hit ? __float_as_uint(tn[c]) : 0x7F800000u));
+      nh += cm[c] != 0u ? 1 : 0;
+    }
+    if (nh == 0) continue;
+    // lane c (c < 8) ranks child c: children nearer than it (ties by slot)
+    float mine = INFINITY;
+    unsigned mymask = 0u;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (lane == c) {
+        mine = cmin[c];
+        mymask = cm[c];
+      }
+    int rank = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      rank += (cm[c] != 0u && (cmin[c] < mine || (cmin[c] == mine && c < lane))) ? 1 : 0;
+    const int avail = kWarpStack - sp;
+    const int npush = nh < avail ? nh : avail;
+    if (lane < 8 && mymask != 0u && rank < npush) {
+      const float4 rw = __ldg(nd + 12 + (lane >> 2));
+      const float rv = (lane & 3) == 0 ? rw.x : ((lane & 3) == 1 ? rw.y : ((lane & 3) == 2 ? rw.z : rw.w));
+      const int pos = sp + npush - 1 - rank;  // nearest on top
+      ws.ref[pos] = __float_as_uint(rv);
+      ws.mask[pos] = mymask;
+      ws.tmin[pos] = mine;
+    }
+    if (nh > avail) {
+      // stack full: the farthest children are dropped; their rays only trust
+      // keys nearer than the dropped entry distance
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        int rc = 0;
+#pragma unroll
+        for (int c2 = 0; c2 < 8; ++c2)
+          rc += (cm[c2] != 0u && (cmin[c2] < cmin[c] || (cmin[c2] == cmin[c] && c2 < c))) ? 1 : 0;
+        if (cm[c] != 0u && rc >= npush && ((cm[c] >> lane) & 1u)) t_drop = fminf(t_drop, cmin[c]);
+      }
+    }
+    __syncwarp();
+    sp += npush;
   }
 }
 
@@ -352,133 +494,257 @@ __device__ __forceinline__ Smem thread_smem() {
   return s;
 }
 
-// Visits the hit stream of one ray in the reference's chunk order and calls
-// visit(prim, t) for each hit at or beyond the near plane; visit returns true
-// to end the ray (transmittance cut-off).
-template <class Visit>
-__device__ __forceinline__ void march(const BvhView& bvh, float3 o, float3 d, int tmin_inclusive, Smem sm,
-                                      int* status, Counters& cnt, Visit&& visit) {
-  unsigned long long key_min = tmin_inclusive ? 0ull : (1ull << 32);
-  float last_hit_t = 0.f;
-  int ref_pos = 0;
-  for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
-    float t_drop;
-    {
+// Where a ray's next k-closest query starts, and where it is inside the
+// reference's 16-hit chunk.
+struct Cursor {
+  unsigned long long key_min;
+  float last_hit_t;
+  int ref_pos;
+  int chunks;
+};
+
+__device__ __forceinline__ Cursor first_cursor(int tmin_inclusive) {
+  Cursor c;
+  c.key_min = tmin_inclusive ? 0ull : (1ull << 32);
+  c.last_hit_t = 0.f;
+  c.ref_pos = 0;
+  c.chunks = 0;
+  return c;
+}
+
+// Visits the staged keys of one query in the reference's chunk order
+// (forward.cu:99-154) and calls sh.visit(prim) for each hit at or beyond the
+// near plane; visit returns true to end the ray (transmittance cut-off).
+// Returns true when the ray is finished, else leaves in `cur` where the next
+// query starts: after every 16th visited hit the reference re-traces from
+// last_hit_t (closed interval) or just after it (open); after a truncated
+// query (stack overflow) the stream resumes right after the last key taken.
+template <class Shader>
+__device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Cursor& cur, int tmin_inclusive,
+                                              int* status, Shader& sh) {
+  const bool truncated = t_drop < INFINITY;
+  int consumed = 0;
+  unsigned long long last_key = 0;
+  for (int i = 0; i < kChunk; ++i) {
+    const unsigned long long key = sm.keys[i * sm.stride];
+    if (key == kEmptyKey || (truncated && key_t(key) >= t_drop)) break;
+    ++consumed;
+    last_key = key;
+    const float t = key_t(key);
+    // fmaxf(last + STEP_EPSILON, t) with the sum in double (forward.cu:111)
+    cur.last_hit_t = fmaxf(__double2float_rn(__dadd_rn((double)cur.last_hit_t, kStepEps)), t);
+    ++cur.ref_pos;
+    if (t >= kNear && sh.visit(key_prim(key))) return true;
+    if (cur.ref_pos == kChunk) {
+      cur.ref_pos = 0;
+      const unsigned long long tb = __float_as_uint(cur.last_hit_t);
+      cur.key_min = tmin_inclusive ? (tb << 32) : ((tb + 1ull) << 32);
+      return false;
+    }
+  }
+  if (truncated) {
+    if (consumed == 0) {
+      atomicOr(status, kStatusStack);
+      return true;
+    }
+    cur.key_min = last_key + 1ull;
+    return false;
+  }
+  return true;  // fewer than 16 hits left: the stream is exhausted
+}
+
+// Persistent warp driver. Each round: lanes without a ray take the next rays
+// of the tile-ordered image (8x4 pixels per 32 slots) from the global counter,
+// then every lane holding a ray runs its k-closest query, then every such lane
+// shades its chunk. Traversal and shading never mix inside a warp, and lanes
+// whose ray finished are refilled instead of idling.
+template <class Shader>
+__device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shader& sh, Counters& cnt) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int total = p.ntiles * 32;
+  bool have = false, exhausted = false;
+  Cursor cur = first_cursor(p.tmin_inclusive);
+  float3 o = make_float3(0.f, 0.f, 0.f), d = o;
+  for (;;) {
+    const unsigned need = __ballot_sync(full, !have && !exhausted);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(p.work, __popc(need));
+      base = __shfl_sync(full, base, leader);
+      if (!have && !exhausted) {
+        const int slot = base + __popc(need & lt);
+        if (slot >= total) {
+          exhausted = true;
+        } else {
+          const int tile = slot >> 5, l = slot & 31;
+          const int px = (tile % p.ntx) * 8 + (l & 7), py = (tile / p.ntx) * 4 + (l >> 3);
+          if (px < p.W && py < p.H) {
+            const int pix = py * p.W + px;
+            o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
+            d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
+            sh.begin(pix, o, d);
+            cur = first_cursor(p.tmin_inclusive);
+            have = true;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(full, have) == 0) {
+      if (__all_sync(full, exhausted)) break;
+      continue;
+    }
+    float t_drop = INFINITY;
+    if (have) {
       const RayW r = make_ray(o, d);
       unsigned long long kb[kChunk];
-      query(bvh, r, key_min, kb, sm.st, t_drop, status, cnt);
+      query(p.bvh, r, cur.key_min, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
       for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
     }
-    const bool truncated = t_drop < INFINITY;
-    int consumed = 0;
-    unsigned long long last_key = 0;
-    bool boundary = false, done = false;
-    for (int i = 0; i < kChunk; ++i) {
-      const unsigned long long key = sm.keys[i * sm.stride];
-      if (key == kEmptyKey || (truncated && key_t(key) >= t_drop)) break;
-      ++consumed;
-      last_key = key;
-      const float t = key_t(key);
-      // fmaxf(last + STEP_EPSILON, t) with the sum in double (forward.cu:111)
-      last_hit_t = fmaxf(__double2float_rn(__dadd_rn((double)last_hit_t, kStepEps)), t);
-      ++ref_pos;
-      if (t >= kNear && visit(key_prim(key), t)) {
+    __syncwarp();
+    if (have) {
+      bool done = consume_chunk(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+      if (!done && ++cur.chunks >= kMaxChunks) {
+        atomicOr(p.status, kStatusTimeout);
         done = true;
-        break;
       }
-      if (ref_pos == kChunk) {
-        boundary = true;
-        break;
+      if (done) {
+        sh.end();
+        have = false;
       }
     }
-    if (done) return;
-    if (boundary) {
-      // the reference's next optixTrace starts at last_hit_t
-      ref_pos = 0;
-      const unsigned long long tb = __float_as_uint(last_hit_t);
-      key_min = tmin_inclusive ? (tb << 32) : ((tb + 1ull) << 32);
-      continue;
-    }
-    if (truncated) {
-      if (consumed == 0) {
-        atomicOr(status, kStatusStack);
-        return;
-      }
-      key_min = last_key + 1ull;  // continue the same stream exactly
-      continue;
-    }
-    return;  // fewer than 16 hits left: the stream is exhausted
   }
-  atomicOr(status, kStatusTimeout);
 }
 
-__device__ __forceinline__ bool next_tile(const TraceParams& p, int& px, int& py) {
+// Packet driver: a warp takes an 8x4-pixel tile, then runs rounds of one
+// packet query (all lanes whose ray is unfinished) and one shading pass until
+// every ray of the tile is done.
+__device__ __forceinline__ WarpStack warp_stack(unsigned char* base) {
+  const int w = threadIdx.x >> 5;
+  WarpStack ws;
+  ws.ref = reinterpret_cast<uint32_t*>(base) + w * kWarpStack;
+  ws.mask = reinterpret_cast<unsigned*>(base + (size_t)(blockDim.x / 32) * kWarpStack * 4) + w * kWarpStack;
+  ws.tmin = reinterpret_cast<float*>(base + (size_t)(blockDim.x / 32) * kWarpStack * 8) + w * kWarpStack;
+  return ws;
+}
+
+template <class Shader>
+__device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& sm, WarpStack ws, Shader& sh,
+                                              Counters& cnt) {
+  const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
-  int tile = 0;
-  if (lane == 0) tile = atomicAdd(p.work, 1);
-  tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-  if (tile >= p.ntiles) return false;
-  const int tx = tile % p.ntx, ty = tile / p.ntx;
-  px = tx * 8 + (lane & 7);
-  py = ty * 4 + (lane >> 3);
-  return true;
+  for (;;) {
+    int tile = 0;
+    if (lane == 0) tile = atomicAdd(p.work, 1);
+    tile = __shfl_sync(full, tile, 0);
+    if (tile >= p.ntiles) break;
+    const int px = (tile % p.ntx) * 8 + (lane & 7), py = (tile / p.ntx) * 4 + (lane >> 3);
+    bool active = px < p.W && py < p.H;
+    float3 o = make_float3(0.f, 0.f, 1.f), d = make_float3(0.f, 0.f, 1.f);
+    Cursor cur = first_cursor(p.tmin_inclusive);
+    if (active) {
+      const int pix = py * p.W + px;
+      o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
+      d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
+      sh.begin(pix, o, d);
+    }
+    const RayW r = make_ray(o, d);
+    while (__any_sync(full, active)) {
+      float t_drop;
+      {
+        unsigned long long kb[kChunk];
+        packet_query(p.bvh, r, active, cur.key_min, kb, ws, t_drop, p.status, cnt);
+#pragma unroll
+        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+      }
+      if (active) {
+        bool done = consume_chunk(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+        if (!done && ++cur.chunks >= kMaxChunks) {
+          atomicOr(p.status, kStatusTimeout);
+          done = true;
+        }
+        if (done) {
+          sh.end();
+          active = false;
+        }
+      }
+    }
+  }
 }
 
-__device__ __forceinline__ void load_ray(const float* ro, const float* rd, int pix, float3& o, float3& d) {
-  o = make_float3(ro[3 * pix], ro[3 * pix + 1], ro[3 * pix + 2]);
-  d = make_float3(rd[3 * pix], rd[3 * pix + 1], rd[3 * pix + 2]);
+__device__ __forceinline__ Smem packet_smem(unsigned char*& rest) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem s;
+  s.keys = reinterpret_cast<unsigned long long*>(smem_raw) + threadIdx.x;
+  s.stride = blockDim.x;
+  s.st.ref = nullptr;
+  s.st.tn = nullptr;
+  s.st.stride = 0;
+  rest = smem_raw + (size_t)kChunk * blockDim.x * 8;
+  return s;
 }
 
 // ---------------------------------------------------------------- forward
 __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends,
                                           const Counters& c) {
-  const unsigned v[6] = {rays, evals, blends, c.nodes, c.tris, c.queries};
+  const unsigned v[7] = {rays, evals, blends, c.nodes, c.tris, c.queries, c.warp_nodes};
 #pragma unroll
-  for (int i = 0; i < 6; ++i) {
+  for (int i = 0; i < 7; ++i) {
     const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[i]);
     if ((threadIdx.x & 31) == 0) atomicAdd(stats + i, (unsigned long long)s);
   }
 }
 
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TraceParams p) {
-  const Smem sm = thread_smem();
-  const int HW = p.H * p.W;
+// forward.cu:109-152 per hit and :204-214 per ray.
+struct FwdShader {
+  const TraceParams& p;
+  int pix;
+  float3 o, d;
+  float C0, C1, C2, N0, N1, N2, T;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
-  Counters cnt;
-  int px, py;
-  while (next_tile(p, px, py)) {
-    if (px >= p.W || py >= p.H) continue;
+
+  __device__ explicit FwdShader(const TraceParams& params) : p(params) {}
+
+  __device__ __forceinline__ void begin(int pixel, float3 ro, float3 rd) {
+    pix = pixel;
+    o = ro;
+    d = rd;
+    C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
+    T = 1.0f;
     ++n_rays;
-    const int pix = py * p.W + px;
-    float3 o, d;
-    load_ray(p.ray_o, p.ray_d, pix, o, d);
-    float C0 = 0.f, C1 = 0.f, C2 = 0.f, N0 = 0.f, N1 = 0.f, N2 = 0.f, T = 1.0f;
-    march(p.bvh, o, d, p.tmin_inclusive, sm, p.status, cnt, [&](uint32_t prim, float) -> bool {
-      const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-      const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
-      ++n_eval;
-      const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
-      if (alpha < kAlphaMin) return false;
-      const float test_T = T * (1.0f - alpha);
-      if (test_T < kTMin) return true;
-      ++n_blend;
-      p.density[prim] = 1.0f;
-      compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
-      const float w = alpha * T;
-      atomicMax(reinterpret_cast<int*>(p.max_blending) + prim, __float_as_int(w));
-      N0 += g.n.x * w;
-      N1 += g.n.y * w;
-      N2 += g.n.z * w;
-      float B[16];
-      sh_basis(unit(d), p.sh_degree, B);
-      const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
-      C0 += fmaxf(c.x, 0.f) * w;
-      C1 += fmaxf(c.y, 0.f) * w;
-      C2 += fmaxf(c.z, 0.f) * w;
-      T = test_T;
-      return false;
-    });
+  }
+
+  __device__ __forceinline__ bool visit(uint32_t prim) {
+    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
+    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
+    ++n_eval;
+    const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
+    if (alpha < kAlphaMin) return false;
+    const float test_T = T * (1.0f - alpha);
+    if (test_T < kTMin) return true;
+    ++n_blend;
+    p.density[prim] = 1.0f;
+    compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
+    const float w = alpha * T;
+    atomicMax(reinterpret_cast<int*>(p.max_blending) + prim, __float_as_int(w));
+    N0 += g.n.x * w;
+    N1 += g.n.y * w;
+    N2 += g.n.z * w;
+    float B[16];
+    sh_basis(unit(d), p.sh_degree, B);
+    const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+    C0 += fmaxf(c.x, 0.f) * w;
+    C1 += fmaxf(c.y, 0.f) * w;
+    C2 += fmaxf(c.z, 0.f) * w;
+    T = test_T;
+    return false;
+  }
+
+  __device__ __forceinline__ void end() {
+    const int HW = p.H * p.W;
     p.out_color[pix] = C0 + T * p.bg[0];
     p.out_color[HW + pix] = C1 + T * p.bg[1];
     p.out_color[2 * HW + pix] = C2 + T * p.bg[2];
@@ -490,7 +756,20 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TracePara
     p.out_others[kMidDepthCh * HW + pix] = 0.0f;
     p.out_others[kDistortionCh * HW + pix] = 0.0f;
   }
-  add_stats(p.stats, n_rays, n_eval, n_blend, cnt);
+};
+
+template <int kPackets>
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TraceParams p) {
+  Counters cnt;
+  FwdShader sh(p);
+  if (kPackets) {
+    unsigned char* rest;
+    const Smem sm = packet_smem(rest);
+    drive_packets(p, sm, warp_stack(rest), sh, cnt);
+  } else {
+    drive(p, thread_smem(), sh, cnt);
+  }
+  add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
 // ---------------------------------------------------------------- adjoint
@@ -535,94 +814,122 @@ __device__ __forceinline__ void window_bwd(const Geom& g, float dL_dphi, float3 
   }
 }
 
+// backward.cu:191-350: the same march, running C/N/D that include the current
+// hit, dL/dalpha from the final values, scattered gradients.
+struct BwdShader {
+  const TraceParams& p;
+  float3 o, d;
+  float Cf0, Cf1, Cf2, Df, Nf0, Nf1, Nf2;
+  float g0, g1, g2, gD, gN0, gN1, gN2;
+  float C0, C1, C2, N0, N1, N2, D, T;
+
+  __device__ explicit BwdShader(const TraceParams& params) : p(params) {}
+
+  __device__ __forceinline__ void begin(int pix, float3 ro, float3 rd) {
+    const int HW = p.H * p.W;
+    o = ro;
+    d = rd;
+    Cf0 = p.colors[pix];
+    Cf1 = p.colors[HW + pix];
+    Cf2 = p.colors[2 * HW + pix];
+    Df = p.others[kDepthCh * HW + pix];
+    Nf0 = p.others[(kNormalCh + 0) * HW + pix];
+    Nf1 = p.others[(kNormalCh + 1) * HW + pix];
+    Nf2 = p.others[(kNormalCh + 2) * HW + pix];
+    g0 = p.dL_dpix[pix];
+    g1 = p.dL_dpix[HW + pix];
+    g2 = p.dL_dpix[2 * HW + pix];
+    gD = p.dL_doth[kDepthCh * HW + pix];
+    gN0 = p.dL_doth[(kNormalCh + 0) * HW + pix];
+    gN1 = p.dL_doth[(kNormalCh + 1) * HW + pix];
+    gN2 = p.dL_doth[(kNormalCh + 2) * HW + pix];
+    C0 = C1 = C2 = N0 = N1 = N2 = D = 0.f;
+    T = 1.0f;
+  }
+
+  __device__ __forceinline__ bool visit(uint32_t prim) {
+    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
+    const float sig = __ldg(p.sigma + prim);
+    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
+    const float opacity = __ldg(p.opac + prim);
+    const float alpha = fminf(kAlphaMax, opacity * g.Cx);
+    if (alpha < kAlphaMin) return false;
+    const float test_T = T * (1.0f - alpha);
+    if (test_T < kTMin) return true;
+    const float w = alpha * T;
+    float B[16];
+    sh_basis(unit(d), p.sh_degree, B);
+    const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+    const float c0 = fmaxf(raw.x, 0.f), c1 = fmaxf(raw.y, 0.f), c2 = fmaxf(raw.z, 0.f);
+    C0 += c0 * w;
+    C1 += c1 * w;
+    C2 += c2 * w;
+    N0 += g.n.x * w;
+    N1 += g.n.y * w;
+    N2 += g.n.z * w;
+    D += w * g.t;
+    // backward.cu:296-312; C/N/D already include this hit
+    const float inv1a = 1.0f / (1.0f - alpha);
+    float dL_dalpha = g0 * (T * c0 - (Cf0 - C0) * inv1a) + g1 * (T * c1 - (Cf1 - C1) * inv1a) +
+                      g2 * (T * c2 - (Cf2 - C2) * inv1a);
+    dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
+    dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
+                 gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
+    red_add(p.d_opac + prim, dL_dalpha * g.Cx);
+    const float dL_dC = opacity * dL_dalpha;
+    if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
+    const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
+    float3 gv[3];
+    window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
+    float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      red_add(dt + 3 * k + 0, gv[k].x);
+      red_add(dt + 3 * k + 1, gv[k].y);
+      red_add(dt + 3 * k + 2, gv[k].z);
+    }
+    // SH: dRGB/dsh_k = B_k, masked where the colour was clamped at 0
+    const float e0 = raw.x < 0.f ? 0.f : g0 * w, e1 = raw.y < 0.f ? 0.f : g1 * w, e2 = raw.z < 0.f ? 0.f : g2 * w;
+    float* dsh = p.d_sh + (size_t)prim * p.M * 3;
+    const int n = sh_count(p.sh_degree);
+    if (p.M == 16 && n == 16) {
+#pragma unroll
+      for (int q = 0; q < 12; ++q) {
+        float v4[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int idx = 4 * q + j, k = idx / 3, ch = idx % 3;
+          v4[j] = B[k] * (ch == 0 ? e0 : (ch == 1 ? e1 : e2));
+        }
+        red_add4(dsh + 4 * q, v4[0], v4[1], v4[2], v4[3]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k < n) {
+          red_add(dsh + 3 * k + 0, B[k] * e0);
+          red_add(dsh + 3 * k + 1, B[k] * e1);
+          red_add(dsh + 3 * k + 2, B[k] * e2);
+        }
+      }
+    }
+    T = test_T;
+    return false;
+  }
+
+  __device__ __forceinline__ void end() {}
+};
+
+template <int kPackets>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(TraceParams p) {
-  const Smem sm = thread_smem();
-  const int HW = p.H * p.W;
-  int px, py;
-  while (next_tile(p, px, py)) {
-    if (px >= p.W || py >= p.H) continue;
-    const int pix = py * p.W + px;
-    float3 o, d;
-    load_ray(p.ray_o, p.ray_d, pix, o, d);
-    const float Cf0 = p.colors[pix], Cf1 = p.colors[HW + pix], Cf2 = p.colors[2 * HW + pix];
-    const float Df = p.others[kDepthCh * HW + pix];
-    const float Nf0 = p.others[(kNormalCh + 0) * HW + pix], Nf1 = p.others[(kNormalCh + 1) * HW + pix],
-                Nf2 = p.others[(kNormalCh + 2) * HW + pix];
-    const float g0 = p.dL_dpix[pix], g1 = p.dL_dpix[HW + pix], g2 = p.dL_dpix[2 * HW + pix];
-    const float gD = p.dL_doth[kDepthCh * HW + pix];
-    const float gN0 = p.dL_doth[(kNormalCh + 0) * HW + pix], gN1 = p.dL_doth[(kNormalCh + 1) * HW + pix],
-                gN2 = p.dL_doth[(kNormalCh + 2) * HW + pix];
-    float C0 = 0.f, C1 = 0.f, C2 = 0.f, N0 = 0.f, N1 = 0.f, N2 = 0.f, D = 0.f, T = 1.0f;
-    Counters cnt;
-    march(p.bvh, o, d, p.tmin_inclusive, sm, p.status, cnt, [&](uint32_t prim, float) -> bool {
-      const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-      const float sig = __ldg(p.sigma + prim);
-      const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
-      const float opacity = __ldg(p.opac + prim);
-      const float alpha = fminf(kAlphaMax, opacity * g.Cx);
-      if (alpha < kAlphaMin) return false;
-      const float test_T = T * (1.0f - alpha);
-      if (test_T < kTMin) return true;
-      const float w = alpha * T;
-      float B[16];
-      sh_basis(unit(d), p.sh_degree, B);
-      const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
-      const float c0 = fmaxf(raw.x, 0.f), c1 = fmaxf(raw.y, 0.f), c2 = fmaxf(raw.z, 0.f);
-      C0 += c0 * w;
-      C1 += c1 * w;
-      C2 += c2 * w;
-      N0 += g.n.x * w;
-      N1 += g.n.y * w;
-      N2 += g.n.z * w;
-      D += w * g.t;
-      // backward.cu:296-312; C/N/D already include this hit
-      const float inv1a = 1.0f / (1.0f - alpha);
-      float dL_dalpha = g0 * (T * c0 - (Cf0 - C0) * inv1a) + g1 * (T * c1 - (Cf1 - C1) * inv1a) +
-                        g2 * (T * c2 - (Cf2 - C2) * inv1a);
-      dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
-      dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
-                   gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
-      red_add(p.d_opac + prim, dL_dalpha * g.Cx);
-      const float dL_dC = opacity * dL_dalpha;
-      if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
-      const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
-      float3 gv[3];
-      window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
-      float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        red_add(dt + 3 * k + 0, gv[k].x);
-        red_add(dt + 3 * k + 1, gv[k].y);
-        red_add(dt + 3 * k + 2, gv[k].z);
-      }
-      // SH: dRGB/dsh_k = B_k, masked where the colour was clamped at 0
-      const float e0 = raw.x < 0.f ? 0.f : g0 * w, e1 = raw.y < 0.f ? 0.f : g1 * w, e2 = raw.z < 0.f ? 0.f : g2 * w;
-      float* dsh = p.d_sh + (size_t)prim * p.M * 3;
-      const int n = sh_count(p.sh_degree);
-      if (p.M == 16 && n == 16) {
-#pragma unroll
-        for (int q = 0; q < 12; ++q) {
-          float v4[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int idx = 4 * q + j, k = idx / 3, ch = idx % 3;
-            v4[j] = B[k] * (ch == 0 ? e0 : (ch == 1 ? e1 : e2));
-          }
-          red_add4(dsh + 4 * q, v4[0], v4[1], v4[2], v4[3]);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          if (k < n) {
-            red_add(dsh + 3 * k + 0, B[k] * e0);
-            red_add(dsh + 3 * k + 1, B[k] * e1);
-            red_add(dsh + 3 * k + 2, B[k] * e2);
-          }
-        }
-      }
-      T = test_T;
-      return false;
-    });
+  Counters cnt;
+  BwdShader sh(p);
+  if (kPackets) {
+    unsigned char* rest;
+    const Smem sm = packet_smem(rest);
+    drive_packets(p, sm, warp_stack(rest), sh, cnt);
+  } else {
+    drive(p, thread_smem(), sh, cnt);
   }
 }
 
@@ -631,8 +938,8 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
   const Stack st = thread_smem().st;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.R) return;
-  float3 o, d;
-  load_ray(p.ray_o, p.ray_d, i, o, d);
+  const float3 o = make_float3(p.ray_o[3 * i], p.ray_o[3 * i + 1], p.ray_o[3 * i + 2]);
+  const float3 d = make_float3(p.ray_d[3 * i], p.ray_d[3 * i + 1], p.ray_d[3 * i + 2]);
   const RayW r = make_ray(o, d);
   unsigned long long key_min = 0ull;
   unsigned long long kb[kChunk];
@@ -667,29 +974,40 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
 
 }  // namespace
 
-size_t trace_smem_bytes() { return (size_t)kTraceThreads * (kStackDepth * 8 + kChunk * 8); }
+size_t trace_smem_bytes(int packets) {
+  if (packets) return (size_t)kTraceThreads * kChunk * 8 + (size_t)(kTraceThreads / 32) * kWarpStack * 12;
+  return (size_t)kTraceThreads * (kStackDepth * 8 + kChunk * 8);
+}
 
-int trace_blocks_per_sm(int which) {
+int trace_blocks_per_sm(int which, int packets) {
   int n = 0;
-  const void* fn = which == 0 ? (const void*)k_forward : (const void*)k_backward;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, trace_smem_bytes()) != cudaSuccess) n = 1;
+  const void* fn = which == 0 ? (packets ? (const void*)k_forward<1> : (const void*)k_forward<0>)
+                              : (packets ? (const void*)k_backward<1> : (const void*)k_backward<0>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, trace_smem_bytes(packets)) != cudaSuccess)
+    n = 1;
   return n > 0 ? n : 1;
 }
 
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {
-  k_forward<<<grid, kTraceThreads, trace_smem_bytes(), s>>>(p);
+  if (p.packets)
+    k_forward<1><<<grid, kTraceThreads, trace_smem_bytes(1), s>>>(p);
+  else
+    k_forward<0><<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
-  k_backward<<<grid, kTraceThreads, trace_smem_bytes(), s>>>(p);
+  if (p.packets)
+    k_backward<1><<<grid, kTraceThreads, trace_smem_bytes(1), s>>>(p);
+  else
+    k_backward<0><<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s) {
   const int grid = (p.R + kTraceThreads - 1) / kTraceThreads;
   if (grid == 0) return cudaSuccess;
-  k_hit_stream<<<grid, kTraceThreads, trace_smem_bytes(), s>>>(p);
+  k_hit_stream<<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ struct TraceParams {
   float sph_r, sph_cx, sph_cy, sph_cz;
   int samples;
   int tmin_inclusive;
+  int packets;  // 1: warp packet traversal (coherent rays), 0: one independent ray per lane
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward: rays, evaluated hits, blended hits, node visits, triangle tests, queries
@@ -60,9 +61,9 @@ struct HitStreamParams {
 constexpr int kTraceThreads = 128;
 constexpr int kStackDepth = 32;
 
-size_t trace_smem_bytes();
+size_t trace_smem_bytes(int packets);
 // Resident blocks per SM of the forward / adjoint kernels (occupancy query).
-int trace_blocks_per_sm(int which /*0 forward, 1 adjoint*/);
+int trace_blocks_per_sm(int which /*0 forward, 1 adjoint*/, int packets);
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);

@@ -72,7 +72,7 @@ class OptixTracer:
     refract.ptx, envlight.ptx / backward.ptx)."""
 
     def __init__(self, pkg_dir: str = "", forward: str = "forward.ptx", backward: str = "backward.ptx",
-                 tmin_inclusive: bool = True):
+                 tmin_inclusive: bool = True, traversal: str = "auto"):
         if forward not in _VARIANTS:
             raise RuntimeError(f"unknown forward program {forward!r}; expected one of {sorted(_VARIANTS)}")
         if backward != "backward.ptx":
@@ -84,6 +84,10 @@ class OptixTracer:
         cfg = _lib.TtConfig()
         cfg.variant = self.variant
         cfg.tmin_inclusive = 1 if tmin_inclusive else 0
+        modes = {"auto": _lib.TT_TRAVERSAL_AUTO, "packets": _lib.TT_TRAVERSAL_PACKETS, "lanes": _lib.TT_TRAVERSAL_LANES}
+        if traversal not in modes:
+            raise RuntimeError(f"traversal must be one of {sorted(modes)}")
+        cfg.traversal = modes[traversal]
         h = ctypes.c_void_p(0)
         rc = lib.tt_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != _lib.TT_OK:

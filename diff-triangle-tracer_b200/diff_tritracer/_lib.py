@@ -25,13 +25,18 @@ TT_VARIANT_REFLECT = 1
 TT_VARIANT_REFRACT = 2
 TT_VARIANT_ENVLIGHT = 3
 
+TT_TRAVERSAL_AUTO = 0
+TT_TRAVERSAL_PACKETS = 1
+TT_TRAVERSAL_LANES = 2
+
 _f = ctypes.POINTER(ctypes.c_float)
 _i = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
 
 
 class TtConfig(ctypes.Structure):
-    _fields_ = [("variant", ctypes.c_int), ("tmin_inclusive", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+    _fields_ = [("variant", ctypes.c_int), ("tmin_inclusive", ctypes.c_int), ("traversal", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
 
 
 class TtFwdArgs(ctypes.Structure):
@@ -69,7 +74,7 @@ class TtStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
                 ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
                 ("node_visits", ctypes.c_ulonglong), ("triangle_tests", ctypes.c_ulonglong),
-                ("queries", ctypes.c_ulonglong)]
+                ("queries", ctypes.c_ulonglong), ("packet_node_visits", ctypes.c_ulonglong)]
 
 
 EXPORTS = (

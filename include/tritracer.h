@@ -55,11 +55,17 @@ extern "C" {
 
 typedef struct tt_tracer tt_tracer;
 
+/* How the rays of a warp traverse the BVH. */
+#define TT_TRAVERSAL_AUTO 0    /* packets for camera-ordered rays (default) */
+#define TT_TRAVERSAL_PACKETS 1 /* a warp traverses its 8x4-pixel tile as one packet */
+#define TT_TRAVERSAL_LANES 2   /* every lane traverses its own ray */
+
 typedef struct tt_config {
   int variant;        /* TT_VARIANT_* (default PLAIN) */
   int tmin_inclusive; /* 1 (default): each re-trace starts AT the last hit's t,
                          the closed interval of optixTrace; 0: strictly after */
-  int reserved[6];    /* zero */
+  int traversal;      /* TT_TRAVERSAL_* */
+  int reserved[5];    /* zero */
 } tt_config;
 
 /* Arguments of the forward trace: OptixTracer::trace_fwd
@@ -156,8 +162,8 @@ int tt_device_status(tt_tracer* h, void* stream);
 /* Counters of the handle's forward kernels since the last tt_reset_stats (no
  * reference counterpart; the reference reports only gpu_time). Evaluated hits
  * are hits at or beyond the near plane whose window function was computed;
- * blended hits are those composited; node visits, triangle tests and queries
- * (k-closest traversals) describe the traversal work. kernel_launches counts
+ * blended hits are those composited; node visits (per ray), triangle tests and
+ * queries (k-closest traversals) describe the traversal work. kernel_launches counts
  * every kernel this handle enqueued (BVH steps included). */
 typedef struct tt_stats {
   unsigned long long rays;
@@ -167,6 +173,7 @@ typedef struct tt_stats {
   unsigned long long node_visits;
   unsigned long long triangle_tests;
   unsigned long long queries;
+  unsigned long long packet_node_visits; /* node visits counted once per warp packet */
 } tt_stats;
 
 /* Synchronises `stream`, then fills *out. */
