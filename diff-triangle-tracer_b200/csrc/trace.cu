@@ -27,7 +27,10 @@ namespace {
 
 constexpr int kMaxChunks = 1 << 20;   // bound on re-traces per ray
 constexpr int kMaxSteps = 1 << 24;    // bound on stack pops per query
-constexpr int kMinBlocks = 4;         // resident blocks per SM the register budget must allow
+#ifndef TT_MIN_BLOCKS
+#define TT_MIN_BLOCKS 5
+#endif
+constexpr int kMinBlocks = TT_MIN_BLOCKS;  // resident blocks per SM the register budget must allow
 
 struct Stack {
   uint32_t* ref;
@@ -180,13 +183,30 @@ struct WarpStack {
   float* tmin;
 };
 
+// Sorted insert into the lane's k-buffer in shared memory (hits are rare
+// next to box tests, so the buffer need not occupy 32 registers); kb_last
+// mirrors the largest key.
+__device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key,
+                                               unsigned long long& kb_last) {
+  int i = kChunk - 1;
+  while (i > 0) {
+    const unsigned long long prev = kb[(i - 1) * stride];
+    if (prev <= key) break;
+    kb[i * stride] = prev;
+    --i;
+  }
+  kb[i * stride] = key;
+  kb_last = kb[(kChunk - 1) * stride];
+}
+
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
-                                             unsigned long long key_min, unsigned long long (&kb)[kChunk],
+                                             unsigned long long key_min, unsigned long long* kb, int kstride,
                                              WarpStack ws, float& t_drop, int* status, Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int i = 0; i < kChunk; ++i) kb[i] = kEmptyKey;
+  for (int i = 0; i < kChunk; ++i) kb[i * kstride] = kEmptyKey;
+  unsigned long long kb_last = kEmptyKey;
   t_drop = INFINITY;
   const unsigned act = __ballot_sync(full, want);
   if (act == 0 || !bvh.has_root) return;
@@ -225,9 +245,9 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
         if (!on || !isect_tri(r, a, b, c, t)) continue;
         if (!(t >= t_lo) || !(t <= tmax)) continue;
         const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-        if (key >= key_min && key < kb[kChunk - 1]) {
-          kb_insert(kb, key);
-          if (kb[kChunk - 1] != kEmptyKey) tmax = key_t(kb[kChunk - 1]);
+        if (key >= key_min && key < kb_last) {
+          kb_insert_smem(kb, kstride, key, kb_last);
+          if (kb_last != kEmptyKey) tmax = key_t(kb_last);
         }
       }
       continue;
@@ -525,6 +545,7 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
   const bool truncated = t_drop < INFINITY;
   int consumed = 0;
   unsigned long long last_key = 0;
+  sh.prepare();
   for (int i = 0; i < kChunk; ++i) {
     const unsigned long long key = sm.keys[i * sm.stride];
     if (key == kEmptyKey || (truncated && key_t(key) >= t_drop)) break;
@@ -654,12 +675,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
     const RayW r = make_ray(o, d);
     while (__any_sync(full, active)) {
       float t_drop;
-      {
-        unsigned long long kb[kChunk];
-        packet_query(p.bvh, r, active, cur.key_min, kb, ws, t_drop, p.status, cnt);
-#pragma unroll
-        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
-      }
+      packet_query(p.bvh, r, active, cur.key_min, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
       if (active) {
         bool done = consume_chunk(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
         if (!done && ++cur.chunks >= kMaxChunks) {
@@ -716,6 +732,8 @@ struct FwdShader {
     T = 1.0f;
     ++n_rays;
   }
+
+  __device__ __forceinline__ void prepare() {}
 
   __device__ __forceinline__ bool visit(uint32_t prim) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
@@ -818,33 +836,40 @@ __device__ __forceinline__ void window_bwd(const Geom& g, float dL_dphi, float3 
 // hit, dL/dalpha from the final values, scattered gradients.
 struct BwdShader {
   const TraceParams& p;
+  int pix;
   float3 o, d;
+  // per-ray finals and upstream gradients, loaded for each chunk (so they do
+  // not occupy registers during traversal)
   float Cf0, Cf1, Cf2, Df, Nf0, Nf1, Nf2;
   float g0, g1, g2, gD, gN0, gN1, gN2;
   float C0, C1, C2, N0, N1, N2, D, T;
 
   __device__ explicit BwdShader(const TraceParams& params) : p(params) {}
 
-  __device__ __forceinline__ void begin(int pix, float3 ro, float3 rd) {
-    const int HW = p.H * p.W;
+  __device__ __forceinline__ void begin(int pixel, float3 ro, float3 rd) {
+    pix = pixel;
     o = ro;
     d = rd;
-    Cf0 = p.colors[pix];
-    Cf1 = p.colors[HW + pix];
-    Cf2 = p.colors[2 * HW + pix];
-    Df = p.others[kDepthCh * HW + pix];
-    Nf0 = p.others[(kNormalCh + 0) * HW + pix];
-    Nf1 = p.others[(kNormalCh + 1) * HW + pix];
-    Nf2 = p.others[(kNormalCh + 2) * HW + pix];
-    g0 = p.dL_dpix[pix];
-    g1 = p.dL_dpix[HW + pix];
-    g2 = p.dL_dpix[2 * HW + pix];
-    gD = p.dL_doth[kDepthCh * HW + pix];
-    gN0 = p.dL_doth[(kNormalCh + 0) * HW + pix];
-    gN1 = p.dL_doth[(kNormalCh + 1) * HW + pix];
-    gN2 = p.dL_doth[(kNormalCh + 2) * HW + pix];
     C0 = C1 = C2 = N0 = N1 = N2 = D = 0.f;
     T = 1.0f;
+  }
+
+  __device__ __forceinline__ void prepare() {
+    const int HW = p.H * p.W;
+    Cf0 = __ldg(p.colors + pix);
+    Cf1 = __ldg(p.colors + HW + pix);
+    Cf2 = __ldg(p.colors + 2 * HW + pix);
+    Df = __ldg(p.others + kDepthCh * HW + pix);
+    Nf0 = __ldg(p.others + (kNormalCh + 0) * HW + pix);
+    Nf1 = __ldg(p.others + (kNormalCh + 1) * HW + pix);
+    Nf2 = __ldg(p.others + (kNormalCh + 2) * HW + pix);
+    g0 = __ldg(p.dL_dpix + pix);
+    g1 = __ldg(p.dL_dpix + HW + pix);
+    g2 = __ldg(p.dL_dpix + 2 * HW + pix);
+    gD = __ldg(p.dL_doth + kDepthCh * HW + pix);
+    gN0 = __ldg(p.dL_doth + (kNormalCh + 0) * HW + pix);
+    gN1 = __ldg(p.dL_doth + (kNormalCh + 1) * HW + pix);
+    gN2 = __ldg(p.dL_doth + (kNormalCh + 2) * HW + pix);
   }
 
   __device__ __forceinline__ bool visit(uint32_t prim) {
