@@ -106,7 +106,8 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
     delete h;
     return TT_ERR_INVALID;
   }
-  h->packets = h->cfg.traversal != TT_TRAVERSAL_LANES ? 1 : 0;
+  // sphere variants bend rays incoherently: they always use per-lane traversal
+  h->packets = (h->cfg.traversal != TT_TRAVERSAL_LANES && h->cfg.variant == TT_VARIANT_PLAIN) ? 1 : 0;
   h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(0, h->packets);
   h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1, h->packets);
   *out = h;
@@ -163,10 +164,13 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   TT_REQUIRE(h, a->bg, "null background");
   int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
   if (rc != TT_OK) return rc;
+  float ex[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   if (h->cfg.variant != TT_VARIANT_PLAIN) {
     TT_REQUIRE(h, a->extra && a->extra_len >= (h->cfg.variant == TT_VARIANT_ENVLIGHT ? 5 : 4),
                "variant needs extra = [r, cx, cy, cz(, samples)]");
-    return fail(h, TT_ERR_INVALID, "secondary-ray variants are not available in this build");
+    // the sphere parameters are a few floats of a device tensor (extract_sphere, common.h:143-148)
+    TT_CUDA(h, cudaMemcpyAsync(ex, a->extra, sizeof(float) * (a->extra_len >= 5 ? 5 : 4), cudaMemcpyDeviceToHost, s));
+    TT_CUDA(h, cudaStreamSynchronize(s));
   }
   rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
   if (rc != TT_OK) return rc;
@@ -185,6 +189,11 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   p.max_blending = a->max_blending;
   p.out_color = a->out_color;
   p.out_others = a->out_others;
+  p.sph_r = ex[0];
+  p.sph_cx = ex[1];
+  p.sph_cy = ex[2];
+  p.sph_cz = ex[3];
+  p.samples = (int)ex[4];
   if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));

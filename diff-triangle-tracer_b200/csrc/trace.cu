@@ -606,9 +606,11 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
             const int pix = py * p.W + px;
             o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
             d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
-            sh.begin(pix, o, d);
             cur = first_cursor(p.tmin_inclusive);
-            have = true;
+            if (sh.begin(pix, o, d))
+              have = true;
+            else
+              sh.end();
           }
         }
       }
@@ -633,8 +635,12 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
         done = true;
       }
       if (done) {
-        sh.end();
-        have = false;
+        if (sh.next(o, d)) {  // another ray of the same pixel (envlight samples)
+          cur = first_cursor(p.tmin_inclusive);
+        } else {
+          sh.end();
+          have = false;
+        }
       }
     }
   }
@@ -670,7 +676,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       const int pix = py * p.W + px;
       o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
       d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
-      sh.begin(pix, o, d);
+      sh.begin(pix, o, d);  // the plain shaders always trace their one ray
     }
     const RayW r = make_ray(o, d);
     while (__any_sync(full, active)) {
@@ -724,14 +730,17 @@ struct FwdShader {
 
   __device__ explicit FwdShader(const TraceParams& params) : p(params) {}
 
-  __device__ __forceinline__ void begin(int pixel, float3 ro, float3 rd) {
+  __device__ __forceinline__ bool begin(int pixel, float3 ro, float3 rd) {
     pix = pixel;
     o = ro;
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
     T = 1.0f;
     ++n_rays;
+    return true;
   }
+
+  __device__ __forceinline__ bool next(float3&, float3&) { return false; }
 
   __device__ __forceinline__ void prepare() {}
 
@@ -787,6 +796,208 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TracePara
   } else {
     drive(p, thread_smem(), sh, cnt);
   }
+  add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
+}
+
+// ---------------------------------------------------------------- variants
+// Sphere variants of the reference (tritracer/reflect.cu, refract.cu,
+// envlight.cu, common.h:116-148), forward only as there. The analytic sphere
+// is extra = [r, cx, cy, cz, samples]. The secondary-ray set-up repeats the
+// reference's FP32 expressions with explicit round-to-nearest operations (no
+// contraction), so the bent rays equal the oracle's.
+namespace vf {
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return make_float3(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return make_float3(sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)); }
+__device__ __forceinline__ float3 scale(float3 a, float s) { return make_float3(mul(a.x, s), mul(a.y, s), mul(a.z, s)); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+  return make_float3(sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
+                     sub(mul(a.x, b.y), mul(a.y, b.x)));
+}
+__device__ __forceinline__ float3 normalize(float3 v) { return scale(v, div(1.0f, __fsqrt_rn(dot(v, v)))); }
+__device__ __forceinline__ float3 neg(float3 v) { return make_float3(-v.x, -v.y, -v.z); }
+// vecmath.h reflect: i - (2 n) dot(n, i)
+__device__ __forceinline__ float3 reflect(float3 i, float3 n) { return sub(i, scale(scale(n, 2.0f), dot(n, i))); }
+
+// common.h:116-141
+__device__ __forceinline__ bool hit_sphere(float r, float3 cnt, float3 o, float3 d, float& t) {
+  const float3 op = sub(o, cnt);
+  const float a = dot(d, d);
+  if (a <= 0.0f) return false;
+  const float b = dot(op, d);
+  const float c = sub(dot(op, op), mul(r, r));
+  float det = sub(mul(b, b), mul(c, a));
+  if (det < 0.0f) return false;
+  det = __fsqrt_rn(det);
+  t = div(sub(-b, det), a);
+  if ((double)t < kStepEps) {
+    t = div(add(-b, det), a);
+    if ((double)t < kStepEps) return false;
+  }
+  return true;
+}
+
+// refract.cu:24-45, kept as written (square roots where Snell's law has
+// squares; the same double/float mix)
+__device__ __forceinline__ bool refract_dir(float3& out, float3 in, float3 n, float eta_org) {
+  const float cos_i = dot(in, n);
+  float eta = eta_org;
+  if ((double)cos_i > 0.0) {
+    eta = __double2float_rn(__drcp_rn((double)eta_org));
+    n = neg(n);
+  }
+  const float sin2_i = __double2float_rn(fmax(0.0, __dsub_rn(1.0, (double)sqrtf(cos_i))));
+  const float sin2_t = div(sin2_i, __fsqrt_rn(eta));
+  if (sin2_t >= 1.0f) return false;
+  const float cos_t = __double2float_rn(sqrt(fmax(0.0, __dsub_rn(1.0, (double)sin2_t))));
+  out = add(scale(in, div(1.0f, eta)), scale(n, sub(div(-cos_i, eta), cos_t)));
+  return true;
+}
+
+// envlight.cu:25-51
+__device__ __forceinline__ float lcg(uint32_t& u) {
+  u = u * 1664525u + 1013904223u;
+  return mul((float)(u & 0x00FFFFFFu), 1.0f / 16777216.0f);
+}
+__device__ __forceinline__ float3 cosine_hemisphere(uint32_t& seed, float3 n) {
+  const float u = lcg(seed);
+  const float v = lcg(seed);
+  const float z = __fsqrt_rn(u);
+  const float rr = __fsqrt_rn(fmaxf(0.0f, __double2float_rn(__dsub_rn(1.0, (double)mul(z, z)))));
+  const float phi = mul(v, 6.2831853071795864769f);
+  const float3 dir = make_float3(mul(rr, cosf(phi)), mul(rr, sinf(phi)), z);
+  const float3 up = fabsf(n.z) < 0.999f ? make_float3(0.f, 0.f, 1.f) : make_float3(0.f, 1.f, 0.f);
+  const float3 t = normalize(cross(up, n));
+  const float3 b = normalize(cross(n, t));
+  return normalize(add(add(scale(t, dir.x), scale(b, dir.y)), scale(n, dir.z)));
+}
+}  // namespace vf
+
+struct VarShader {
+  const TraceParams& p;
+  int pix;
+  float3 o, d;
+  float C0, C1, C2, T;
+  // envlight: the bent surface point, sample index and running radiance
+  bool env;
+  int sample;
+  float3 so;
+  float A0, A1, A2;
+  unsigned n_rays = 0, n_eval = 0, n_blend = 0;
+
+  __device__ explicit VarShader(const TraceParams& params) : p(params) {}
+
+  __device__ __forceinline__ void env_ray(float3& ro, float3& rd) {
+    const float3 cnt = make_float3(p.sph_cx, p.sph_cy, p.sph_cz);
+    const float3 n = vf::normalize(vf::sub(so, cnt));
+    uint32_t seed = ((uint32_t)(pix + 1u) * 9781u) ^ ((uint32_t)(sample + 1u) * 6271u);
+    rd = vf::cosine_hemisphere(seed, n);
+    ro = vf::add(so, vf::scale(rd, (float)kStepEps));
+  }
+
+  __device__ __forceinline__ bool begin(int pixel, float3& ro, float3& rd) {
+    pix = pixel;
+    C0 = C1 = C2 = 0.f;
+    T = 1.0f;
+    env = false;
+    A0 = A1 = A2 = 0.f;
+    ++n_rays;
+    const float3 cnt = make_float3(p.sph_cx, p.sph_cy, p.sph_cz);
+    const float eps = (float)kStepEps;
+    float st;
+    const bool hit = vf::hit_sphere(p.sph_r, cnt, ro, rd, st);
+    if (p.variant == 1) {  // reflect.cu:42-48
+      if (hit) {
+        ro = vf::add(ro, vf::scale(rd, st));
+        const float3 n = vf::normalize(vf::sub(ro, cnt));
+        ro = vf::add(ro, vf::scale(n, eps));
+        rd = vf::reflect(vf::normalize(rd), n);
+      }
+    } else if (p.variant == 2) {  // refract.cu:47-71
+      if (hit) {
+        const float3 hp = vf::add(ro, vf::scale(rd, st));
+        const float3 n = vf::normalize(vf::sub(hp, cnt));
+        const float3 in = vf::normalize(rd);
+        const float ior = vf::div(1.5f, 1.0003f);
+        float3 nd = in;
+        if (!vf::refract_dir(nd, in, n, ior)) nd = vf::reflect(in, vf::dot(in, n) < 0.0f ? n : vf::neg(n));
+        ro = vf::add(hp, vf::scale(n, eps));
+        rd = nd;
+      }
+    } else if (hit) {  // envlight.cu:116-166
+      so = vf::add(ro, vf::scale(rd, st));
+      so = vf::add(so, vf::scale(vf::normalize(vf::sub(so, cnt)), eps));
+      env = true;
+      sample = 0;
+      if (p.samples <= 0) return false;
+      env_ray(ro, rd);
+    }
+    o = ro;
+    d = rd;
+    return true;
+  }
+
+  __device__ __forceinline__ void prepare() {}
+
+  __device__ __forceinline__ bool visit(uint32_t prim) {
+    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
+    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
+    ++n_eval;
+    const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
+    if (alpha < kAlphaMin) return false;
+    const float test_T = T * (1.0f - alpha);
+    if (test_T < kTMin) return true;
+    ++n_blend;
+    const float w = alpha * T;
+    float B[16];
+    sh_basis(unit(d), p.sh_degree, B);
+    const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+    C0 += fmaxf(c.x, 0.f) * w;
+    C1 += fmaxf(c.y, 0.f) * w;
+    C2 += fmaxf(c.z, 0.f) * w;
+    T = test_T;
+    return false;
+  }
+
+  __device__ __forceinline__ bool next(float3& ro, float3& rd) {
+    if (!env) return false;
+    A0 += C0 + T * p.bg[0];
+    A1 += C1 + T * p.bg[1];
+    A2 += C2 + T * p.bg[2];
+    if (++sample >= p.samples) return false;
+    C0 = C1 = C2 = 0.f;
+    T = 1.0f;
+    env_ray(ro, rd);
+    o = ro;
+    d = rd;
+    return true;
+  }
+
+  __device__ __forceinline__ void end() {
+    const int HW = p.H * p.W;
+    if (env) {  // mean sample radiance; transmittance 0
+      const float inv = 1.0f / (float)p.samples;
+      C0 = A0 * inv;
+      C1 = A1 * inv;
+      C2 = A2 * inv;
+      T = 0.0f;
+    }
+    p.out_color[pix] = C0 + T * p.bg[0];
+    p.out_color[HW + pix] = C1 + T * p.bg[1];
+    p.out_color[2 * HW + pix] = C2 + T * p.bg[2];
+#pragma unroll
+    for (int c = 0; c < 7; ++c) p.out_others[c * HW + pix] = 0.0f;  // variants write colour only
+  }
+};
+
+__global__ void __launch_bounds__(kTraceThreads, 4) k_variant(TraceParams p) {
+  Counters cnt;
+  VarShader sh(p);
+  drive(p, thread_smem(), sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
@@ -846,13 +1057,16 @@ struct BwdShader {
 
   __device__ explicit BwdShader(const TraceParams& params) : p(params) {}
 
-  __device__ __forceinline__ void begin(int pixel, float3 ro, float3 rd) {
+  __device__ __forceinline__ bool begin(int pixel, float3 ro, float3 rd) {
     pix = pixel;
     o = ro;
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = D = 0.f;
     T = 1.0f;
+    return true;
   }
+
+  __device__ __forceinline__ bool next(float3&, float3&) { return false; }
 
   __device__ __forceinline__ void prepare() {
     const int HW = p.H * p.W;
@@ -1014,7 +1228,9 @@ int trace_blocks_per_sm(int which, int packets) {
 }
 
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {
-  if (p.packets)
+  if (p.variant != 0)
+    k_variant<<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
+  else if (p.packets)
     k_forward<1><<<grid, kTraceThreads, trace_smem_bytes(1), s>>>(p);
   else
     k_forward<0><<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);

@@ -219,3 +219,44 @@ def test_traversal_modes_agree(name, sc, rays):
         np.testing.assert_array_equal(fp[k], fl[k], err_msg=k)
     for k in ("dtri", "dsigma", "dopac", "dsh"):
         assert rel_norm(bp[k], bl[k]) < 1e-5, k
+
+
+VARIANTS = [("reflect.ptx", 1), ("refract.ptx", 2), ("envlight.ptx", 3)]
+
+
+@pytest.mark.parametrize("prog,variant", VARIANTS, ids=[v[0] for v in VARIANTS])
+def test_sphere_variants_vs_fp64_oracle(oracle, prog, variant):
+    """Reflect / refract / envlight programs (forward only, as in the
+    reference) against the FP64 oracle's restatement of reflect.cu,
+    refract.cu and envlight.cu. The bent rays are built with the same FP32
+    operations on both sides; envlight's sample directions go through cosf /
+    sinf, whose last-bit differences between CUDA and the host libm move the
+    sample rays slightly, so its tolerance is wider."""
+    from scenes_for_tests import sphere_extra
+
+    sc = dense_scene(seed=1, P=3000)
+    ro, rd = dense_view(H=48, W=64)
+    H, W = ro.shape[:2]
+    extra = sphere_extra(samples=3)
+    bg = np.array([0.1, 0.2, 0.3], np.float32)
+    tr = _C.OptixTracer("", prog, "backward.ptx")
+    out = gpu_forward(tr, sc, ro, rd, settings(bg=bg, extra=extra))
+    tr.device_status()
+    ref = oracle.forward(sc, ro, rd, bg=bg, extra=extra, variant=variant, precision=64, exact=True,
+                         canonical=True, record=512, nthreads=8)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    assert ok.mean() > 0.9
+    plain = oracle.forward(sc, ro, rd, bg=bg, precision=64, exact=True, canonical=True, nthreads=8)
+    assert (np.abs(ref.color - plain.color).max(0) > 1e-4).mean() > 0.2  # the sphere bends many rays
+    err = np.abs(out["color"] - ref.color)[:, ok]
+    b = np.abs(ref.color)[:, ok]
+    print(f"{prog}: max abs {err.max():.2e}, rms {np.sqrt((err ** 2).mean()):.2e}")
+    assert np.all(out["others"] == 0)
+    if variant == 3:
+        assert np.sqrt((err ** 2).mean()) < 1e-4 and err.max() < 2e-2
+    else:
+        assert np.all(err <= RTOL * b + ATOL)
+    # reference-style backward after a variant forward: the plain adjoint
+    g, go = scenes.upstream_grads(H, W, seed=3)
+    grads = gpu_backward(tr, sc, ro, rd, settings(bg=bg), out["color"], out["others"], g, go)
+    assert all(np.isfinite(v).all() for v in grads.values())
