@@ -14,7 +14,7 @@ struct tt_tracer {
   int device = 0;
   int num_sms = 148;
   int fwd_grid = 0, bwd_grid = 0;
-  int packets = 1;
+  int cfg_id = tt::kCfgPackets16;
   std::string err;
   tt::Bvh bvh;
   tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[6] from byte 16
@@ -102,15 +102,35 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
   }
-  if (h->cfg.traversal < TT_TRAVERSAL_AUTO || h->cfg.traversal > TT_TRAVERSAL_LANES) {
+  if (tt_set_traversal(h, h->cfg.traversal, h->cfg.k, h->cfg.stack_depth) != TT_OK) {
     delete h;
     return TT_ERR_INVALID;
   }
-  // sphere variants bend rays incoherently: they always use per-lane traversal
-  h->packets = (h->cfg.traversal != TT_TRAVERSAL_LANES && h->cfg.variant == TT_VARIANT_PLAIN) ? 1 : 0;
-  h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(0, h->packets);
-  h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1, h->packets);
   *out = h;
+  return TT_OK;
+}
+
+int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, traversal >= TT_TRAVERSAL_AUTO && traversal <= TT_TRAVERSAL_LANES, "unknown traversal mode");
+  TT_REQUIRE(h, k == 0 || k == 16 || k == 32, "k must be 16 or 32");
+  TT_REQUIRE(h, stack_depth == 0 || stack_depth == 24 || stack_depth == 32, "stack_depth must be 24 or 32");
+  // sphere variants bend rays incoherently: they always trace lane by lane
+  const bool lanes = traversal == TT_TRAVERSAL_LANES || h->cfg.variant != TT_VARIANT_PLAIN;
+  TT_REQUIRE(h, !(lanes && k == 32), "k = 32 needs packet traversal");
+  TT_REQUIRE(h, lanes || stack_depth == 0 || stack_depth == 32, "stack_depth applies to lane traversal");
+  int id;
+  if (lanes)
+    id = stack_depth == 24 ? tt::kCfgLanes24 : tt::kCfgLanes32;
+  else
+    id = k == 32 ? tt::kCfgPackets32 : tt::kCfgPackets16;
+  h->cfg.traversal = traversal;
+  h->cfg.k = k;
+  h->cfg.stack_depth = stack_depth;
+  h->cfg_id = id;
+  const int which = h->cfg.variant != TT_VARIANT_PLAIN ? 2 : 0;
+  h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(which, id);
+  h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1, id);
   return TT_OK;
 }
 
@@ -132,32 +152,49 @@ int tt_build(tt_tracer* h, const float* vertices, int num_vertices, const int* c
   return accel_step(h, vertices, num_vertices, cumsum, P, mode, as_stream(stream));
 }
 
-static tt::TraceParams base_params(tt_tracer* h, int H, int W, const float* ro, const float* rd) {
+static tt::TraceParams base_params(tt_tracer* h) {
   tt::TraceParams p;
   std::memset(&p, 0, sizeof(p));
   p.bvh = h->bvh.view();
-  p.H = H;
-  p.W = W;
-  p.ntx = (W + 7) / 8;
-  p.ntiles = p.ntx * ((H + 3) / 4);
-  p.ray_o = ro;
-  p.ray_d = rd;
   p.tmin_inclusive = h->cfg.tmin_inclusive;
   p.variant = h->cfg.variant;
-  p.packets = h->packets;
+  p.cfg = h->cfg_id;
   p.work = h->scratch.as<int>();
   p.status = h->scratch.as<int>() + 1;
   p.stats = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 16);
   return p;
 }
 
-int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
-  if (!h) return TT_ERR_INVALID;
-  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+// Appends a view to the launch: its tiles follow the previous views'.
+static int add_view(tt_tracer* h, tt::TraceParams& p, const tt_view& v) {
+  TT_REQUIRE(h, p.nviews < tt::kMaxViews, "at most 32 views per call");
+  TT_REQUIRE(h, v.H > 0 && v.W > 0, "every view needs H, W > 0");
+  TT_REQUIRE(h, (long long)v.H * v.W < (1ll << 31), "too many rays in a view");
+  TT_REQUIRE(h, v.ray_o && v.ray_d, "null ray pointer in a view");
+  tt::ViewDesc& d = p.views[p.nviews++];
+  d.ray_o = v.ray_o;
+  d.ray_d = v.ray_d;
+  d.out_color = v.out_color;
+  d.out_others = v.out_others;
+  d.colors = v.colors;
+  d.others = v.others;
+  d.dL_dpix = v.dL_dpixels;
+  d.dL_doth = v.dL_dothers;
+  d.H = v.H;
+  d.W = v.W;
+  d.ntx = (v.W + 7) / 8;
+  d.tile_begin = p.ntiles;
+  const long long tiles = (long long)p.ntiles + (long long)d.ntx * ((v.H + 3) / 4);
+  TT_REQUIRE(h, tiles < (1ll << 26), "too many tiles in one call");
+  p.ntiles = (int)tiles;
+  return TT_OK;
+}
+
+static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views, int nviews, void* stream) {
   const cudaStream_t s = as_stream(stream);
-  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
-  TT_REQUIRE(h, (long long)a->H * a->W < (1ll << 31), "too many rays");
-  TT_REQUIRE(h, a->ray_o && a->ray_d && a->out_color && a->out_others, "null ray or output pointer");
+  TT_REQUIRE(h, nviews >= 1, "need at least one view");
+  for (int i = 0; i < nviews; ++i)
+    TT_REQUIRE(h, views[i].out_color && views[i].out_others, "null output pointer in a view");
   TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->scaling && a->density_factor && a->max_blending &&
                               a->num_points),
              "null per-triangle pointer");
@@ -172,9 +209,14 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
     TT_CUDA(h, cudaMemcpyAsync(ex, a->extra, sizeof(float) * (a->extra_len >= 5 ? 5 : 4), cudaMemcpyDeviceToHost, s));
     TT_CUDA(h, cudaStreamSynchronize(s));
   }
+  tt::TraceParams p = base_params(h);
+  for (int i = 0; i < nviews; ++i) {
+    rc = add_view(h, p, views[i]);
+    if (rc != TT_OK) return rc;
+  }
   rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
   if (rc != TT_OK) return rc;
-  tt::TraceParams p = base_params(h, a->H, a->W, a->ray_o, a->ray_d);
+  p.bvh = h->bvh.view();
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
   p.num_points = a->num_points;
@@ -187,8 +229,6 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   p.scaling = a->scaling;
   p.density = a->density_factor;
   p.max_blending = a->max_blending;
-  p.out_color = a->out_color;
-  p.out_others = a->out_others;
   p.sph_r = ex[0];
   p.sph_cx = ex[1];
   p.sph_cy = ex[2];
@@ -209,13 +249,34 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   return TT_OK;
 }
 
-int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
+int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
   if (!h) return TT_ERR_INVALID;
   if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
-  const cudaStream_t s = as_stream(stream);
   TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
-  TT_REQUIRE(h, a->ray_o && a->ray_d && a->colors && a->others && a->dL_dpixels && a->dL_dothers,
-             "null ray, forward-output or upstream-gradient pointer");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->out_color && a->out_others, "null ray or output pointer");
+  tt_view v;
+  std::memset(&v, 0, sizeof(v));
+  v.H = a->H;
+  v.W = a->W;
+  v.ray_o = a->ray_o;
+  v.ray_d = a->ray_d;
+  v.out_color = a->out_color;
+  v.out_others = a->out_others;
+  return forward_impl(h, a, &v, 1, stream);
+}
+
+int tt_forward_views(tt_tracer* h, const tt_fwd_args* a, const tt_view* views, int n_views, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a || !views) return fail(h, TT_ERR_INVALID, "null argument block or view list");
+  return forward_impl(h, a, views, n_views, stream);
+}
+
+static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, int nviews, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  TT_REQUIRE(h, nviews >= 1, "need at least one view");
+  for (int i = 0; i < nviews; ++i)
+    TT_REQUIRE(h, views[i].colors && views[i].others && views[i].dL_dpixels && views[i].dL_dothers,
+               "null forward-output or upstream-gradient pointer in a view");
   TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->cumsum && a->vertices), "null per-triangle pointer");
   TT_REQUIRE(h, a->P == 0 || (a->dL_dtriangle && a->dL_dsigma && a->dL_dopacity && a->dL_dsh),
              "null gradient output");
@@ -223,13 +284,17 @@ int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
   if (rc != TT_OK) return rc;
   if (!h->bvh.built()) return fail(h, TT_ERR_STATE, "backward before any forward/build");
   if (h->bvh.P() != a->P) return fail(h, TT_ERR_STATE, "backward with a different triangle count than the forward");
+  tt::TraceParams p = base_params(h);
+  for (int i = 0; i < nviews; ++i) {
+    rc = add_view(h, p, views[i]);
+    if (rc != TT_OK) return rc;
+  }
   if (a->P > 0) {
     TT_CUDA(h, cudaMemsetAsync(a->dL_dtriangle, 0, (size_t)a->num_vertices * 3 * sizeof(float), s));
     TT_CUDA(h, cudaMemsetAsync(a->dL_dsigma, 0, (size_t)a->P * sizeof(float), s));
     TT_CUDA(h, cudaMemsetAsync(a->dL_dopacity, 0, (size_t)a->P * sizeof(float), s));
     TT_CUDA(h, cudaMemsetAsync(a->dL_dsh, 0, (size_t)a->P * a->M * 3 * sizeof(float), s));
   }
-  tt::TraceParams p = base_params(h, a->H, a->W, a->ray_o, a->ray_d);
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
   p.num_points = a->num_points;
@@ -239,10 +304,6 @@ int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
   p.opac = a->opacities;
   p.sigma = a->sigma;
   p.bg = a->bg;
-  p.colors = a->colors;
-  p.others = a->others;
-  p.dL_dpix = a->dL_dpixels;
-  p.dL_doth = a->dL_dothers;
   p.d_tri = a->dL_dtriangle;
   p.d_sigma = a->dL_dsigma;
   p.d_opac = a->dL_dopacity;
@@ -259,6 +320,31 @@ int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
     if (a->gpu_time_ms) *a->gpu_time_ms = ms;
   }
   return TT_OK;
+}
+
+int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->colors && a->others && a->dL_dpixels && a->dL_dothers,
+             "null ray, forward-output or upstream-gradient pointer");
+  tt_view v;
+  std::memset(&v, 0, sizeof(v));
+  v.H = a->H;
+  v.W = a->W;
+  v.ray_o = a->ray_o;
+  v.ray_d = a->ray_d;
+  v.colors = a->colors;
+  v.others = a->others;
+  v.dL_dpixels = a->dL_dpixels;
+  v.dL_dothers = a->dL_dothers;
+  return backward_impl(h, a, &v, 1, stream);
+}
+
+int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, int n_views, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a || !views) return fail(h, TT_ERR_INVALID, "null argument block or view list");
+  return backward_impl(h, a, views, n_views, stream);
 }
 
 int tt_device_status(tt_tracer* h, void* stream) {

@@ -64,7 +64,7 @@ int setup_current_device(DeviceSetup** out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TT_ERR_CUDA;
     s.base = static_cast<unsigned char*>(p);
-    s.grid = sms * tt::trace_blocks_per_sm(0, 1);
+    s.grid = sms * tt::trace_blocks_per_sm(0, tt::kCfgPackets16);
     s.done = true;
   }
   *out = &s;
@@ -104,12 +104,17 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   tt::TraceParams p;
   std::memset(&p, 0, sizeof(p));
   p.bvh = tt::bvh_storage_view(st, a->P);
-  p.H = a->H;
-  p.W = a->W;
-  p.ntx = (a->W + 7) / 8;
-  p.ntiles = p.ntx * ((a->H + 3) / 4);
-  p.ray_o = a->ray_o;
-  p.ray_d = a->ray_d;
+  p.nviews = 1;
+  tt::ViewDesc& v = p.views[0];
+  v.ray_o = a->ray_o;
+  v.ray_d = a->ray_d;
+  v.out_color = a->out_color;
+  v.out_others = a->out_others;
+  v.H = a->H;
+  v.W = a->W;
+  v.ntx = (a->W + 7) / 8;
+  v.tile_begin = 0;
+  p.ntiles = v.ntx * ((a->H + 3) / 4);
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
   p.num_points = a->num_points;
@@ -122,11 +127,9 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   p.scaling = a->scaling;
   p.density = a->density_factor;
   p.max_blending = a->max_blending;
-  p.out_color = a->out_color;
-  p.out_others = a->out_others;
   p.variant = TT_VARIANT_PLAIN;
   p.tmin_inclusive = tmin_inclusive;
-  p.packets = 1;
+  p.cfg = tt::kCfgPackets16;
   p.work = reinterpret_cast<int*>(counters);
   p.status = reinterpret_cast<int*>(counters) + 1;
   p.stats = reinterpret_cast<unsigned long long*>(counters + 16);

@@ -32,6 +32,10 @@ constexpr int kMaxSteps = 1 << 24;    // bound on stack pops per query
 #endif
 constexpr int kMinBlocks = TT_MIN_BLOCKS;  // resident blocks per SM the register budget must allow
 
+// Per-lane traversal stack: the top SD entries in shared memory (strided by
+// the block size, conflict-free), continued in thread-local memory for deep
+// trees (only touched when the shared part is full).
+constexpr int kSpill = 64;
 struct Stack {
   uint32_t* ref;
   float* tn;
@@ -66,6 +70,7 @@ struct Counters {
 // boxes are padded outward when written (k_wide_boxes) so the rounded test
 // never culls a reported hit, and empty slots hold inverted boxes that never
 // pass. Hit children are pushed in slot order with the nearest one on top.
+template <int SD>
 __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min,
                                       unsigned long long (&kb)[kChunk], Stack st, float& t_drop, int* status,
                                       Counters& cnt) {
@@ -79,8 +84,19 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
   // word offsets of the near / far planes (lo at +0, hi at +2 within each axis)
   const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
   const int fx = nx ^ 2, fy = ny ^ 2, fz = nz ^ 2;
+  // entries at index >= SD live in thread-local memory
+  uint32_t xref[kSpill];
+  float xtn[kSpill];
+  auto put = [&](int i, uint32_t r, float t) {
+    if (i < SD) {
+      st.put(i, r, t);
+    } else {
+      xref[i - SD] = r;
+      xtn[i - SD] = t;
+    }
+  };
   int sp = 0;
-  st.put(sp++, 0u, t_lo);
+  put(sp++, 0u, t_lo);
   int steps = 0;
   while (sp > 0) {
     if (++steps > kMaxSteps) {
@@ -88,8 +104,8 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
       break;
     }
     --sp;
-    const uint32_t ref = st.ref[sp * st.stride];
-    if (st.tn[sp * st.stride] > tmax) continue;
+    const uint32_t ref = sp < SD ? st.ref[sp * st.stride] : xref[sp - SD];
+    if ((sp < SD ? st.tn[sp * st.stride] : xtn[sp - SD]) > tmax) continue;
     if (ref_is_leaf(ref)) {
       const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
       cnt.tris += ntri;
@@ -149,18 +165,16 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
                               __float_as_uint(r1.z), __float_as_uint(r1.w)};
     // nearest child last (top of the stack); on overflow drop the others and
     // remember the smallest distance dropped
-    const int avail = kStackDepth - sp;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       if (!hit[c] || c == best) continue;
-      if (sp < kStackDepth - 1) {
-        st.put(sp++, cref[c], tn[c]);
+      if (sp < SD + kSpill - 1) {
+        put(sp++, cref[c], tn[c]);
       } else {
         t_drop = fminf(t_drop, tn[c]);
       }
     }
-    (void)avail;
-    st.put(sp++, cref[best], best_t);
+    put(sp++, cref[best], best_t);
   }
 }
 
@@ -175,7 +189,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
 // lane-parallel (lane c ranks child c) and pushed far-to-near. Control flow
 // is warp-uniform, so SIMT efficiency equals the fraction of lanes whose ray
 // still needs the node, and every node/triangle record is read once per warp.
-constexpr int kWarpStack = 96;
+constexpr int kWarpStack = 192;
 
 struct WarpStack {
   uint32_t* ref;
@@ -186,9 +200,10 @@ struct WarpStack {
 // Sorted insert into the lane's k-buffer in shared memory (hits are rare
 // next to box tests, so the buffer need not occupy 32 registers); kb_last
 // mirrors the largest key.
+template <int K>
 __device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key,
                                                unsigned long long& kb_last) {
-  int i = kChunk - 1;
+  int i = K - 1;
   while (i > 0) {
     const unsigned long long prev = kb[(i - 1) * stride];
     if (prev <= key) break;
@@ -196,16 +211,17 @@ __device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int strid
     --i;
   }
   kb[i * stride] = key;
-  kb_last = kb[(kChunk - 1) * stride];
+  kb_last = kb[(K - 1) * stride];
 }
 
+template <int K>
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
                                              unsigned long long key_min, unsigned long long* kb, int kstride,
                                              WarpStack ws, float& t_drop, int* status, Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int i = 0; i < kChunk; ++i) kb[i * kstride] = kEmptyKey;
+  for (int i = 0; i < K; ++i) kb[i * kstride] = kEmptyKey;
   unsigned long long kb_last = kEmptyKey;
   t_drop = INFINITY;
   const unsigned act = __ballot_sync(full, want);
@@ -246,7 +262,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
         if (!(t >= t_lo) || !(t <= tmax)) continue;
         const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
         if (key >= key_min && key < kb_last) {
-          kb_insert_smem(kb, kstride, key, kb_last);
+          kb_insert_smem<K>(kb, kstride, key, kb_last);
           if (kb_last != kEmptyKey) tmax = key_t(kb_last);
         }
       }
@@ -499,13 +515,14 @@ struct Smem {
   int stride;
 };
 
+template <int SD>
 __device__ __forceinline__ Smem thread_smem() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem s;
   const int nt = blockDim.x;
   unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw);
   uint32_t* refs = reinterpret_cast<uint32_t*>(smem_raw + (size_t)kChunk * nt * 8);
-  float* tns = reinterpret_cast<float*>(refs + (size_t)kStackDepth * nt);
+  float* tns = reinterpret_cast<float*>(refs + (size_t)SD * nt);
   s.keys = keys + threadIdx.x;
   s.stride = nt;
   s.st.ref = refs + threadIdx.x;
@@ -532,24 +549,36 @@ __device__ __forceinline__ Cursor first_cursor(int tmin_inclusive) {
   return c;
 }
 
-// Visits the staged keys of one query in the reference's chunk order
-// (forward.cu:99-154) and calls sh.visit(prim) for each hit at or beyond the
-// near plane; visit returns true to end the ray (transmittance cut-off).
-// Returns true when the ray is finished, else leaves in `cur` where the next
-// query starts: after every 16th visited hit the reference re-traces from
-// last_hit_t (closed interval) or just after it (open); after a truncated
-// query (stack overflow) the stream resumes right after the last key taken.
-template <class Shader>
+// Visits the keys of one query (K keys, ascending, staged in shared memory)
+// in the reference's chunk order (forward.cu:99-154) and calls sh.visit(prim)
+// for each hit at or beyond the near plane; visit returns true to end the ray
+// (transmittance cut-off). Returns true when the ray is finished, else leaves
+// in `cur` where the next query starts.
+//
+// The reference re-traces after every 16th visited hit from last_hit_t
+// (closed interval: the hit(s) at last_hit_t come again) or just after it
+// (open). A query buffer holds EVERY key between its lower bound and its last
+// key, so the position "first key >= the new bound" is found inside the
+// buffer whenever the buffer reaches it, and only otherwise does the next
+// query start at that bound; after a full or truncated buffer the stream
+// resumes right after the last key taken. The query size K is therefore a
+// performance choice that never changes the visited sequence.
+template <int K, class Shader>
 __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Cursor& cur, int tmin_inclusive,
                                               int* status, Shader& sh) {
   const bool truncated = t_drop < INFINITY;
-  int consumed = 0;
+  auto trusted = [&](unsigned long long key) {
+    return key != kEmptyKey && !(truncated && key_t(key) >= t_drop);
+  };
   unsigned long long last_key = 0;
+  bool any = false;
+  int boundaries = 0;
   sh.prepare();
-  for (int i = 0; i < kChunk; ++i) {
+  int i = 0;
+  while (i < K) {
     const unsigned long long key = sm.keys[i * sm.stride];
-    if (key == kEmptyKey || (truncated && key_t(key) >= t_drop)) break;
-    ++consumed;
+    if (!trusted(key)) break;
+    any = true;
     last_key = key;
     const float t = key_t(key);
     // fmaxf(last + STEP_EPSILON, t) with the sum in double (forward.cu:111)
@@ -557,21 +586,46 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
     ++cur.ref_pos;
     if (t >= kNear && sh.visit(key_prim(key))) return true;
     if (cur.ref_pos == kChunk) {
+      // the reference's next optixTrace starts at last_hit_t
       cur.ref_pos = 0;
       const unsigned long long tb = __float_as_uint(cur.last_hit_t);
-      cur.key_min = tmin_inclusive ? (tb << 32) : ((tb + 1ull) << 32);
+      const unsigned long long bound = tmin_inclusive ? (tb << 32) : ((tb + 1ull) << 32);
+      if (++boundaries > K) {  // 16+ hits at one t under the closed interval: no progress
+        atomicOr(status, kStatusTimeout);
+        return true;
+      }
+      int j = 0;
+      while (j < K && trusted(sm.keys[j * sm.stride]) && sm.keys[j * sm.stride] < bound) ++j;
+      if (j < K && trusted(sm.keys[j * sm.stride])) {
+        i = j;  // continue inside the buffer
+        continue;
+      }
+      if (j < K && sm.keys[j * sm.stride] == kEmptyKey && !truncated) return true;  // stream exhausted
+      cur.key_min = bound;
       return false;
     }
+    ++i;
   }
-  if (truncated) {
-    if (consumed == 0) {
-      atomicOr(status, kStatusStack);
-      return true;
-    }
-    cur.key_min = last_key + 1ull;
-    return false;
+  if (i < K && sm.keys[i * sm.stride] == kEmptyKey && !truncated) return true;  // stream exhausted
+  if (!any) {
+    atomicOr(status, kStatusStack);  // a truncated query that trusted nothing
+    return true;
   }
-  return true;  // fewer than 16 hits left: the stream is exhausted
+  cur.key_min = last_key + 1ull;
+  return false;
+}
+
+// View holding global tile `tile` (views are stored in tile order).
+__device__ __forceinline__ int find_view(const TraceParams& p, int tile) {
+  int lo = 0, hi = p.nviews - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (p.views[mid].tile_begin <= tile)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 
 // Persistent warp driver. Each round: lanes without a ray take the next rays
@@ -579,8 +633,9 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
 // then every lane holding a ray runs its k-closest query, then every such lane
 // shades its chunk. Traversal and shading never mix inside a warp, and lanes
 // whose ray finished are refilled instead of idling.
-template <class Shader>
+template <int SD, class Shader>
 __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shader& sh, Counters& cnt) {
+  constexpr int K = kChunk;  // per-lane k-buffers live in registers
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -601,13 +656,15 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
           exhausted = true;
         } else {
           const int tile = slot >> 5, l = slot & 31;
-          const int px = (tile % p.ntx) * 8 + (l & 7), py = (tile / p.ntx) * 4 + (l >> 3);
-          if (px < p.W && py < p.H) {
-            const int pix = py * p.W + px;
-            o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
-            d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
+          const ViewDesc& v = p.views[find_view(p, tile)];
+          const int lt = tile - v.tile_begin;
+          const int px = (lt % v.ntx) * 8 + (l & 7), py = (lt / v.ntx) * 4 + (l >> 3);
+          if (px < v.W && py < v.H) {
+            const int pix = py * v.W + px;
+            o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
+            d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
             cur = first_cursor(p.tmin_inclusive);
-            if (sh.begin(pix, o, d))
+            if (sh.begin(&v, pix, o, d))
               have = true;
             else
               sh.end();
@@ -623,13 +680,13 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
     if (have) {
       const RayW r = make_ray(o, d);
       unsigned long long kb[kChunk];
-      query(p.bvh, r, cur.key_min, kb, sm.st, t_drop, p.status, cnt);
+      query<SD>(p.bvh, r, cur.key_min, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
       for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
     }
     __syncwarp();
     if (have) {
-      bool done = consume_chunk(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+      bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
       if (!done && ++cur.chunks >= kMaxChunks) {
         atomicOr(p.status, kStatusTimeout);
         done = true;
@@ -658,7 +715,7 @@ __device__ __forceinline__ WarpStack warp_stack(unsigned char* base) {
   return ws;
 }
 
-template <class Shader>
+template <int K, class Shader>
 __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& sm, WarpStack ws, Shader& sh,
                                               Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
@@ -668,22 +725,24 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
     if (lane == 0) tile = atomicAdd(p.work, 1);
     tile = __shfl_sync(full, tile, 0);
     if (tile >= p.ntiles) break;
-    const int px = (tile % p.ntx) * 8 + (lane & 7), py = (tile / p.ntx) * 4 + (lane >> 3);
-    bool active = px < p.W && py < p.H;
+    const ViewDesc& v = p.views[find_view(p, tile)];
+    const int lt = tile - v.tile_begin;
+    const int px = (lt % v.ntx) * 8 + (lane & 7), py = (lt / v.ntx) * 4 + (lane >> 3);
+    bool active = px < v.W && py < v.H;
     float3 o = make_float3(0.f, 0.f, 1.f), d = make_float3(0.f, 0.f, 1.f);
     Cursor cur = first_cursor(p.tmin_inclusive);
     if (active) {
-      const int pix = py * p.W + px;
-      o = make_float3(p.ray_o[3 * pix], p.ray_o[3 * pix + 1], p.ray_o[3 * pix + 2]);
-      d = make_float3(p.ray_d[3 * pix], p.ray_d[3 * pix + 1], p.ray_d[3 * pix + 2]);
-      sh.begin(pix, o, d);  // the plain shaders always trace their one ray
+      const int pix = py * v.W + px;
+      o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
+      d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
+      sh.begin(&v, pix, o, d);  // the plain shaders always trace their one ray
     }
     const RayW r = make_ray(o, d);
     while (__any_sync(full, active)) {
       float t_drop;
-      packet_query(p.bvh, r, active, cur.key_min, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+      packet_query<K>(p.bvh, r, active, cur.key_min, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
       if (active) {
-        bool done = consume_chunk(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+        bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
         if (!done && ++cur.chunks >= kMaxChunks) {
           atomicOr(p.status, kStatusTimeout);
           done = true;
@@ -697,6 +756,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
   }
 }
 
+template <int K>
 __device__ __forceinline__ Smem packet_smem(unsigned char*& rest) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem s;
@@ -705,8 +765,53 @@ __device__ __forceinline__ Smem packet_smem(unsigned char*& rest) {
   s.st.ref = nullptr;
   s.st.tn = nullptr;
   s.st.stride = 0;
-  rest = smem_raw + (size_t)kChunk * blockDim.x * 8;
+  rest = smem_raw + (size_t)K * blockDim.x * 8;
   return s;
+}
+
+// Traversal configurations the kernels are instantiated for (the autotuner
+// picks one per workload): warp packets with 16 or 32 hits per query, or
+// independent lanes with a 32- or 24-entry stack per ray.
+template <int CFG>
+struct TraversalCfg;
+template <>
+struct TraversalCfg<kCfgLanes32> {
+  static constexpr bool packets = false;
+  static constexpr int K = 16, SD = 32;
+};
+template <>
+struct TraversalCfg<kCfgPackets16> {
+  static constexpr bool packets = true;
+  static constexpr int K = 16, SD = 0;
+};
+template <>
+struct TraversalCfg<kCfgPackets32> {
+  static constexpr bool packets = true;
+  static constexpr int K = 32, SD = 0;
+};
+template <>
+struct TraversalCfg<kCfgLanes24> {
+  static constexpr bool packets = false;
+  static constexpr int K = 16, SD = 24;
+};
+
+template <int CFG>
+constexpr size_t smem_bytes_for() {
+  using C = TraversalCfg<CFG>;
+  return C::packets ? (size_t)kTraceThreads * C::K * 8 + (size_t)(kTraceThreads / 32) * kWarpStack * 12
+                    : (size_t)kTraceThreads * (C::SD * 8 + kChunk * 8);
+}
+
+template <int CFG, class Shader>
+__device__ __forceinline__ void run(const TraceParams& p, Shader& sh, Counters& cnt) {
+  using C = TraversalCfg<CFG>;
+  if constexpr (C::packets) {
+    unsigned char* rest;
+    const Smem sm = packet_smem<C::K>(rest);
+    drive_packets<C::K>(p, sm, warp_stack(rest), sh, cnt);
+  } else {
+    drive<C::SD>(p, thread_smem<C::SD>(), sh, cnt);
+  }
 }
 
 // ---------------------------------------------------------------- forward
@@ -723,6 +828,7 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned ra
 // forward.cu:109-152 per hit and :204-214 per ray.
 struct FwdShader {
   const TraceParams& p;
+  const ViewDesc* v;
   int pix;
   float3 o, d;
   float C0, C1, C2, N0, N1, N2, T;
@@ -730,7 +836,8 @@ struct FwdShader {
 
   __device__ explicit FwdShader(const TraceParams& params) : p(params) {}
 
-  __device__ __forceinline__ bool begin(int pixel, float3 ro, float3 rd) {
+  __device__ __forceinline__ bool begin(const ViewDesc* view, int pixel, float3 ro, float3 rd) {
+    v = view;
     pix = pixel;
     o = ro;
     d = rd;
@@ -771,31 +878,25 @@ struct FwdShader {
   }
 
   __device__ __forceinline__ void end() {
-    const int HW = p.H * p.W;
-    p.out_color[pix] = C0 + T * p.bg[0];
-    p.out_color[HW + pix] = C1 + T * p.bg[1];
-    p.out_color[2 * HW + pix] = C2 + T * p.bg[2];
-    p.out_others[kDepthCh * HW + pix] = 0.0f;  // the reference never accumulates depth
-    p.out_others[kAlphaCh * HW + pix] = 1.0f - T;
-    p.out_others[(kNormalCh + 0) * HW + pix] = N0;
-    p.out_others[(kNormalCh + 1) * HW + pix] = N1;
-    p.out_others[(kNormalCh + 2) * HW + pix] = N2;
-    p.out_others[kMidDepthCh * HW + pix] = 0.0f;
-    p.out_others[kDistortionCh * HW + pix] = 0.0f;
+    const int HW = v->H * v->W;
+    v->out_color[pix] = C0 + T * p.bg[0];
+    v->out_color[HW + pix] = C1 + T * p.bg[1];
+    v->out_color[2 * HW + pix] = C2 + T * p.bg[2];
+    v->out_others[kDepthCh * HW + pix] = 0.0f;  // the reference never accumulates depth
+    v->out_others[kAlphaCh * HW + pix] = 1.0f - T;
+    v->out_others[(kNormalCh + 0) * HW + pix] = N0;
+    v->out_others[(kNormalCh + 1) * HW + pix] = N1;
+    v->out_others[(kNormalCh + 2) * HW + pix] = N2;
+    v->out_others[kMidDepthCh * HW + pix] = 0.0f;
+    v->out_others[kDistortionCh * HW + pix] = 0.0f;
   }
 };
 
-template <int kPackets>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(TraceParams p) {
+template <int CFG>
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
   Counters cnt;
   FwdShader sh(p);
-  if (kPackets) {
-    unsigned char* rest;
-    const Smem sm = packet_smem(rest);
-    drive_packets(p, sm, warp_stack(rest), sh, cnt);
-  } else {
-    drive(p, thread_smem(), sh, cnt);
-  }
+  run<CFG>(p, sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
@@ -879,6 +980,7 @@ __device__ __forceinline__ float3 cosine_hemisphere(uint32_t& seed, float3 n) {
 
 struct VarShader {
   const TraceParams& p;
+  const ViewDesc* v;
   int pix;
   float3 o, d;
   float C0, C1, C2, T;
@@ -899,7 +1001,8 @@ struct VarShader {
     ro = vf::add(so, vf::scale(rd, (float)kStepEps));
   }
 
-  __device__ __forceinline__ bool begin(int pixel, float3& ro, float3& rd) {
+  __device__ __forceinline__ bool begin(const ViewDesc* view, int pixel, float3& ro, float3& rd) {
+    v = view;
     pix = pixel;
     C0 = C1 = C2 = 0.f;
     T = 1.0f;
@@ -978,7 +1081,7 @@ struct VarShader {
   }
 
   __device__ __forceinline__ void end() {
-    const int HW = p.H * p.W;
+    const int HW = v->H * v->W;
     if (env) {  // mean sample radiance; transmittance 0
       const float inv = 1.0f / (float)p.samples;
       C0 = A0 * inv;
@@ -986,18 +1089,18 @@ struct VarShader {
       C2 = A2 * inv;
       T = 0.0f;
     }
-    p.out_color[pix] = C0 + T * p.bg[0];
-    p.out_color[HW + pix] = C1 + T * p.bg[1];
-    p.out_color[2 * HW + pix] = C2 + T * p.bg[2];
+    v->out_color[pix] = C0 + T * p.bg[0];
+    v->out_color[HW + pix] = C1 + T * p.bg[1];
+    v->out_color[2 * HW + pix] = C2 + T * p.bg[2];
 #pragma unroll
-    for (int c = 0; c < 7; ++c) p.out_others[c * HW + pix] = 0.0f;  // variants write colour only
+    for (int c = 0; c < 7; ++c) v->out_others[c * HW + pix] = 0.0f;  // variants write colour only
   }
 };
 
-__global__ void __launch_bounds__(kTraceThreads, 4) k_variant(TraceParams p) {
+__global__ void __launch_bounds__(kTraceThreads, 4) k_variant(const __grid_constant__ TraceParams p) {
   Counters cnt;
   VarShader sh(p);
-  drive(p, thread_smem(), sh, cnt);
+  drive<32>(p, thread_smem<32>(), sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
@@ -1047,6 +1150,7 @@ __device__ __forceinline__ void window_bwd(const Geom& g, float dL_dphi, float3 
 // hit, dL/dalpha from the final values, scattered gradients.
 struct BwdShader {
   const TraceParams& p;
+  const ViewDesc* v;
   int pix;
   float3 o, d;
   // per-ray finals and upstream gradients, loaded for each chunk (so they do
@@ -1057,7 +1161,8 @@ struct BwdShader {
 
   __device__ explicit BwdShader(const TraceParams& params) : p(params) {}
 
-  __device__ __forceinline__ bool begin(int pixel, float3 ro, float3 rd) {
+  __device__ __forceinline__ bool begin(const ViewDesc* view, int pixel, float3 ro, float3 rd) {
+    v = view;
     pix = pixel;
     o = ro;
     d = rd;
@@ -1069,21 +1174,21 @@ struct BwdShader {
   __device__ __forceinline__ bool next(float3&, float3&) { return false; }
 
   __device__ __forceinline__ void prepare() {
-    const int HW = p.H * p.W;
-    Cf0 = __ldg(p.colors + pix);
-    Cf1 = __ldg(p.colors + HW + pix);
-    Cf2 = __ldg(p.colors + 2 * HW + pix);
-    Df = __ldg(p.others + kDepthCh * HW + pix);
-    Nf0 = __ldg(p.others + (kNormalCh + 0) * HW + pix);
-    Nf1 = __ldg(p.others + (kNormalCh + 1) * HW + pix);
-    Nf2 = __ldg(p.others + (kNormalCh + 2) * HW + pix);
-    g0 = __ldg(p.dL_dpix + pix);
-    g1 = __ldg(p.dL_dpix + HW + pix);
-    g2 = __ldg(p.dL_dpix + 2 * HW + pix);
-    gD = __ldg(p.dL_doth + kDepthCh * HW + pix);
-    gN0 = __ldg(p.dL_doth + (kNormalCh + 0) * HW + pix);
-    gN1 = __ldg(p.dL_doth + (kNormalCh + 1) * HW + pix);
-    gN2 = __ldg(p.dL_doth + (kNormalCh + 2) * HW + pix);
+    const int HW = v->H * v->W;
+    Cf0 = __ldg(v->colors + pix);
+    Cf1 = __ldg(v->colors + HW + pix);
+    Cf2 = __ldg(v->colors + 2 * HW + pix);
+    Df = __ldg(v->others + kDepthCh * HW + pix);
+    Nf0 = __ldg(v->others + (kNormalCh + 0) * HW + pix);
+    Nf1 = __ldg(v->others + (kNormalCh + 1) * HW + pix);
+    Nf2 = __ldg(v->others + (kNormalCh + 2) * HW + pix);
+    g0 = __ldg(v->dL_dpix + pix);
+    g1 = __ldg(v->dL_dpix + HW + pix);
+    g2 = __ldg(v->dL_dpix + 2 * HW + pix);
+    gD = __ldg(v->dL_doth + kDepthCh * HW + pix);
+    gN0 = __ldg(v->dL_doth + (kNormalCh + 0) * HW + pix);
+    gN1 = __ldg(v->dL_doth + (kNormalCh + 1) * HW + pix);
+    gN2 = __ldg(v->dL_doth + (kNormalCh + 2) * HW + pix);
   }
 
   __device__ __forceinline__ bool visit(uint32_t prim) {
@@ -1159,22 +1264,16 @@ struct BwdShader {
   __device__ __forceinline__ void end() {}
 };
 
-template <int kPackets>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(TraceParams p) {
+template <int CFG>
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
   Counters cnt;
   BwdShader sh(p);
-  if (kPackets) {
-    unsigned char* rest;
-    const Smem sm = packet_smem(rest);
-    drive_packets(p, sm, warp_stack(rest), sh, cnt);
-  } else {
-    drive(p, thread_smem(), sh, cnt);
-  }
+  run<CFG>(p, sh, cnt);
 }
 
 // ---------------------------------------------------------------- hit stream
 __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p) {
-  const Stack st = thread_smem().st;
+  const Stack st = thread_smem<kStackDepth>().st;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.R) return;
   const float3 o = make_float3(p.ray_o[3 * i], p.ray_o[3 * i + 1], p.ray_o[3 * i + 2]);
@@ -1186,7 +1285,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
     Counters cnt;
-    query(p.bvh, r, key_min, kb, st, t_drop, p.status, cnt);
+    query<kStackDepth>(p.bvh, r, key_min, kb, st, t_drop, p.status, cnt);
     int consumed = 0;
     unsigned long long last = 0;
 #pragma unroll
@@ -1213,42 +1312,66 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
 
 }  // namespace
 
-size_t trace_smem_bytes(int packets) {
-  if (packets) return (size_t)kTraceThreads * kChunk * 8 + (size_t)(kTraceThreads / 32) * kWarpStack * 12;
-  return (size_t)kTraceThreads * (kStackDepth * 8 + kChunk * 8);
+size_t trace_smem_bytes(int cfg) {
+  switch (cfg) {
+    case kCfgPackets16: return smem_bytes_for<kCfgPackets16>();
+    case kCfgPackets32: return smem_bytes_for<kCfgPackets32>();
+    case kCfgLanes24: return smem_bytes_for<kCfgLanes24>();
+    default: return smem_bytes_for<kCfgLanes32>();
+  }
 }
 
-int trace_blocks_per_sm(int which, int packets) {
+namespace {
+template <int CFG>
+const void* fwd_fn() { return (const void*)k_forward<CFG>; }
+template <int CFG>
+const void* bwd_fn() { return (const void*)k_backward<CFG>; }
+const void* kernel_for(int which, int cfg) {
+  switch (cfg) {
+    case kCfgPackets16: return which == 0 ? fwd_fn<kCfgPackets16>() : bwd_fn<kCfgPackets16>();
+    case kCfgPackets32: return which == 0 ? fwd_fn<kCfgPackets32>() : bwd_fn<kCfgPackets32>();
+    case kCfgLanes24: return which == 0 ? fwd_fn<kCfgLanes24>() : bwd_fn<kCfgLanes24>();
+    default: return which == 0 ? fwd_fn<kCfgLanes32>() : bwd_fn<kCfgLanes32>();
+  }
+}
+}  // namespace
+
+int trace_blocks_per_sm(int which, int cfg) {
   int n = 0;
-  const void* fn = which == 0 ? (packets ? (const void*)k_forward<1> : (const void*)k_forward<0>)
-                              : (packets ? (const void*)k_backward<1> : (const void*)k_backward<0>);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, trace_smem_bytes(packets)) != cudaSuccess)
-    n = 1;
+  const void* fn = which == 2 ? (const void*)k_variant : kernel_for(which, cfg);
+  const size_t smem = which == 2 ? smem_bytes_for<kCfgLanes32>() : trace_smem_bytes(cfg);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem) != cudaSuccess) n = 1;
   return n > 0 ? n : 1;
 }
 
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {
-  if (p.variant != 0)
-    k_variant<<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
-  else if (p.packets)
-    k_forward<1><<<grid, kTraceThreads, trace_smem_bytes(1), s>>>(p);
-  else
-    k_forward<0><<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
+  if (p.variant != 0) {
+    k_variant<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
+    return cudaGetLastError();
+  }
+  switch (p.cfg) {
+    case kCfgPackets16: k_forward<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_forward<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_forward<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_forward<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
-  if (p.packets)
-    k_backward<1><<<grid, kTraceThreads, trace_smem_bytes(1), s>>>(p);
-  else
-    k_backward<0><<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
+  switch (p.cfg) {
+    case kCfgPackets16: k_backward<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_backward<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_backward<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_backward<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s) {
   const int grid = (p.R + kTraceThreads - 1) / kTraceThreads;
   if (grid == 0) return cudaSuccess;
-  k_hit_stream<<<grid, kTraceThreads, trace_smem_bytes(0), s>>>(p);
+  k_hit_stream<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
   return cudaGetLastError();
 }
 

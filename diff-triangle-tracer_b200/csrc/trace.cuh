@@ -6,12 +6,27 @@
 
 namespace tt {
 
-struct TraceParams {
-  BvhView bvh;
-  int H, W;
-  int ntx, ntiles;  // 8x4 pixel tiles
+// One camera image: its rays ([H][W][3]) and per-pixel outputs/inputs
+// (channel-major [C][H][W]). Tiles are 8x4 pixels; tile_begin is the view's
+// first tile in the launch's global tile numbering.
+constexpr int kMaxViews = 32;
+struct ViewDesc {
   const float* ray_o;
   const float* ray_d;
+  float* out_color;
+  float* out_others;
+  const float* colors;   // adjoint: forward colour
+  const float* others;   // adjoint: forward side outputs
+  const float* dL_dpix;  // adjoint: upstream gradients
+  const float* dL_doth;
+  int H, W, ntx, tile_begin;
+};
+
+struct TraceParams {
+  BvhView bvh;
+  int nviews;
+  int ntiles;  // tiles over all views
+  ViewDesc views[kMaxViews];
   const float* verts;
   const int* cumsum;
   const int* num_points;
@@ -20,17 +35,11 @@ struct TraceParams {
   const float* opac;
   const float* sigma;
   const float* bg;
-  // forward outputs
+  // per-triangle forward outputs
   float* scaling;
   float* density;
   float* max_blending;
-  float* out_color;
-  float* out_others;
-  // adjoint inputs/outputs
-  const float* colors;
-  const float* others;
-  const float* dL_dpix;
-  const float* dL_doth;
+  // adjoint outputs
   float* d_tri;
   float* d_sigma;
   float* d_opac;
@@ -40,7 +49,7 @@ struct TraceParams {
   float sph_r, sph_cx, sph_cy, sph_cz;
   int samples;
   int tmin_inclusive;
-  int packets;  // 1: warp packet traversal (coherent rays), 0: one independent ray per lane
+  int cfg;      // traversal configuration, kCfg*
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward: rays, evaluated hits, blended hits, node visits, triangle tests, queries
@@ -60,10 +69,16 @@ struct HitStreamParams {
 
 constexpr int kTraceThreads = 128;
 constexpr int kStackDepth = 32;
+// traversal configurations (see trace.cu)
+constexpr int kCfgLanes32 = 0;    // one ray per lane, 32-entry stack, 16 hits per query
+constexpr int kCfgPackets16 = 1;  // warp packets of 8x4 pixels, 16 hits per query
+constexpr int kCfgPackets32 = 2;  // warp packets, 32 hits per query
+constexpr int kCfgLanes24 = 3;    // one ray per lane, 24-entry stack
+constexpr int kNumCfgs = 4;
 
-size_t trace_smem_bytes(int packets);
-// Resident blocks per SM of the forward / adjoint kernels (occupancy query).
-int trace_blocks_per_sm(int which /*0 forward, 1 adjoint*/, int packets);
+size_t trace_smem_bytes(int cfg);
+// Resident blocks per SM of the forward / adjoint / variant kernels.
+int trace_blocks_per_sm(int which /*0 forward, 1 adjoint, 2 variant*/, int cfg);
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);

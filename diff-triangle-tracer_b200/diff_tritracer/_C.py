@@ -212,6 +212,113 @@ class OptixTracer:
         return BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
 
     # ------------------------------------------------------------------
+    def set_traversal(self, traversal: str = "auto", k: int = 16, stack_depth: int = 32):
+        """Switches the traversal configuration (the BVH is kept)."""
+        modes = {"auto": _lib.TT_TRAVERSAL_AUTO, "packets": _lib.TT_TRAVERSAL_PACKETS, "lanes": _lib.TT_TRAVERSAL_LANES}
+        check(self._h, lib.tt_set_traversal(self._h, modes[traversal], int(k), int(stack_depth)))
+
+    def _scene_fwd_args(self, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,
+                        number_of_points, shs, sh_degree, opacities, scaling, density_factor, bg_color,
+                        rebuild_gas_opt, max_blending):
+        dev = self.device
+        verts = _f32(triangles_points, "triangles_points", dev)
+        sig = _f32(sigma, "sigma", dev)
+        npts = _i32(num_points_per_triangle, "num_points_per_triangle", dev)
+        cums = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        sh = _f32(shs, "shs", dev)
+        opac = _f32(opacities, "opacities", dev)
+        bg = _f32(bg_color, "bg_color", dev)
+        if not (scaling.is_contiguous() and density_factor.is_contiguous()):
+            raise RuntimeError("scaling and density_factor must be contiguous for batched calls")
+        a = _lib.TtFwdArgs()
+        a.vertices, a.num_vertices = _ptr(verts), verts.numel() // 3
+        a.num_points, a.cumsum, a.P = _ptr(npts), _ptr(cums), int(number_of_points)
+        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), int(sh.shape[1]) if sh.dim() >= 2 and sh.shape[0] else 0
+        a.opacities, a.sigma = _ptr(opac), _ptr(sig)
+        a.scaling, a.density_factor = _ptr(scaling), _ptr(density_factor)
+        a.bg = _ptr(bg)
+        a.rebuild_gas = int(rebuild_gas_opt)
+        a.max_blending = _ptr(max_blending)
+        a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        return a, (verts, sig, npts, cums, sh, opac, bg)
+
+    def trace_forward_views(self, rays, triangles_points, sigma, num_points_per_triangle,
+                            cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities, scaling,
+                            density_factor, bg_color, rebuild_gas_opt, outputs=None, max_blending=None):
+        """Forward over up to 32 views of any resolutions in one launch.
+        rays: list of (ray_o, ray_d), each [H, W, 3]. Returns ([(color, others)], max_blending)."""
+        dev = self.device
+        P = int(number_of_points)
+        if max_blending is None:
+            max_blending = torch.empty((P,), dtype=torch.float32, device=dev)
+        a, keep = self._scene_fwd_args(triangles_points, sigma, num_points_per_triangle,
+                                       cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities,
+                                       scaling, density_factor, bg_color, rebuild_gas_opt, max_blending)
+        vs = (_lib.TtView * len(rays))()
+        outs = []
+        for i, (ro, rd) in enumerate(rays):
+            ro = _f32(ro, "ray_o", dev)
+            rd = _f32(rd, "ray_d", dev)
+            H, W = int(ro.shape[0]), int(ro.shape[1])
+            if outputs is None:
+                col = torch.empty((3, H, W), dtype=torch.float32, device=dev)
+                oth = torch.empty((7, H, W), dtype=torch.float32, device=dev)
+            else:
+                col, oth = outputs[i]
+            vs[i].H, vs[i].W = H, W
+            vs[i].ray_o, vs[i].ray_d = _ptr(ro), _ptr(rd)
+            vs[i].out_color, vs[i].out_others = _ptr(col), _ptr(oth)
+            outs.append((col, oth))
+            keep = keep + (ro, rd)
+        check(self._h, lib.tt_forward_views(self._h, ctypes.byref(a), vs, len(rays), _stream()))
+        self._keep = keep
+        return outs, max_blending
+
+    def trace_backward_views(self, rays, forward_outputs, upstream, triangles_points, sigma,
+                             num_points_per_triangle, cumsum_of_points_per_triangle, number_of_points, shs,
+                             sh_degree, opacities, bg_color, grads=None):
+        """Adjoint over the views of trace_forward_views. upstream: list of
+        (dL_dpixels [3,H,W], dL_dothers [7,H,W]). Returns (dL_dtriangle, dL_dsigma,
+        dL_dopacity, dL_dsh) summed over the views."""
+        dev = self.device
+        P = int(number_of_points)
+        verts = _f32(triangles_points, "triangles_points", dev)
+        sig = _f32(sigma, "sigma", dev)
+        npts = _i32(num_points_per_triangle, "num_points_per_triangle", dev)
+        cums = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        sh = _f32(shs, "shs", dev)
+        M = int(sh.shape[1]) if sh.dim() >= 2 and sh.shape[0] != 0 else 0
+        opac = _f32(opacities, "opacities", dev)
+        bg = _f32(bg_color, "bg_color", dev)
+        V = verts.numel() // 3
+        if grads is None:
+            grads = (torch.empty((V, 3), dtype=torch.float32, device=dev),
+                     torch.empty_like(sigma, memory_format=torch.contiguous_format),
+                     torch.empty_like(opacities, memory_format=torch.contiguous_format),
+                     torch.empty((P, M, 3), dtype=torch.float32, device=dev))
+        a = _lib.TtBwdArgs()
+        a.bg = _ptr(bg)
+        a.vertices, a.num_vertices = _ptr(verts), V
+        a.sigma, a.num_points, a.cumsum, a.P = _ptr(sig), _ptr(npts), _ptr(cums), P
+        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
+        a.opacities = _ptr(opac)
+        a.dL_dtriangle, a.dL_dsigma, a.dL_dopacity, a.dL_dsh = [_ptr(g) for g in grads]
+        a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        vs = (_lib.TtView * len(rays))()
+        keep = (verts, sig, npts, cums, sh, opac, bg)
+        for i, ((ro, rd), (col, oth), (g, go)) in enumerate(zip(rays, forward_outputs, upstream)):
+            ro, rd = _f32(ro, "ray_o", dev), _f32(rd, "ray_d", dev)
+            col, oth = _f32(col, "colors", dev), _f32(oth, "others", dev)
+            g, go = _f32(g, "dL_dpixels", dev), _f32(go, "dL_dothers", dev)
+            vs[i].H, vs[i].W = int(ro.shape[0]), int(ro.shape[1])
+            vs[i].ray_o, vs[i].ray_d = _ptr(ro), _ptr(rd)
+            vs[i].colors, vs[i].others = _ptr(col), _ptr(oth)
+            vs[i].dL_dpixels, vs[i].dL_dothers = _ptr(g), _ptr(go)
+            keep = keep + (ro, rd, col, oth, g, go)
+        check(self._h, lib.tt_backward_views(self._h, ctypes.byref(a), vs, len(rays), _stream()))
+        self._keep = keep
+        return grads
+
     def device_status(self):
         """Synchronises and raises if a bounded device loop gave up since the
         last check (no reference counterpart)."""

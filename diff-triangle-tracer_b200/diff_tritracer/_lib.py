@@ -36,7 +36,7 @@ _vp = ctypes.c_void_p
 
 class TtConfig(ctypes.Structure):
     _fields_ = [("variant", ctypes.c_int), ("tmin_inclusive", ctypes.c_int), ("traversal", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("k", ctypes.c_int), ("stack_depth", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class TtFwdArgs(ctypes.Structure):
@@ -70,6 +70,12 @@ class TtBwdArgs(ctypes.Structure):
     ]
 
 
+class TtView(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_int), ("W", ctypes.c_int), ("ray_o", _vp), ("ray_d", _vp),
+                ("out_color", _vp), ("out_others", _vp), ("colors", _vp), ("others", _vp),
+                ("dL_dpixels", _vp), ("dL_dothers", _vp)]
+
+
 class TtStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
                 ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
@@ -79,7 +85,8 @@ class TtStats(ctypes.Structure):
 
 EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
-    "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats",
+    "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
+    "tt_backward_views", "tt_set_traversal",
 )
 
 
@@ -97,6 +104,9 @@ def _load():
     lib.tt_last_error.argtypes = [_vp]
     lib.tt_last_error.restype = ctypes.c_char_p
     lib.tt_device_status.argtypes = [_vp, _vp]
+    lib.tt_forward_views.argtypes = [_vp, ctypes.POINTER(TtFwdArgs), ctypes.POINTER(TtView), ctypes.c_int, _vp]
+    lib.tt_backward_views.argtypes = [_vp, ctypes.POINTER(TtBwdArgs), ctypes.POINTER(TtView), ctypes.c_int, _vp]
+    lib.tt_set_traversal.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.tt_get_stats.argtypes = [_vp, ctypes.POINTER(TtStats), _vp]
     lib.tt_reset_stats.argtypes = [_vp, _vp]
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]

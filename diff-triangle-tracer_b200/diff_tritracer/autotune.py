@@ -1,0 +1,67 @@
+"""Autotuner of the traversal configuration: rays per warp (one 8x4-pixel
+packet per warp, or one independent ray per lane), hits gathered per traversal
+k (16 or 32) and the per-lane stack depth (32 or 24).
+
+`autotune(tracer, step)` times `step()` (a callable running the workload on
+`tracer`, e.g. ViewBatch.step or a forward+backward pass) under every
+configuration with CUDA events, keeps the fastest on the tracer and caches it
+in a JSON file keyed by GPU name and workload. Every configuration produces the
+same results (the visited hit sequence does not depend on them), so tuning
+never changes outputs.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+
+import torch
+
+CANDIDATES = (
+    {"traversal": "packets", "k": 16, "stack_depth": 0},
+    {"traversal": "packets", "k": 32, "stack_depth": 0},
+    {"traversal": "lanes", "k": 16, "stack_depth": 32},
+    {"traversal": "lanes", "k": 16, "stack_depth": 24},
+)
+
+DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "diff_tritracer", "autotune.json")
+
+
+def _load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int = 3, force: bool = False):
+    """Returns the chosen configuration (dict) and applies it to `tracer`."""
+    full_key = f"{torch.cuda.get_device_name(tracer.device)}|{key}"
+    cache = _load(cache_path)
+    if not force and full_key in cache:
+        best = cache[full_key]
+        tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
+        return best
+    timings = []
+    for cand in CANDIDATES:
+        tracer.set_traversal(cand["traversal"], cand["k"], cand["stack_depth"])
+        step()  # warm-up
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(iters):
+            step()
+        end.record()
+        torch.cuda.synchronize()
+        timings.append((start.elapsed_time(end) / iters, cand))
+    ms, best = min(timings, key=lambda x: x[0])
+    best = dict(best, ms=ms, all={f"{c['traversal']}/k{c['k']}/s{c['stack_depth']}": t for t, c in timings})
+    tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
+    cache[full_key] = best
+    os.makedirs(os.path.dirname(cache_path), exist_ok=True)
+    tmp = cache_path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(cache, f, indent=1)
+    os.replace(tmp, cache_path)
+    return best

@@ -1,0 +1,85 @@
+"""Batched camera views of uneven resolution, captured in a CUDA graph.
+
+`ViewBatch` traces a fixed set of views (each its own [H, W] image, up to 32)
+through ONE persistent forward launch and ONE adjoint launch per step
+(tt_forward_views / tt_backward_views). With `graph=True` the step - BVH refit
+to the current vertices, forward, adjoint - is recorded once into a CUDA graph
+and replayed, so a training step costs one graph launch on the host. Rays and
+upstream gradients are copied into the batch's static buffers before replay;
+the scene tensors must keep their storage between steps (optimisers update
+them in place).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from ._C import OptixTracer
+
+
+class ViewBatch:
+    def __init__(self, tracer: OptixTracer, shapes, scene: dict, sh_degree: int, bg: torch.Tensor,
+                 graph: bool = True):
+        """shapes: [(H, W)] per view. scene: dict with triangles_points, sigma,
+        num_points_per_triangle, cumsum_of_points_per_triangle, number_of_points,
+        shs, opacities, scaling, density_factor (device tensors)."""
+        if not 1 <= len(shapes) <= 32:
+            raise RuntimeError("a batch holds 1 to 32 views")
+        self.tracer = tracer
+        self.scene = scene
+        self.sh_degree = sh_degree
+        self.bg = bg
+        dev = tracer.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.rays = [(torch.zeros((H, W, 3), **f32), torch.zeros((H, W, 3), **f32)) for H, W in shapes]
+        self.outputs = [(torch.zeros((3, H, W), **f32), torch.zeros((7, H, W), **f32)) for H, W in shapes]
+        self.upstream = [(torch.zeros((3, H, W), **f32), torch.zeros((7, H, W), **f32)) for H, W in shapes]
+        P = int(scene["number_of_points"])
+        self.max_blending = torch.zeros((P,), **f32)
+        V = scene["triangles_points"].numel() // 3
+        M = scene["shs"].shape[1]
+        self.grads = (torch.zeros((V, 3), **f32), torch.zeros_like(scene["sigma"]),
+                      torch.zeros_like(scene["opacities"]), torch.zeros((P, M, 3), **f32))
+        self.graph = None
+        # the first pass builds the BVH outside any capture
+        self._forward(0)
+        self._backward()
+        torch.cuda.synchronize()
+        if graph:
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._forward(1)
+                self._backward()
+
+    def _forward(self, rebuild_gas):
+        s = self.scene
+        self.tracer.trace_forward_views(self.rays, s["triangles_points"], s["sigma"], s["num_points_per_triangle"],
+                                        s["cumsum_of_points_per_triangle"], s["number_of_points"], s["shs"],
+                                        self.sh_degree, s["opacities"], s["scaling"], s["density_factor"], self.bg,
+                                        rebuild_gas, outputs=self.outputs, max_blending=self.max_blending)
+
+    def _backward(self):
+        s = self.scene
+        self.tracer.trace_backward_views(self.rays, self.outputs, self.upstream, s["triangles_points"], s["sigma"],
+                                         s["num_points_per_triangle"], s["cumsum_of_points_per_triangle"],
+                                         s["number_of_points"], s["shs"], self.sh_degree, s["opacities"], self.bg,
+                                         grads=self.grads)
+
+    def set_rays(self, rays):
+        for (ro, rd), (so, sd) in zip(rays, self.rays):
+            so.copy_(ro, non_blocking=True)
+            sd.copy_(rd, non_blocking=True)
+
+    def set_upstream(self, upstream):
+        for (g, go), (sg, sgo) in zip(upstream, self.upstream):
+            sg.copy_(g, non_blocking=True)
+            sgo.copy_(go, non_blocking=True)
+
+    def step(self):
+        """Refit + forward + adjoint over all views; results in .outputs,
+        .max_blending and .grads."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._forward(1)
+            self._backward()

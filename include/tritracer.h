@@ -65,7 +65,10 @@ typedef struct tt_config {
   int tmin_inclusive; /* 1 (default): each re-trace starts AT the last hit's t,
                          the closed interval of optixTrace; 0: strictly after */
   int traversal;      /* TT_TRAVERSAL_* */
-  int reserved[5];    /* zero */
+  int k;              /* hits gathered per traversal: 16 (0 = default) or 32 (packets
+                         only); compositing keeps the reference's 16-hit chunks */
+  int stack_depth;    /* per-lane traversal stack: 32 (0 = default) or 24 (lanes only) */
+  int reserved[3];    /* zero */
 } tt_config;
 
 /* Arguments of the forward trace: OptixTracer::trace_fwd
@@ -129,6 +132,22 @@ typedef struct tt_bwd_args {
   float* gpu_time_ms;  /* host pointer, may be NULL */
 } tt_bwd_args;
 
+/* One camera image of a batched call: rays [H][W][3]; the forward writes
+ * out_color [3][H][W] / out_others [7][H][W]; the adjoint reads colors /
+ * others (forward outputs) and dL_dpixels / dL_dothers. Pointers a call does
+ * not use may be NULL. */
+typedef struct tt_view {
+  int H, W;
+  const float* ray_o;
+  const float* ray_d;
+  float* out_color;
+  float* out_others;
+  const float* colors;
+  const float* others;
+  const float* dL_dpixels;
+  const float* dL_dothers;
+} tt_view;
+
 /* OptixTracer::OptixTracer (tritracer/pipeline.cpp:267-302). `cfg` may be
  * NULL for the defaults. Uses the CUDA device current at the call. */
 int tt_create(const tt_config* cfg, tt_tracer** out);
@@ -149,6 +168,20 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream);
 /* OptixTracer::trace_bwd (tritracer/tracer.cpp:144-228). Re-traces with the
  * structure of the last forward/build call. */
 int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream);
+
+/* Batched forms of tt_forward / tt_backward, no reference counterpart (the
+ * reference traces one [H, W] image per call): up to 32 views of uneven
+ * resolution go through ONE persistent launch; the per-view fields of `a`
+ * (H, W, ray and image pointers) are ignored, the per-triangle outputs
+ * (scaling, density_factor, max_blending; gradients) accumulate over all
+ * views. The view list travels in the kernel's parameters, so the call can be
+ * captured in a CUDA graph (plain variant, debug = 0). */
+int tt_forward_views(tt_tracer* h, const tt_fwd_args* a, const tt_view* views, int n_views, void* stream);
+int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, int n_views, void* stream);
+
+/* Switches the traversal configuration of a live handle (the BVH is kept);
+ * used by the autotuner. No reference counterpart. */
+int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
 
 /* Message of the last failed call on this handle (never NULL). */
 const char* tt_last_error(const tt_tracer* h);
