@@ -38,7 +38,20 @@ WORKLOADS = {
     "c1_100k_1x400": (100_000, 1, 400, 400),
     # one view of the 1M scene: the profiling case (inputs still larger than L2)
     "c2_1M_1x800": (1_000_000, 1, 800, 800),
+    # 16 views of uneven resolution over 3M triangles, one graph-captured launch per pass
+    "c4_3M_16views": (3_000_000, 16, 0, 0),
 }
+C4_SIDES = (256, 512, 768, 1024)
+
+
+def c4_views(seed=0):
+    """16 cameras on the radius-3 sphere, side lengths drawn from {256, 512, 768, 1024}."""
+    from diff_tritracer import scenes
+
+    rng = np.random.default_rng(seed + 4)
+    sides = rng.choice(C4_SIDES, size=16)
+    cams = [scenes.sphere_cameras(1, int(n), int(n), seed=seed + 100 + i)[0] for i, n in enumerate(sides)]
+    return [scenes.camera_rays(c) for c in cams]
 
 
 def make_workload(name, seed=0):
@@ -46,6 +59,10 @@ def make_workload(name, seed=0):
 
     P, views, H, W = WORKLOADS[name]
     sc = scenes.make_scene(P, seed=seed)
+    if name.startswith("c4"):
+        rays = c4_views(seed)
+        ups = [scenes.upstream_grads(r[0].shape[0], r[0].shape[1], seed=seed + i) for i, r in enumerate(rays)]
+        return sc, rays, ups
     cams = scenes.sphere_cameras(views, H, W, seed=seed)
     rays = [scenes.camera_rays(c) for c in cams]
     ro = np.ascontiguousarray(np.concatenate([r[0] for r in rays], 0))
@@ -200,6 +217,82 @@ def algorithmic_bytes(rays, evals, blends):
     return fwd, bwd
 
 
+def run_views(args, world, rank, local, dev):
+    """Batched uneven views: every step is one CUDA-graph replay of refit +
+    forward + adjoint over all 16 views (ViewBatch), after autotuning."""
+    import torch
+    import torch.distributed as dist
+
+    from diff_tritracer import _C
+    from diff_tritracer.autotune import autotune
+    from diff_tritracer.batch import ViewBatch
+
+    name = args.workload
+    P = WORKLOADS[name][0]
+    sc, rays_np, ups_np = make_workload(name)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    scene = dict(triangles_points=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), num_points_per_triangle=T(sc.num_points),
+                 cumsum_of_points_per_triangle=T(sc.cumsum), number_of_points=P, shs=T(sc.shs),
+                 opacities=T(sc.opacities), scaling=torch.zeros(P, device=dev), density_factor=torch.zeros(P, device=dev))
+    shapes = [r[0].shape[:2] for r in rays_np]
+    R = int(sum(h * w for h, w in shapes))
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    bg = torch.zeros(3, device=dev)
+    eager = ViewBatch(tr, shapes, scene, 3, bg, graph=False)
+    eager.set_rays([(T(a), T(b)) for a, b in rays_np])
+    eager.set_upstream([(T(a), T(b)) for a, b in ups_np])
+    tuned = None if args.no_autotune else autotune(tr, eager.step, key=name, iters=2)
+    # kernels per step, counted on an eager step (graph replays are not seen by the host counter)
+    tr.reset_stats()
+    eager.step()
+    per_step = tr.stats()["kernel_launches"]
+    vb = ViewBatch(tr, shapes, scene, 3, bg, graph=True)
+    vb.set_rays([(T(a), T(b)) for a, b in rays_np])
+    vb.set_upstream([(T(a), T(b)) for a, b in ups_np])
+    for _ in range(max(3, args.warmup)):
+        vb.step()
+    torch.cuda.synchronize()
+    tr.device_status()
+    sampler = ClockSampler(local)
+    tr.reset_stats()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        vb.step()
+    t1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = t0.elapsed_time(t1)
+    st = tr.stats()
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": world * R * args.steps / (ms / 1e3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "triangles": P, "views": len(shapes),
+                   "resolutions": [f"{h}x{w}" for h, w in shapes], "rays_per_step": R,
+                   "step": "one CUDA-graph replay: refit + forward + adjoint over all views",
+                   "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
+                   "autotune_ms": tuned.get("all") if tuned else None,
+                   "hits_per_ray": {"evaluated": st["evaluated_hits"] / max(st["rays"], 1),
+                                    "blended": st["blended_hits"] / max(st["rays"], 1)}},
+        "gpu_launches": int(per_step * args.steps), "clocks": clocks,
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -210,6 +303,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-budget", type=float, default=3.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default traversal configuration")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -231,8 +325,11 @@ def main():
 
     import diff_tritracer
     from diff_tritracer import _C
+    from diff_tritracer.autotune import autotune
 
     name = args.workload
+    if name.startswith("c4"):
+        return run_views(args, world, rank, local, dev)
     P, views, H, W = WORKLOADS[name]
     sc, ro_np, rd_np, g_np, go_np = make_workload(name)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -272,6 +369,9 @@ def main():
             bwd_ms.append(e[1].elapsed_time(e[2]))
         return float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
 
+    tuned = None
+    if not args.no_autotune:
+        tuned = autotune(tr, step, key=f"{name}", iters=2)
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -382,6 +482,7 @@ def main():
                    "step": "BVH refit + forward trace + adjoint trace",
                    "l2": "inputs larger than L2 (scene + BVH + rays ~0.5 GB per step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
                    "hits_per_ray": {"evaluated": evals / max(rays_step, 1), "blended": blends / max(rays_step, 1)},
                    "traversal_per_ray": {k: st[k] / max(st["rays"], 1)
                                          for k in ("queries", "node_visits", "triangle_tests",
