@@ -1,5 +1,7 @@
 // C ABI (include/tritracer.h): the handle that replaces the reference's
 // OptixTracer class (tritracer/tracer.h:67-126, tracer.cpp, pipeline.cpp).
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -7,6 +9,7 @@
 
 #include "../../include/tritracer.h"
 #include "bvh.cuh"
+#include "proposal.cuh"
 #include "trace.cuh"
 
 struct tt_tracer {
@@ -17,7 +20,7 @@ struct tt_tracer {
   int cfg_id = tt::kCfgPackets16;
   std::string err;
   tt::Bvh bvh;
-  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[6] from byte 16
+  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[kNumStats] from byte 16
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
@@ -180,6 +183,10 @@ static int add_view(tt_tracer* h, tt::TraceParams& p, const tt_view& v) {
   d.others = v.others;
   d.dL_dpix = v.dL_dpixels;
   d.dL_doth = v.dL_dothers;
+  d.interval = v.interval;
+  d.record = v.record;
+  TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN || (!v.interval && !v.record),
+             "proposed intervals and hit records are for the plain variant only");
   d.H = v.H;
   d.W = v.W;
   d.ntx = (v.W + 7) / 8;
@@ -363,7 +370,7 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   if (!h) return TT_ERR_INVALID;
   if (!out) return fail(h, TT_ERR_INVALID, "null stats pointer");
   const cudaStream_t s = as_stream(stream);
-  unsigned long long v[7] = {0, 0, 0, 0, 0, 0, 0};
+  unsigned long long v[tt::kNumStats] = {};
   TT_CUDA(h, cudaMemcpyAsync(v, h->scratch.as<char>() + 16, sizeof(v), cudaMemcpyDeviceToHost, s));
   TT_CUDA(h, cudaStreamSynchronize(s));
   out->rays = v[0];
@@ -374,12 +381,14 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   out->triangle_tests = v[4];
   out->queries = v[5];
   out->packet_node_visits = v[6];
+  out->interval_continuations = v[7];
+  out->interval_retraces = v[8];
   return TT_OK;
 }
 
 int tt_reset_stats(tt_tracer* h, void* stream) {
   if (!h) return TT_ERR_INVALID;
-  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, 56, as_stream(stream)));
+  TT_CUDA(h, cudaMemsetAsync(h->scratch.as<char>() + 16, 0, tt::kNumStats * 8, as_stream(stream)));
   h->launch_base = h->launches();
   return TT_OK;
 }
@@ -403,6 +412,148 @@ int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, i
   TT_CUDA(h, tt::launch_hit_stream(p, as_stream(stream)));
   if (R > 0) ++h->trace_launches;
   return TT_OK;
+}
+
+// ---------------------------------------------------------------- proposal network
+static int check_mlp(tt_tracer* h, const tt_mlp* net) {
+  TT_REQUIRE(h, net != nullptr, "null network");
+  TT_REQUIRE(h, net->weights && net->master, "network weights must be device pointers");
+  TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(net->weights) & 15u) == 0, "network weights must be 16-byte aligned");
+  TT_REQUIRE(h, net->t_scale != 0.f, "t_scale must be nonzero");
+  return TT_OK;
+}
+
+int tt_mlp_update(tt_tracer* h, const tt_mlp* net, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  int rc = check_mlp(h, net);
+  if (rc != TT_OK) return rc;
+  tt::mlp::AdamParams a;
+  std::memset(&a, 0, sizeof(a));
+  a.master = net->master;
+  a.w = net->weights;
+  a.adam = 0;
+  TT_CUDA(h, tt::mlp::launch_adam(a, as_stream(stream)));
+  ++h->trace_launches;
+  return TT_OK;
+}
+
+int tt_mlp_train_step(tt_tracer* h, const tt_mlp* net, const tt_mlp_step* st, const float* rays,
+                      const float* targets, int n, float* loss, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  int rc = check_mlp(h, net);
+  if (rc != TT_OK) return rc;
+  TT_REQUIRE(h, st != nullptr && st->step >= 1, "need a step description with step >= 1");
+  TT_REQUIRE(h, n > 0 && rays && targets, "need n > 0 rays and targets");
+  TT_REQUIRE(h, net->adam_m && net->adam_v && net->partial, "Adam state and partial buffer must be device pointers");
+  const cudaStream_t s = as_stream(stream);
+  const int ntiles = (n + tt::mlp::kTileRows - 1) / tt::mlp::kTileRows;
+  const int per = (ntiles + h->num_sms - 1) / h->num_sms;
+  const int grid = (ntiles + per - 1) / per;
+  TT_REQUIRE(h, grid <= net->partial_ctas, "partial buffer too small for this batch");
+  tt::mlp::TrainParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.w = net->weights;
+  p.rays = rays;
+  p.targets = targets;
+  p.n = n;
+  p.ntiles = ntiles;
+  p.tiles_per_cta = per;
+  p.origin_scale = net->origin_scale;
+  p.t_shift = net->t_shift;
+  p.inv_t_scale = 1.0f / net->t_scale;
+  p.near_weight = st->near_weight;
+  p.far_weight = st->far_weight;
+  p.partial = net->partial;
+  p.status = h->scratch.as<int>() + 1;
+  TT_CUDA(h, tt::mlp::launch_train(p, grid, s));
+  tt::mlp::AdamParams a;
+  std::memset(&a, 0, sizeof(a));
+  a.partial = net->partial;
+  a.nparts = grid;
+  a.grad_scale = 1.0f / (float)n;
+  a.master = net->master;
+  a.m = net->adam_m;
+  a.v = net->adam_v;
+  a.w = net->weights;
+  a.lr = st->lr;
+  a.beta1 = st->beta1;
+  a.beta2 = st->beta2;
+  a.eps = st->eps;
+  a.c1 = (float)(1.0 / (1.0 - std::pow((double)st->beta1, st->step)));
+  a.c2 = (float)(1.0 / (1.0 - std::pow((double)st->beta2, st->step)));
+  a.loss = loss;
+  a.adam = 1;
+  TT_CUDA(h, tt::mlp::launch_adam(a, s));
+  h->trace_launches += 2;
+  return TT_OK;
+}
+
+static int mlp_infer(tt_tracer* h, const tt_mlp* net, tt::mlp::InferParams& p, float margin_near, float margin_far,
+                     float far_cap, cudaStream_t s) {
+  p.w = net->weights;
+  p.origin_scale = net->origin_scale;
+  p.t_shift = net->t_shift;
+  p.t_scale = net->t_scale;
+  p.margin_near = margin_near;
+  p.margin_far = margin_far;
+  p.far_cap = far_cap;
+  p.status = h->scratch.as<int>() + 1;
+  if (p.ntiles == 0) return TT_OK;
+  const int grid = std::min(p.ntiles, h->num_sms * tt::mlp::infer_blocks_per_sm());
+  TT_CUDA(h, tt::mlp::launch_infer(p, grid, s));
+  ++h->trace_launches;
+  return TT_OK;
+}
+
+int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, float* out, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  int rc = check_mlp(h, net);
+  if (rc != TT_OK) return rc;
+  TT_REQUIRE(h, n >= 0 && (n == 0 || (rays && out)), "need rays and out for n > 0");
+  tt::mlp::InferParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.nsets = 1;
+  tt::mlp::RaySet& r = p.sets[0];
+  r.o = rays;
+  r.d = rays + 3;
+  r.stride = 6;
+  r.out0 = out;
+  r.out1 = out + 1;
+  r.ostride = 2;
+  r.n = n;
+  r.tile_begin = 0;
+  p.ntiles = (n + tt::mlp::kTileRows - 1) / tt::mlp::kTileRows;
+  return mlp_infer(h, net, p, 0.f, 0.f, INFINITY, as_stream(stream));
+}
+
+int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int n_views, float* const* intervals,
+                     float margin_near, float margin_far, float far_cap, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  int rc = check_mlp(h, net);
+  if (rc != TT_OK) return rc;
+  TT_REQUIRE(h, views && intervals && n_views >= 1 && n_views <= tt::mlp::kMaxViews, "need 1..32 views");
+  tt::mlp::InferParams p;
+  std::memset(&p, 0, sizeof(p));
+  long long tiles = 0;
+  for (int i = 0; i < n_views; ++i) {
+    const tt_view& v = views[i];
+    TT_REQUIRE(h, v.H > 0 && v.W > 0 && v.ray_o && v.ray_d && intervals[i], "view needs H, W > 0, rays and an interval");
+    TT_REQUIRE(h, (long long)v.H * v.W < (1ll << 31), "too many rays in a view");
+    tt::mlp::RaySet& r = p.sets[i];
+    r.n = v.H * v.W;
+    r.o = v.ray_o;
+    r.d = v.ray_d;
+    r.stride = 3;
+    r.out0 = intervals[i];
+    r.out1 = intervals[i] + r.n;
+    r.ostride = 1;
+    r.tile_begin = (int)tiles;
+    tiles += (r.n + tt::mlp::kTileRows - 1) / tt::mlp::kTileRows;
+  }
+  TT_REQUIRE(h, tiles < (1ll << 30), "too many rays");
+  p.nsets = n_views;
+  p.ntiles = (int)tiles;
+  return mlp_infer(h, net, p, margin_near, margin_far, far_cap, as_stream(stream));
 }
 
 }  // extern "C"

@@ -58,9 +58,10 @@ __device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsi
 
 struct Counters {
   unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
+  unsigned cont = 0, restart = 0;  // proposed intervals left by continuation / re-trace
 };
 
-// The kChunk smallest hit keys >= key_min (t <= far) along the ray, in
+// The kChunk smallest hit keys >= key_min (t <= t_hi) along the ray, in
 // ascending order, EMPTY-padded. If the stack overflowed, subtrees were
 // dropped and t_drop is the smallest entry distance among them: only keys with
 // t < t_drop are then guaranteed.
@@ -71,7 +72,7 @@ struct Counters {
 // never culls a reported hit, and empty slots hold inverted boxes that never
 // pass. Hit children are pushed in slot order with the nearest one on top.
 template <int SD>
-__device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min,
+__device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min, float t_hi,
                                       unsigned long long (&kb)[kChunk], Stack st, float& t_drop, int* status,
                                       Counters& cnt) {
   ++cnt.queries;
@@ -80,7 +81,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
   t_drop = INFINITY;
   if (!bvh.has_root) return;
   const float t_lo = key_t(key_min);
-  float tmax = kFar;
+  float tmax = t_hi;
   // word offsets of the near / far planes (lo at +0, hi at +2 within each axis)
   const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
   const int fx = nx ^ 2, fy = ny ^ 2, fz = nz ^ 2;
@@ -216,7 +217,7 @@ __device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int strid
 
 template <int K>
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
-                                             unsigned long long key_min, unsigned long long* kb, int kstride,
+                                             unsigned long long key_min, float t_hi, unsigned long long* kb, int kstride,
                                              WarpStack ws, float& t_drop, int* status, Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
@@ -228,7 +229,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
   if (act == 0 || !bvh.has_root) return;
   if (want) ++cnt.queries;
   const float t_lo = want ? key_t(key_min) : 0.f;
-  float tmax = want ? kFar : -1.0f;  // a lane without a query never passes a test
+  float tmax = want ? t_hi : -1.0f;  // a lane without a query never passes a test
   const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
   const int fx = nx ^ 2, fy = ny ^ 2, fz = nz ^ 2;
   if (lane == 0) {
@@ -531,22 +532,38 @@ __device__ __forceinline__ Smem thread_smem() {
   return s;
 }
 
-// Where a ray's next k-closest query starts, and where it is inside the
-// reference's 16-hit chunk.
+// Where a ray's next k-closest query starts, where it is inside the
+// reference's 16-hit chunk, and the far bound of its queries (the far plane,
+// or the end of a proposed interval until the ray leaves it).
 struct Cursor {
   unsigned long long key_min;
   float last_hit_t;
+  float t_hi;
   int ref_pos;
   int chunks;
 };
 
+__device__ __forceinline__ unsigned long long first_key(int tmin_inclusive) {
+  return tmin_inclusive ? 0ull : (1ull << 32);
+}
+
 __device__ __forceinline__ Cursor first_cursor(int tmin_inclusive) {
   Cursor c;
-  c.key_min = tmin_inclusive ? 0ull : (1ull << 32);
+  c.key_min = first_key(tmin_inclusive);
   c.last_hit_t = 0.f;
+  c.t_hi = kFar;
   c.ref_pos = 0;
   c.chunks = 0;
   return c;
+}
+
+// Clips a ray's first query to the proposed interval [t_near, t_far]
+// (interval planes [2][H][W]); a NaN or out-of-range bound falls back to the
+// plain one.
+__device__ __forceinline__ void clip_cursor(Cursor& c, const float* interval, int HW, int pix) {
+  const float tn = __ldg(interval + pix), tf = __ldg(interval + HW + pix);
+  if (tn > 0.f && tn < kFar) c.key_min = max(c.key_min, (unsigned long long)__float_as_uint(tn) << 32);
+  if (tf >= 0.f && tf < kFar) c.t_hi = tf;
 }
 
 // Visits the keys of one query (K keys, ascending, staged in shared memory)
@@ -563,15 +580,35 @@ __device__ __forceinline__ Cursor first_cursor(int tmin_inclusive) {
 // query start at that bound; after a full or truncated buffer the stream
 // resumes right after the last key taken. The query size K is therefore a
 // performance choice that never changes the visited sequence.
+//
+// Proposed intervals: when a clipped stream runs out (no key left below
+// cur.t_hi) before the ray terminated, the ray is not finished: its queries go
+// on from the next key with the far plane as bound (a continuation, counted
+// in cnt.cont), or, if the interval held no hit at all, from the start of the
+// ray (a plain re-trace, cnt.restart). Either way every hit at or beyond
+// t_near is visited in the plain order.
 template <int K, class Shader>
 __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Cursor& cur, int tmin_inclusive,
-                                              int* status, Shader& sh) {
+                                              int* status, Shader& sh, Counters& cnt) {
   const bool truncated = t_drop < INFINITY;
   auto trusted = [&](unsigned long long key) {
     return key != kEmptyKey && !(truncated && key_t(key) >= t_drop);
   };
   unsigned long long last_key = 0;
   bool any = false;
+  // the stream ran out below cur.t_hi; `next` is where it would resume
+  auto exhausted = [&](unsigned long long next) {
+    if (cur.t_hi >= kFar) return true;
+    cur.t_hi = kFar;
+    if (!any && cur.chunks == 0) {
+      cur.key_min = first_key(tmin_inclusive);
+      ++cnt.restart;
+    } else {
+      cur.key_min = next;
+      ++cnt.cont;
+    }
+    return false;
+  };
   int boundaries = 0;
   sh.prepare();
   int i = 0;
@@ -584,7 +621,7 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
     // fmaxf(last + STEP_EPSILON, t) with the sum in double (forward.cu:111)
     cur.last_hit_t = fmaxf(__double2float_rn(__dadd_rn((double)cur.last_hit_t, kStepEps)), t);
     ++cur.ref_pos;
-    if (t >= kNear && sh.visit(key_prim(key))) return true;
+    if (t >= kNear && sh.visit(key_prim(key), t)) return true;
     if (cur.ref_pos == kChunk) {
       // the reference's next optixTrace starts at last_hit_t
       cur.ref_pos = 0;
@@ -600,13 +637,14 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
         i = j;  // continue inside the buffer
         continue;
       }
-      if (j < K && sm.keys[j * sm.stride] == kEmptyKey && !truncated) return true;  // stream exhausted
+      if (j < K && sm.keys[j * sm.stride] == kEmptyKey && !truncated) return exhausted(bound);
       cur.key_min = bound;
       return false;
     }
     ++i;
   }
-  if (i < K && sm.keys[i * sm.stride] == kEmptyKey && !truncated) return true;  // stream exhausted
+  if (i < K && sm.keys[i * sm.stride] == kEmptyKey && !truncated)
+    return exhausted(any ? last_key + 1ull : cur.key_min);
   if (!any) {
     atomicOr(status, kStatusStack);  // a truncated query that trusted nothing
     return true;
@@ -664,6 +702,7 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
             o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
             d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
             cur = first_cursor(p.tmin_inclusive);
+            if (v.interval) clip_cursor(cur, v.interval, v.H * v.W, pix);
             if (sh.begin(&v, pix, o, d))
               have = true;
             else
@@ -680,13 +719,13 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
     if (have) {
       const RayW r = make_ray(o, d);
       unsigned long long kb[kChunk];
-      query<SD>(p.bvh, r, cur.key_min, kb, sm.st, t_drop, p.status, cnt);
+      query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
       for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
     }
     __syncwarp();
     if (have) {
-      bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+      bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);
       if (!done && ++cur.chunks >= kMaxChunks) {
         atomicOr(p.status, kStatusTimeout);
         done = true;
@@ -735,14 +774,15 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       const int pix = py * v.W + px;
       o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
       d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
+      if (v.interval) clip_cursor(cur, v.interval, v.H * v.W, pix);
       sh.begin(&v, pix, o, d);  // the plain shaders always trace their one ray
     }
     const RayW r = make_ray(o, d);
     while (__any_sync(full, active)) {
       float t_drop;
-      packet_query<K>(p.bvh, r, active, cur.key_min, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+      packet_query<K>(p.bvh, r, active, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
       if (active) {
-        bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh);
+        bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);
         if (!done && ++cur.chunks >= kMaxChunks) {
           atomicOr(p.status, kStatusTimeout);
           done = true;
@@ -817,9 +857,9 @@ __device__ __forceinline__ void run(const TraceParams& p, Shader& sh, Counters& 
 // ---------------------------------------------------------------- forward
 __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends,
                                           const Counters& c) {
-  const unsigned v[7] = {rays, evals, blends, c.nodes, c.tris, c.queries, c.warp_nodes};
+  const unsigned v[kNumStats] = {rays, evals, blends, c.nodes, c.tris, c.queries, c.warp_nodes, c.cont, c.restart};
 #pragma unroll
-  for (int i = 0; i < 7; ++i) {
+  for (int i = 0; i < kNumStats; ++i) {
     const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[i]);
     if ((threadIdx.x & 31) == 0) atomicAdd(stats + i, (unsigned long long)s);
   }
@@ -833,6 +873,7 @@ struct FwdShader {
   float3 o, d;
   float C0, C1, C2, N0, N1, N2, T;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
+  unsigned first_eval = 0;  // value of n_eval at the ray's first hit (record only)
 
   __device__ explicit FwdShader(const TraceParams& params) : p(params) {}
 
@@ -844,6 +885,14 @@ struct FwdShader {
     C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
     T = 1.0f;
     ++n_rays;
+    if (v->record) {
+      // t of the first and last hit visited, and whether the ray terminated
+      const int HW = v->H * v->W;
+      v->record[pix] = INFINITY;
+      v->record[HW + pix] = INFINITY;
+      v->record[2 * HW + pix] = 0.0f;
+      first_eval = n_eval + 1;
+    }
     return true;
   }
 
@@ -851,14 +900,23 @@ struct FwdShader {
 
   __device__ __forceinline__ void prepare() {}
 
-  __device__ __forceinline__ bool visit(uint32_t prim) {
+  __device__ __forceinline__ bool visit(uint32_t prim, float t) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
     ++n_eval;
+    float* rec = v->record;
+    const int HW = v->H * v->W;
+    if (rec) {
+      if (n_eval == first_eval) rec[pix] = t;
+      rec[HW + pix] = t;
+    }
     const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
     if (alpha < kAlphaMin) return false;
     const float test_T = T * (1.0f - alpha);
-    if (test_T < kTMin) return true;
+    if (test_T < kTMin) {
+      if (rec) rec[2 * HW + pix] = 1.0f;
+      return true;
+    }
     ++n_blend;
     p.density[prim] = 1.0f;
     compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
@@ -1046,7 +1104,7 @@ struct VarShader {
 
   __device__ __forceinline__ void prepare() {}
 
-  __device__ __forceinline__ bool visit(uint32_t prim) {
+  __device__ __forceinline__ bool visit(uint32_t prim, float) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
     ++n_eval;
@@ -1191,7 +1249,7 @@ struct BwdShader {
     gN2 = __ldg(v->dL_doth + (kNormalCh + 2) * HW + pix);
   }
 
-  __device__ __forceinline__ bool visit(uint32_t prim) {
+  __device__ __forceinline__ bool visit(uint32_t prim, float) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const float sig = __ldg(p.sigma + prim);
     const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
@@ -1285,7 +1343,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
     Counters cnt;
-    query<kStackDepth>(p.bvh, r, key_min, kb, st, t_drop, p.status, cnt);
+    query<kStackDepth>(p.bvh, r, key_min, kFar, kb, st, t_drop, p.status, cnt);
     int consumed = 0;
     unsigned long long last = 0;
 #pragma unroll

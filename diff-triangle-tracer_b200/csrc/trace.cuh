@@ -19,6 +19,8 @@ struct ViewDesc {
   const float* others;   // adjoint: forward side outputs
   const float* dL_dpix;  // adjoint: upstream gradients
   const float* dL_doth;
+  const float* interval;  // optional [2][H][W]: per-ray [t_near, t_far] clip of the traversal
+  float* record;          // optional [3][H][W] (forward): t of the first / last hit visited, terminated
   int H, W, ntx, tile_begin;
 };
 
@@ -52,7 +54,7 @@ struct TraceParams {
   int cfg;      // traversal configuration, kCfg*
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
-  unsigned long long* stats;  // forward: rays, evaluated hits, blended hits, node visits, triangle tests, queries
+  unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)
 };
 
 struct HitStreamParams {
@@ -66,6 +68,11 @@ struct HitStreamParams {
   int* counts;
   int* status;
 };
+
+// forward counters: rays, evaluated hits, blended hits, node visits, triangle
+// tests, queries, warp-packet node visits, interval continuations, interval
+// re-traces
+constexpr int kNumStats = 9;
 
 constexpr int kTraceThreads = 128;
 constexpr int kStackDepth = 32;

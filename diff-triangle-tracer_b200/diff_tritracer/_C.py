@@ -94,6 +94,8 @@ class OptixTracer:
             raise _lib.TracerError(rc, f"OptixTracer construction failed (tt_create returned {rc})")
         self._h = h
         self._keep = ()
+        self._proposal = None
+        self._proposal_args = (None, None, None)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -155,7 +157,16 @@ class OptixTracer:
         a.rebuild_gas, a.debug = int(rebuild_gas_opt), 1 if debug else 0
         a.out_color, a.out_others, a.max_blending = _ptr(out_color), _ptr(out_others), _ptr(max_blending)
         a.gpu_time_ms = ctypes.pointer(ms)
-        check(self._h, lib.tt_forward(self._h, ctypes.byref(a), _stream()))
+        if self._proposal is not None:
+            v = _lib.TtView()
+            v.H, v.W, v.ray_o, v.ray_d = H, W, a.ray_o, a.ray_d
+            v.out_color, v.out_others = a.out_color, a.out_others
+            iv = self._intervals(ro, rd)
+            v.interval = _ptr(iv)
+            check(self._h, lib.tt_forward_views(self._h, ctypes.byref(a), ctypes.byref(v), 1, _stream()))
+        else:
+            iv = None
+            check(self._h, lib.tt_forward(self._h, ctypes.byref(a), _stream()))
         if sc.data_ptr() != scaling.data_ptr():
             scaling.copy_(sc.view_as(scaling))
         if de.data_ptr() != density_factor.data_ptr():
@@ -164,7 +175,7 @@ class OptixTracer:
         if debug:
             gpu_time.fill_(ms.value)
         # the arrays the kernels read must outlive the asynchronous launch
-        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de)
+        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de, iv)
         return FwdTraceResult((out_color, out_others, gpu_time, scaling, density_factor, max_blending))
 
     def trace_backward(self, ray_o, ray_d, background, triangles_points, sigma, num_points_per_triangle,
@@ -207,11 +218,35 @@ class OptixTracer:
         a.dL_dtriangle, a.dL_dsigma = _ptr(dL_dtriangle), _ptr(dL_dsigma)
         a.dL_dopacity, a.dL_dsh = _ptr(dL_dopacity), _ptr(dL_dsh)
         a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
-        check(self._h, lib.tt_backward(self._h, ctypes.byref(a), _stream()))
-        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg)
+        if self._proposal is not None:
+            v = _lib.TtView()
+            v.H, v.W, v.ray_o, v.ray_d = H, W, a.ray_o, a.ray_d
+            v.colors, v.others, v.dL_dpixels, v.dL_dothers = a.colors, a.others, a.dL_dpixels, a.dL_dothers
+            iv = self._intervals(ro, rd)
+            v.interval = _ptr(iv)
+            check(self._h, lib.tt_backward_views(self._h, ctypes.byref(a), ctypes.byref(v), 1, _stream()))
+        else:
+            iv = None
+            check(self._h, lib.tt_backward(self._h, ctypes.byref(a), _stream()))
+        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg, iv)
         return BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
 
     # ------------------------------------------------------------------
+    def set_proposal(self, proposal, margin_near=None, margin_far=None, far_cap=None):
+        """Clips every plain trace_forward / trace_backward of this handle to
+        the intervals of a trained `diff_tritracer.proposal.Proposal` (None:
+        back to the plain traversal). The network runs on the same rays in
+        the forward and in the adjoint, so both visit the same hits. No
+        reference counterpart."""
+        if proposal is not None and self.variant != _lib.TT_VARIANT_PLAIN:
+            raise RuntimeError("proposed intervals are for the plain program only")
+        self._proposal = proposal
+        self._proposal_args = (margin_near, margin_far, far_cap)
+
+    def _intervals(self, ro, rd):
+        mn, mf, cap = self._proposal_args
+        return self._proposal.intervals([(ro, rd)], mn, mf, cap)[0]
+
     def set_traversal(self, traversal: str = "auto", k: int = 16, stack_depth: int = 32):
         """Switches the traversal configuration (the BVH is kept)."""
         modes = {"auto": _lib.TT_TRAVERSAL_AUTO, "packets": _lib.TT_TRAVERSAL_PACKETS, "lanes": _lib.TT_TRAVERSAL_LANES}
@@ -244,9 +279,12 @@ class OptixTracer:
 
     def trace_forward_views(self, rays, triangles_points, sigma, num_points_per_triangle,
                             cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities, scaling,
-                            density_factor, bg_color, rebuild_gas_opt, outputs=None, max_blending=None):
+                            density_factor, bg_color, rebuild_gas_opt, outputs=None, max_blending=None,
+                            intervals=None, records=None):
         """Forward over up to 32 views of any resolutions in one launch.
-        rays: list of (ray_o, ray_d), each [H, W, 3]. Returns ([(color, others)], max_blending)."""
+        rays: list of (ray_o, ray_d), each [H, W, 3]. Returns ([(color, others)], max_blending).
+        intervals: optional per-view [2, H, W] proposed [t_near, t_far] clips (None entries allowed);
+        records: optional per-view [3, H, W] outputs of (t_first, t_last, terminated) per ray."""
         dev = self.device
         P = int(number_of_points)
         if max_blending is None:
@@ -270,13 +308,14 @@ class OptixTracer:
             vs[i].out_color, vs[i].out_others = _ptr(col), _ptr(oth)
             outs.append((col, oth))
             keep = keep + (ro, rd)
+            keep = keep + self._interval_record(vs[i], H, W, intervals, records, i)
         check(self._h, lib.tt_forward_views(self._h, ctypes.byref(a), vs, len(rays), _stream()))
         self._keep = keep
         return outs, max_blending
 
     def trace_backward_views(self, rays, forward_outputs, upstream, triangles_points, sigma,
                              num_points_per_triangle, cumsum_of_points_per_triangle, number_of_points, shs,
-                             sh_degree, opacities, bg_color, grads=None):
+                             sh_degree, opacities, bg_color, grads=None, intervals=None):
         """Adjoint over the views of trace_forward_views. upstream: list of
         (dL_dpixels [3,H,W], dL_dothers [7,H,W]). Returns (dL_dtriangle, dL_dsigma,
         dL_dopacity, dL_dsh) summed over the views."""
@@ -315,6 +354,7 @@ class OptixTracer:
             vs[i].colors, vs[i].others = _ptr(col), _ptr(oth)
             vs[i].dL_dpixels, vs[i].dL_dothers = _ptr(g), _ptr(go)
             keep = keep + (ro, rd, col, oth, g, go)
+            keep = keep + self._interval_record(vs[i], vs[i].H, vs[i].W, intervals, None, i)
         check(self._h, lib.tt_backward_views(self._h, ctypes.byref(a), vs, len(rays), _stream()))
         self._keep = keep
         return grads
@@ -323,6 +363,22 @@ class OptixTracer:
         """Synchronises and raises if a bounded device loop gave up since the
         last check (no reference counterpart)."""
         check(self._h, lib.tt_device_status(self._h, _stream()))
+
+    def _interval_record(self, view, H, W, intervals, records, i):
+        keep = ()
+        if intervals is not None and intervals[i] is not None:
+            iv = _f32(intervals[i], "interval", self.device)
+            if tuple(iv.shape) != (2, H, W):
+                raise ValueError(f"interval of view {i} must be [2, {H}, {W}], got {tuple(iv.shape)}")
+            view.interval = _ptr(iv)
+            keep += (iv,)
+        if records is not None and records[i] is not None:
+            rec = records[i]
+            if rec.dtype != torch.float32 or not rec.is_contiguous() or tuple(rec.shape) != (3, H, W):
+                raise ValueError(f"record of view {i} must be a contiguous float32 [3, {H}, {W}] tensor")
+            view.record = _ptr(rec)
+            keep += (rec,)
+        return keep
 
     def stats(self):
         """Synchronises; returns the handle's counters since reset_stats()."""

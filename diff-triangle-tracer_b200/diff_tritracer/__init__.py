@@ -122,3 +122,8 @@ class Tracer(nn.Module):
         return _Tracer.apply(self.tracer, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
                              cumsum_of_points_per_triangle, number_of_points, shs, colors_precomp, opacities, scaling,
                              density_factor, tracer_settings)
+
+    def set_proposal(self, proposal, margin_near=None, margin_far=None, far_cap=None):
+        """Clips the traversal of the forward and backward passes to the
+        intervals of a trained proposal network (None: plain traversal)."""
+        self.tracer.set_proposal(proposal, margin_near, margin_far, far_cap)

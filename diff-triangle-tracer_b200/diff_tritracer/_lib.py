@@ -73,20 +73,38 @@ class TtBwdArgs(ctypes.Structure):
 class TtView(ctypes.Structure):
     _fields_ = [("H", ctypes.c_int), ("W", ctypes.c_int), ("ray_o", _vp), ("ray_d", _vp),
                 ("out_color", _vp), ("out_others", _vp), ("colors", _vp), ("others", _vp),
-                ("dL_dpixels", _vp), ("dL_dothers", _vp)]
+                ("dL_dpixels", _vp), ("dL_dothers", _vp), ("interval", _vp), ("record", _vp)]
 
 
 class TtStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
                 ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
                 ("node_visits", ctypes.c_ulonglong), ("triangle_tests", ctypes.c_ulonglong),
-                ("queries", ctypes.c_ulonglong), ("packet_node_visits", ctypes.c_ulonglong)]
+                ("queries", ctypes.c_ulonglong), ("packet_node_visits", ctypes.c_ulonglong),
+                ("interval_continuations", ctypes.c_ulonglong), ("interval_retraces", ctypes.c_ulonglong)]
+
+
+TT_MLP_PARAMS = 16640
+TT_MLP_PARTIAL = 16656
+
+
+class TtMlp(ctypes.Structure):
+    _fields_ = [("weights", _vp), ("master", _vp), ("adam_m", _vp), ("adam_v", _vp), ("partial", _vp),
+                ("partial_ctas", ctypes.c_int), ("origin_scale", ctypes.c_float), ("t_shift", ctypes.c_float),
+                ("t_scale", ctypes.c_float)]
+
+
+class TtMlpStep(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("step", ctypes.c_int), ("near_weight", ctypes.c_float),
+                ("far_weight", ctypes.c_float)]
 
 
 EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
-    "tt_backward_views", "tt_set_traversal",
+    "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
+    "tt_mlp_intervals",
 )
 
 
@@ -110,6 +128,12 @@ def _load():
     lib.tt_get_stats.argtypes = [_vp, ctypes.POINTER(TtStats), _vp]
     lib.tt_reset_stats.argtypes = [_vp, _vp]
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+    lib.tt_mlp_update.argtypes = [_vp, ctypes.POINTER(TtMlp), _vp]
+    lib.tt_mlp_train_step.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtMlpStep), _vp, _vp, ctypes.c_int,
+                                      _vp, _vp]
+    lib.tt_mlp_predict.argtypes = [_vp, ctypes.POINTER(TtMlp), _vp, ctypes.c_int, _vp, _vp]
+    lib.tt_mlp_intervals.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtView), ctypes.c_int,
+                                     ctypes.POINTER(_vp), ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype if name == "tt_last_error" else ctypes.c_int
     return lib

@@ -146,6 +146,18 @@ typedef struct tt_view {
   const float* others;
   const float* dL_dpixels;
   const float* dL_dothers;
+  /* Proposed intervals (plain variant; NULL = none): [2][H][W], per ray the
+   * [t_near, t_far] its traversal is clipped to. Hits before t_near are not
+   * visited. A ray still unterminated when its hits up to t_far are used up
+   * goes on beyond t_far (a continuation); a ray with no hit in its interval
+   * is traced again without it. Forward and adjoint of the same rays must get
+   * the same intervals. */
+  const float* interval;
+  /* Forward only (plain variant; NULL = none): [3][H][W], per ray the t of
+   * the first and of the last hit the march visited (INFINITY if none) and
+   * 1.0 if the ray ended on the transmittance cut-off, else 0.0: the
+   * training targets of the proposal network. */
+  float* record;
 } tt_view;
 
 /* OptixTracer::OptixTracer (tritracer/pipeline.cpp:267-302). `cfg` may be
@@ -207,6 +219,8 @@ typedef struct tt_stats {
   unsigned long long triangle_tests;
   unsigned long long queries;
   unsigned long long packet_node_visits; /* node visits counted once per warp packet */
+  unsigned long long interval_continuations; /* rays that went on beyond their proposed t_far */
+  unsigned long long interval_retraces;      /* rays traced again: no hit in their interval */
 } tt_stats;
 
 /* Synchronises `stream`, then fills *out. */
@@ -221,6 +235,71 @@ int tt_reset_stats(tt_tracer* h, void* stream);
  * device arrays, counts [R] receives each ray's total hit count. */
 int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
                   float* ts, int* counts, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Proposal network (no reference counterpart). A small MLP maps each ray to
+ * the interval [t_near, t_far] holding the hits its march visits; the trace
+ * is clipped to it through tt_view.interval. Inputs (80): the ray origin
+ * scaled by origin_scale and the direction, sin and cos of 2^k pi x over
+ * those 6 coordinates for k = 0..5, a constant 1 and a zero. Layers: 80 -> 64
+ * -> 64 -> 64 (ReLU, each output again followed by a constant-1 input) -> 16,
+ * of which outputs 0 and 1 are (t_near - t_shift) / t_scale and
+ * (t_far - t_shift) / t_scale. Every layer runs on the tensor cores (BF16
+ * operands, FP32 accumulation).
+ *
+ * The arrays are device memory owned by the caller:
+ *   master, adam_m, adam_v  float[TT_MLP_PARAMS]: W1 [64][80], W2 [64][80],
+ *       W3 [64][80], W4 [16][80] row-major, one after the other; the bias of
+ *       each layer is the column fed by the constant 1 (column 78 of W1,
+ *       column 64 of W2..W4). Columns fed by a zero and rows 2..15 of W4 are
+ *       never updated and must start at 0.
+ *   weights  uint16[TT_MLP_PARAMS]: the BF16 copy in the kernels' tensor-core
+ *       layout, written by tt_mlp_update and by every training step.
+ *   partial  float[partial_ctas][TT_MLP_PARTIAL]: training scratch; a step
+ *       uses ceil(n / 128 / ceil(n / 128 / SMs)) CTAs (128 for n = 65536 on
+ *       148 SMs).
+ * Status: bounded device waits report through tt_device_status(h). */
+#define TT_MLP_PARAMS 16640
+#define TT_MLP_PARTIAL 16656
+typedef struct tt_mlp {
+  uint16_t* weights;
+  float* master;
+  float* adam_m;
+  float* adam_v;
+  float* partial;
+  int partial_ctas;
+  float origin_scale; /* origins are multiplied by this before encoding */
+  float t_shift;      /* t = output * t_scale + t_shift */
+  float t_scale;
+} tt_mlp;
+
+/* One Adam step on a batch. Loss per ray: w0 e0^2 + w1 e1^2 on the scaled
+ * outputs, e = output - target, averaged over the batch; w0 = near_weight if
+ * t_near is above its target (hits would be cut off), 1 below, 0 for a ray
+ * whose t_near target is negative (no hit); w1 = far_weight if t_far is below
+ * its target (the ray would need a continuation), else 1. */
+typedef struct tt_mlp_step {
+  float lr, beta1, beta2, eps;
+  int step; /* 1-based, for Adam's bias correction */
+  float near_weight;
+  float far_weight;
+} tt_mlp_step;
+
+/* master -> weights (after initialising or loading master). */
+int tt_mlp_update(tt_tracer* h, const tt_mlp* net, void* stream);
+/* rays [n][6] (origin, direction), targets [n][2] (t_near, t_far; t_near < 0
+ * for a ray without hits), device pointers; *loss (device float, may be
+ * NULL) receives the batch's mean loss. */
+int tt_mlp_train_step(tt_tracer* h, const tt_mlp* net, const tt_mlp_step* st, const float* rays,
+                      const float* targets, int n, float* loss, void* stream);
+/* Raw predictions: out [n][2] = (t_near, t_far) for rays [n][6]. */
+int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, float* out, void* stream);
+/* Proposed intervals for the rays of up to 32 views (ray_o / ray_d of each
+ * view; other view fields ignored): intervals[i] is [2][H][W] of view i,
+ * [t_near - margin_near, t_far + margin_far], t_far = +inf when the predicted
+ * t_far + margin_far >= far_cap. */
+int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int n_views, float* const* intervals,
+                     float margin_near, float margin_far, float far_cap, void* stream);
 
 /* Forward trace that allocates nothing. No counterpart in the reference.
  *

@@ -35,5 +35,7 @@ struct or_args {
   int* rec_ids;     // [H*W, max_rec]
   int* rec_count;   // [H*W]
   float* margin;    // [H*W]
+  // optional proposed interval per ray, [2][H*W] (t_near plane, t_far plane)
+  const float* interval;
 };
 }

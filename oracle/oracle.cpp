@@ -39,6 +39,7 @@ static Inputs to_inputs(const or_args* a) {
   in.bg = a->bg;
   in.extra = a->extra;
   in.extra_len = a->extra_len;
+  in.interval = a->interval;
   return in;
 }
 

@@ -290,12 +290,31 @@ inline void trace_chunk(const Scene& sc, const RayPre& r, float tmin, float tmax
 // last_hit_t, visit them in order, re-trace from the last one. `visit`
 // receives (prim, t) for every entry at or beyond the near plane and returns
 // true to end the ray; `record` sees every entry, including near ones.
+//
+// A proposed interval [t_near, t_far] (the GPU's clipped traversal, no
+// reference counterpart) starts the march at t_near, closed, when the
+// interval holds a hit; otherwise, or when t_near is not in (0, far), the
+// march is the plain one. t_far only bounds the GPU's work: a ray that
+// reaches it unterminated goes on, so the visited hits do not depend on it.
 template <class Visit, class Record>
-inline void march(const Scene& sc, const RayPre& r, const Opts& o, Visit&& visit, Record&& record) {
+inline void march(const Scene& sc, const RayPre& r, const Opts& o, Visit&& visit, Record&& record,
+                  float t_near = 0.f, float t_far = kFar) {
   float last_hit_t = 0.f;
   Hit pl[kChunk];
+  bool clipped = false;
+  if (t_near > 0.f && t_near < kFar) {
+    Opts closed = o;
+    closed.tmin_inclusive = true;
+    const float hi = (t_far >= 0.f && t_far < kFar) ? t_far : kFar;
+    trace_chunk(sc, r, t_near, hi, closed, pl);
+    if (pl[0].id != kInvalid) {
+      trace_chunk(sc, r, t_near, kFar, closed, pl);
+      clipped = true;
+    }
+  }
   for (int guard = 0; guard < (1 << 22); ++guard) {
-    trace_chunk(sc, r, last_hit_t, kFar, o, pl);
+    if (!clipped) trace_chunk(sc, r, last_hit_t, kFar, o, pl);
+    clipped = false;
     for (int i = 0; i < kChunk; ++i) {
       const Hit h = pl[i];
       if (h.id == kInvalid) return;
@@ -326,7 +345,17 @@ struct Inputs {
   const float* bg = nullptr;
   const float* extra = nullptr;
   int extra_len = 0;
+  const float* interval = nullptr;  // optional [2][H][W] proposed [t_near, t_far] per ray
 };
+
+inline void ray_interval(const Inputs& in, int pix, float& t_near, float& t_far) {
+  t_near = 0.f;
+  t_far = kFar;
+  if (!in.interval) return;
+  const int HW = in.H * in.W;
+  t_near = in.interval[pix];
+  t_far = in.interval[HW + pix];
+}
 
 template <class R>
 inline V3<R> vert(const Inputs& in, int off) {
@@ -512,6 +541,8 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
   const float* df = in.ray_d + 3 * (size_t)pix;
   const V3<R> o = from_f<R>(of), d = from_f<R>(df);
   const RayPre rp = ray_pre(of, df);
+  float t_near, t_far;
+  ray_interval(in, pix, t_near, t_far);
   R C[3] = {0, 0, 0}, N[3] = {0, 0, 0};
   R T = 1;
   const R D = 0;  // the reference never accumulates depth in the forward pass
@@ -542,7 +573,8 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
       },
       [&](const Hit& h) {
         if (rec) rec->add(h);
-      });
+      },
+      t_near, t_far);
   for (int ch = 0; ch < 3; ++ch) out.color[ch * HW + pix] = C[ch] + T * (R)in.bg[ch];
   out.others[pix + kDepth * HW] = D;
   out.others[pix + kAlphaOff * HW] = R(1) - T;
@@ -832,6 +864,8 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
   const R dL_ddepth = (R)bi.dL_dothers[kDepth * HW + pix];
   const V3<R> dL_dnormal2D = mk<R>((R)bi.dL_dothers[(kNormal + 0) * HW + pix], (R)bi.dL_dothers[(kNormal + 1) * HW + pix],
                                    (R)bi.dL_dothers[(kNormal + 2) * HW + pix]);
+  float t_near, t_far;
+  ray_interval(in, pix, t_near, t_far);
   R C[3] = {0, 0, 0}, N[3] = {0, 0, 0};
   R D = 0, T = 1;
   march(
@@ -879,7 +913,7 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
         T = test_T;
         return false;
       },
-      [](const Hit&) {});
+      [](const Hit&) {}, t_near, t_far);
 }
 
 }  // namespace tto

@@ -38,6 +38,7 @@ class OrArgs(ctypes.Structure):
         ("colors", ctypes.c_void_p), ("others", ctypes.c_void_p),
         ("dL_dpixels", _fp), ("dL_dothers", _fp),
         ("max_rec", ctypes.c_int), ("rec_ids", _ip), ("rec_count", _ip), ("margin", _fp),
+        ("interval", _fp),
     ]
 
 
@@ -119,9 +120,21 @@ class _Runner:
         a.row_begin, a.row_end = (rows if rows is not None else (0, 0))
         return a, keep
 
+    @staticmethod
+    def _interval(a, keep, interval):
+        """Optional proposed interval per ray, [2, H, W] (t_near, t_far)."""
+        if interval is None:
+            return
+        keep["interval"] = _c(interval, np.float32)
+        if keep["interval"].shape != (2, a.H, a.W):
+            raise ValueError("interval must be [2, H, W]")
+        a.interval = _ptr(keep["interval"])
+
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
-                canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None):
+                canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None,
+                interval=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, extra, variant, tmin_inclusive, canonical, exact, nthreads, rows)
+        self._interval(a, keep, interval)
         dt = np.float32 if precision == 32 else np.float64
         H, W, P = a.H, a.W, scene.P
         scaling = np.zeros(P, dt) if scaling is None else _c(scaling, dt).reshape(-1).copy()
@@ -149,8 +162,9 @@ class _Runner:
         return FwdResult(color, others, scaling, density, maxb, rec_ids, rec_count, margin)
 
     def backward(self, scene, ray_o, ray_d, colors, others, dL_dpixels, dL_dothers, bg=None, precision=32,
-                 tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None):
+                 tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, None, 0, tmin_inclusive, canonical, exact, nthreads, rows)
+        self._interval(a, keep, interval)
         dt = np.float32 if precision == 32 else np.float64
         keep["colors"] = _c(colors, dt)
         keep["others"] = _c(others, dt)

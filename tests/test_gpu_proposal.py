@@ -1,0 +1,164 @@
+"""Proposal network on the tensor cores (tt_mlp_*) against the numpy oracle
+(oracle/proposal.py), and the learned-interval trace against the plain one.
+
+* inference: outputs within BF16-rounding noise of the oracle, which rounds
+  at the same points (inputs, weights, activations);
+* training step: the kernels' weight gradients (the per-CTA sums left in the
+  partial buffer) within 2 % (L2) of the oracle's, the loss within 1e-3, and
+  the Adam update exact to FP32 rounding;
+* training on the tracer's own records lowers the loss and gives intervals
+  that miss few hits; the clipped trace then reproduces the plain image
+  within a small RMSE and with fewer node visits (the trained network's gain),
+  and exactly when the margins cover every ray.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from diff_tritracer import _C, proposal, scenes  # noqa: E402
+from gpu_helpers import DEV, T, rel_norm  # noqa: E402
+from oracle import proposal as OP  # noqa: E402
+
+
+def random_rays(n, seed):
+    rng = np.random.default_rng(seed)
+    o = rng.normal(0, 1, (n, 3))
+    o = 3 * o / np.linalg.norm(o, axis=1, keepdims=True)
+    d = -o / 3 + rng.normal(0, 0.2, (n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([o, d], 1).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def tracer():
+    return _C.OptixTracer("", "forward.ptx", "backward.ptx")
+
+
+def make_prop(tracer, seed=3):
+    p = proposal.Proposal(tracer, seed=seed)
+    # a non-trivial network: perturb the output layer and the biases too
+    rng = np.random.default_rng(seed)
+    m = p.master.cpu().numpy()
+    W = [m[proposal.OFF[l]:proposal.OFF[l] + proposal.ROWS[l] * 80].reshape(proposal.ROWS[l], 80) for l in range(4)]
+    W[0][:, 78] = rng.normal(0, 0.1, 64)
+    for l in (1, 2):
+        W[l][:, 64] = rng.normal(0, 0.1, 64)
+    W[3][:2, :64] = rng.normal(0, 0.3, (2, 64))
+    W[3][:2, 64] = [0.2, 0.6]
+    p.master.copy_(torch.from_numpy(m))
+    p.update()
+    return p
+
+
+def test_inference_matches_oracle(tracer):
+    p = make_prop(tracer)
+    rays = random_rays(3000, 1)  # not a multiple of the 128-ray tile
+    got = p.predict(T(rays)).cpu().numpy()
+    tracer.device_status()
+    ref = OP.predict(p.master.cpu().numpy(), rays, p.origin_scale, p.t_shift, p.t_scale)
+    err = np.abs(got - ref)
+    print("inference |err| mean %.2e max %.2e, output spread %.2e" % (err.mean(), err.max(), ref.std()))
+    assert ref.std() > 0.1
+    assert err.mean() < 2e-3 and err.max() < 3e-2
+
+
+def test_intervals_layout(tracer):
+    p = make_prop(tracer)
+    views = [scenes.camera_rays(scenes.look_at_camera([0.3, 0.4, 3.0], H, W, fov_deg=20.0)) for H, W in
+             ((20, 24), (7, 130))]
+    ivs = p.intervals([(T(ro), T(rd)) for ro, rd in views], margin_near=0.1, margin_far=0.2, far_cap=3.4)
+    for (ro, rd), iv in zip(views, ivs):
+        rays = np.concatenate([ro.reshape(-1, 3), rd.reshape(-1, 3)], 1)
+        raw = p.predict(T(rays)).cpu().numpy()
+        got = iv.cpu().numpy().reshape(2, -1)
+        np.testing.assert_allclose(got[0], raw[:, 0] - 0.1, rtol=0, atol=1e-5)
+        far = raw[:, 1] + 0.2
+        np.testing.assert_allclose(got[1], np.where(far >= 3.4, np.inf, far), rtol=0, atol=1e-5)
+
+
+def test_train_step_matches_oracle(tracer):
+    p = make_prop(tracer)
+    n = 70000  # several CTAs, a partial last tile
+    rays = random_rays(n, 2)
+    rng = np.random.default_rng(5)
+    targets = np.stack([rng.uniform(2.0, 3.0, n), rng.uniform(3.0, 4.5, n)], 1).astype(np.float32)
+    targets[::7, 0] = -1.0  # rays without hits: no t_near term
+    m0 = p.master.cpu().numpy().astype(np.float64)
+    loss = torch.zeros(1, device=DEV)
+    p.train_step(T(rays), T(targets), lr=1e-3, near_weight=8.0, far_weight=3.0, loss_out=loss)
+    torch.cuda.synchronize()
+    tracer.device_status()
+    ntiles = (n + 127) // 128
+    per = -(-ntiles // p.partial.shape[0])
+    ctas = -(-ntiles // per)
+    g_gpu = p.partial[:ctas, :proposal.PARAMS].sum(0).double().cpu().numpy() / n
+    l_ref, g_ref = OP.loss_and_grad(m0, rays, targets, p.origin_scale, p.t_shift, p.t_scale, 8.0, 3.0)
+    e = rel_norm(g_gpu, g_ref)
+    print(f"loss gpu {loss.item():.6f} oracle {l_ref:.6f}; gradient rel L2 {e:.2e}")
+    assert abs(loss.item() - l_ref) <= 1e-3 * l_ref
+    assert e < 2e-2
+    # per layer too (the small output layer must not hide in the total)
+    for l in range(4):
+        sl = slice(proposal.OFF[l], proposal.OFF[l] + proposal.ROWS[l] * 80)
+        assert rel_norm(g_gpu[sl], g_ref[sl]) < 3e-2, l
+    # Adam, first step: m = 0.1 g, v = 0.001 g^2 -> update = lr * g / (|g| + eps / sqrt(1000)...)
+    w1 = p.master.cpu().numpy().astype(np.float64)
+    want, _, _ = OP.adam(m0, np.zeros_like(m0), np.zeros_like(m0), g_gpu.astype(np.float32).astype(np.float64), 1,
+                         1e-3)
+    np.testing.assert_allclose(w1, want, rtol=0, atol=2e-7)
+
+
+def scene_dict(sc):
+    return dict(verts=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), npts=T(sc.num_points), cums=T(sc.cumsum),
+                shs=T(sc.shs), opac=T(sc.opacities), P=sc.P)
+
+
+def test_learned_intervals_on_tracer_records():
+    sc = scenes.make_scene(20000, seed=11, center_std=0.3, edge_range=(0.02, 0.1))
+    s = scene_dict(sc)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.build_tri_accel(s["verts"], s["cums"], sc.P, True)
+    cams = scenes.sphere_cameras(40, 96, 96, seed=4)
+    views = [tuple(T(a) for a in scenes.camera_rays(c)) for c in cams]
+    train, held = views[:36], views[36:]
+    p = proposal.Proposal(tr, seed=0)
+    rays, targets, far_target = proposal.collect(tr, s, train)
+    p.far_target, p.far_cap = far_target, far_target - 0.5
+    losses = proposal.fit(p, rays, targets, epochs=30, batch=16384, lr=3e-3)
+    tr.device_status()
+    first, last = losses[:5].mean(), losses[-5:].mean()
+    print(f"loss {first:.4f} -> {last:.4f} over {len(losses)} steps")
+    assert last < 0.2 * first
+    hrays, htargets, _ = proposal.collect(tr, s, held, far_target=far_target)
+    st = proposal.interval_stats(p.predict(hrays), htargets, far_target, 0.1, 0.1, p.far_cap)
+    print("held-out", st)
+    assert st["near_miss"] < 0.05
+    # clipped trace vs plain on the held-out views
+    bg = torch.zeros(3, device=DEV)
+    ivs = p.intervals(held, margin_near=0.1, margin_far=0.1)
+    def render(intervals):
+        outs, _ = tr.trace_forward_views(held, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3,
+                                         s["opac"], torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), bg,
+                                         2, intervals=intervals)
+        return torch.stack([c for c, _ in outs]).cpu().numpy()
+    tr.reset_stats()
+    plain = render(None)
+    st_plain = tr.stats()
+    tr.reset_stats()
+    clipped = render(ivs)
+    st_clip = tr.stats()
+    rmse = float(np.sqrt(np.mean((clipped - plain) ** 2)))
+    print(f"image RMSE clipped vs plain {rmse:.2e}; node visits/ray {st_plain['node_visits'] / st_plain['rays']:.1f}"
+          f" -> {st_clip['node_visits'] / st_clip['rays']:.1f}; continuations {st_clip['interval_continuations']},"
+          f" re-traces {st_clip['interval_retraces']}")
+    assert rmse < 1e-2  # small scene, short training; the benchmark states the real figure
+    assert st_clip["node_visits"] < st_plain["node_visits"]  # what the network gains
+    # margins that cover every ray reproduce the plain image exactly
+    wide = p.intervals(held, margin_near=100.0, margin_far=0.0)
+    np.testing.assert_array_equal(render(wide), plain)
+    tr.device_status()
