@@ -461,6 +461,9 @@ int tt_mlp_train_step(tt_tracer* h, const tt_mlp* net, const tt_mlp_step* st, co
   p.origin_scale = net->origin_scale;
   p.t_shift = net->t_shift;
   p.inv_t_scale = 1.0f / net->t_scale;
+  p.cx = net->center[0];
+  p.cy = net->center[1];
+  p.cz = net->center[2];
   p.near_weight = st->near_weight;
   p.far_weight = st->far_weight;
   p.partial = net->partial;
@@ -494,6 +497,9 @@ static int mlp_infer(tt_tracer* h, const tt_mlp* net, tt::mlp::InferParams& p, f
   p.origin_scale = net->origin_scale;
   p.t_shift = net->t_shift;
   p.t_scale = net->t_scale;
+  p.cx = net->center[0];
+  p.cy = net->center[1];
+  p.cz = net->center[2];
   p.margin_near = margin_near;
   p.margin_far = margin_far;
   p.far_cap = far_cap;

@@ -130,9 +130,20 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// The 80 inputs of one ray as 40 BF16 pairs: the 6 coordinates (origin
-// scaled), then for k = 0..5 the sines and the cosines of 2^k pi x over the 6
-// coordinates, then the constant 1 (bias input) and a zero.
+// Distance s along the ray from its origin to the closest approach of its
+// line to the centre c: the network sees o + s d (centred) and predicts t - s.
+__device__ __forceinline__ float closest_offset(float3& o, float3 d, float cx, float cy, float cz) {
+  o = make_float3(o.x - cx, o.y - cy, o.z - cz);
+  const float dd = d.x * d.x + d.y * d.y + d.z * d.z;
+  const float s = dd > 0.f ? -(o.x * d.x + o.y * d.y + o.z * d.z) / dd : 0.f;
+  o = make_float3(fmaf(s, d.x, o.x), fmaf(s, d.y, o.y), fmaf(s, d.z, o.z));
+  return s;
+}
+
+// The 80 inputs of one ray as 40 BF16 pairs: the 6 coordinates (centred
+// closest-approach origin, scaled, and direction), then for k = 0..5 the sines
+// and the cosines of 2^k pi x over the 6 coordinates, then the constant 1
+// (bias input) and a zero.
 __device__ __forceinline__ void encode(float3 o, float3 d, float scale, uint32_t (&x)[40]) {
   float f[kIn];
   const float v[6] = {o.x * scale, o.y * scale, o.z * scale, d.x, d.y, d.z};
@@ -250,6 +261,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ I
       o = make_float3(__ldg(po), __ldg(po + 1), __ldg(po + 2));
       d = make_float3(__ldg(pd), __ldg(pd + 1), __ldg(pd + 2));
     }
+    const float s_off = closest_offset(o, d, p.cx, p.cy, p.cz);
     uint32_t x[40];
     encode(o, d, p.origin_scale, x);
     put_row<10>(act, tid, x);
@@ -275,9 +287,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ I
         float y[16];
         tmem_ld16(lane_base, y);
         if (valid) {
-          const float t0 = fmaf(y[0], p.t_scale, p.t_shift) - p.margin_near;
-          float t1 = fmaf(y[1], p.t_scale, p.t_shift) + p.margin_far;
-          if (t1 >= p.far_cap) t1 = INFINITY;
+          // far_cap is measured from the closest approach, like the outputs
+          const float t0 = fmaf(y[0], p.t_scale, p.t_shift) + s_off - p.margin_near;
+          const float f1 = fmaf(y[1], p.t_scale, p.t_shift) + p.margin_far;
+          const float t1 = f1 >= p.far_cap ? INFINITY : f1 + s_off;
           rs.out0[(size_t)r * rs.ostride] = t0;
           rs.out1[(size_t)r * rs.ostride] = t1;
         }
@@ -340,10 +353,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_train(const __grid_constant__ T
       const float* pr = p.rays + (size_t)row * 6;
       o = make_float3(__ldg(pr), __ldg(pr + 1), __ldg(pr + 2));
       d = make_float3(__ldg(pr + 3), __ldg(pr + 4), __ldg(pr + 5));
+    }
+    const float s_off = closest_offset(o, d, p.cx, p.cy, p.cz);
+    if (valid) {
       const float t_near = __ldg(p.targets + 2 * (size_t)row);
       has_near = t_near >= 0.f;
-      tg0 = (t_near - p.t_shift) * p.inv_t_scale;
-      tg1 = (__ldg(p.targets + 2 * (size_t)row + 1) - p.t_shift) * p.inv_t_scale;
+      tg0 = (t_near - s_off - p.t_shift) * p.inv_t_scale;
+      tg1 = (__ldg(p.targets + 2 * (size_t)row + 1) - s_off - p.t_shift) * p.inv_t_scale;
     }
     uint32_t x[40];
     encode(o, d, p.origin_scale, x);

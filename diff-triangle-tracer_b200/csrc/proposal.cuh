@@ -1,12 +1,16 @@
 // Launch interface of the proposal network kernels (proposal.cu).
 //
 // The network maps a ray (origin, direction) to the interval [t_near, t_far]
-// of its hits: 80 encoded inputs (the 6 raw coordinates, sin / cos of
-// 2^k pi x for k = 0..5 over the 6 coordinates, a constant 1 standing for the
-// bias, one zero), three hidden layers of 64 ReLU units (each again followed
-// by a constant-1 input) and a linear output layer of 16 rows of which the
-// first two are used. Every contraction runs on the tensor cores
-// (tcgen05.mma, BF16 operands, FP32 accumulators in tensor memory).
+// of its hits. The origin is first moved along the ray to its closest
+// approach to the scene centre (o' = o + s d, s = -(o - c).d / d.d), so the
+// inputs depend on the ray's line only and rays of unseen cameras look like
+// the training rays; the outputs are t - s. 80 encoded inputs: the 6
+// coordinates (o' - c scaled, d), sin / cos of 2^k pi x for k = 0..5 over
+// them, a constant 1 standing for the bias, one zero; three hidden layers of
+// 64 ReLU units (each again followed by a constant-1 input) and a linear
+// output layer of 16 rows of which the first two are used. Every contraction
+// runs on the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulators in
+// tensor memory).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,7 +47,10 @@ struct InferParams {
   int nsets, ntiles;
   RaySet sets[kMaxViews];
   float origin_scale, t_shift, t_scale;
-  float margin_near, margin_far, far_cap;  // interval = [t0 - near, t1 + far]; t1 >= far_cap -> +inf
+  float cx, cy, cz;  // scene centre
+  // interval = [t0 - margin_near, t1 + margin_far]; t_far = +inf when
+  // t1 + margin_far - s >= far_cap (measured from the closest approach)
+  float margin_near, margin_far, far_cap;
   int* status;
 };
 
@@ -53,6 +60,7 @@ struct TrainParams {
   const float* targets;  // [n][2]: t_near (< 0: no t_near target), t_far (t units)
   int n, ntiles, tiles_per_cta;
   float origin_scale, t_shift, inv_t_scale;
+  float cx, cy, cz;
   float near_weight;  // loss weight of a t_near above its target (hits cut off)
   float far_weight;   // loss weight of a t_far below its target (a continuation)
   float* partial;  // [gridDim.x][kPartial]: dL/dW sums (unscaled) and the loss sum

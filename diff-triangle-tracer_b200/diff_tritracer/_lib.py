@@ -91,7 +91,7 @@ TT_MLP_PARTIAL = 16656
 class TtMlp(ctypes.Structure):
     _fields_ = [("weights", _vp), ("master", _vp), ("adam_m", _vp), ("adam_v", _vp), ("partial", _vp),
                 ("partial_ctas", ctypes.c_int), ("origin_scale", ctypes.c_float), ("t_shift", ctypes.c_float),
-                ("t_scale", ctypes.c_float)]
+                ("t_scale", ctypes.c_float), ("center", ctypes.c_float * 3)]
 
 
 class TtMlpStep(ctypes.Structure):

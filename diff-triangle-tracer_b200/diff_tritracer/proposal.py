@@ -8,19 +8,26 @@ and its inference run in the library's tensor-core kernels (tt_mlp_*); this
 module owns the parameter tensors and drives data collection, training,
 validation of the margins and the clipped trace.
 
+The network sees each ray's line only: the origin is moved along the ray
+to its closest approach to the scene centre (o' = o + s d) and the outputs
+are t - s, so rays of cameras it never saw look like its training rays.
+
 Training targets come from the plain tracer itself: a forward with hit
 records gives each ray's first visited hit t_first, its last visited hit
 t_last and whether it terminated on the transmittance cut-off. Targets:
 t_near = t_first (-1 for a ray without hits: no t_near term), t_far = t_last
-for a terminated ray, else `far_target` (no far clip: the ray runs to the end
-of the scene anyway). A t_near above its target would cut hits off and
-changes the image, so it weighs `near_weight` times more; a t_far below its
+for a terminated ray, else s + `far_target` (no far clip: the ray runs to the
+end of the scene anyway). A t_near above its target would cut hits off and
+change the image, so it weighs `near_weight` times more; a t_far below its
 target only costs a continuation and weighs `far_weight`.
 
 At trace time an interval is [t_near - margin_near, t_far + margin_far], with
-t_far = +inf when it reaches `far_cap`. A ray whose interval is too short at
-the far end continues beyond it and one with no hit inside is traced again
-(both exact); only a t_near beyond the ray's first hits changes the result.
+t_far = +inf when t_far + margin_far - s reaches `far_cap`. A ray whose
+interval is too short at the far end continues beyond it and one with no hit
+inside is traced again (both exact); only a t_near beyond the ray's first
+hits changes the result. On triangle clouds the first hit of a ray is too
+erratic to predict within a safe margin, so the default margin_near switches
+the near clip off and the far clip carries the gain.
 """
 from __future__ import annotations
 
@@ -34,6 +41,7 @@ from . import _lib
 from ._lib import check, lib
 
 PARAMS = _lib.TT_MLP_PARAMS
+NO_NEAR_CLIP = 1.0e4  # a margin_near that puts every t_near before the ray origin
 PARTIAL = _lib.TT_MLP_PARTIAL
 IN, HID, OUT_ROWS = 80, 64, 16
 ROWS = (HID, HID, HID, OUT_ROWS)
@@ -68,7 +76,7 @@ class Proposal:
     device, driven through the tracer handle `tracer` (an OptixTracer, for
     its error reporting and status word)."""
 
-    def __init__(self, tracer, origin_scale=1.0 / 3.0, t_shift=3.0, t_scale=1.0, seed=0):
+    def __init__(self, tracer, origin_scale=1.0 / 3.0, t_shift=0.0, t_scale=1.0, center=(0.0, 0.0, 0.0), seed=0):
         self.tracer = tracer
         dev = tracer.device
         self.device = dev
@@ -79,10 +87,11 @@ class Proposal:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         self.partial = torch.zeros((sms, PARTIAL), dtype=torch.float32, device=dev)
         self.origin_scale, self.t_shift, self.t_scale = float(origin_scale), float(t_shift), float(t_scale)
+        self.center = tuple(float(c) for c in center)
         self.steps = 0
-        self.far_target = 6.0
-        self.far_cap = 5.0
-        self.margin_near = 0.05
+        self.far_target = 3.0   # t - s of "no far clip"
+        self.far_cap = 2.5      # t_far - s beyond which no far clip is applied
+        self.margin_near = NO_NEAR_CLIP
         self.margin_far = 0.05
         self.update()
 
@@ -93,6 +102,7 @@ class Proposal:
         n.adam_m, n.adam_v, n.partial = _ptr(self.adam_m), _ptr(self.adam_v), _ptr(self.partial)
         n.partial_ctas = int(self.partial.shape[0])
         n.origin_scale, n.t_shift, n.t_scale = self.origin_scale, self.t_shift, self.t_scale
+        n.center[0], n.center[1], n.center[2] = self.center
         return n
 
     def update(self):
@@ -153,31 +163,40 @@ class Proposal:
     # -------------------------------------------------------------- state
     def state_dict(self):
         return {"master": self.master.clone(), "origin_scale": self.origin_scale, "t_shift": self.t_shift,
-                "t_scale": self.t_scale, "far_target": self.far_target, "far_cap": self.far_cap,
-                "margin_near": self.margin_near, "margin_far": self.margin_far}
+                "t_scale": self.t_scale, "center": self.center, "far_target": self.far_target,
+                "far_cap": self.far_cap, "margin_near": self.margin_near, "margin_far": self.margin_far}
 
     def load_state_dict(self, d):
         self.master.copy_(d["master"].to(self.device))
         for k in ("origin_scale", "t_shift", "t_scale", "far_target", "far_cap", "margin_near", "margin_far"):
             setattr(self, k, float(d[k]))
+        self.center = tuple(float(c) for c in d["center"])
         self.update()
+
+    def offsets(self, rays):
+        """s per ray [n, 6]: distance from the origin to the closest approach."""
+        o = rays[:, :3] - torch.tensor(self.center, device=rays.device)
+        d = rays[:, 3:6]
+        return -(o * d).sum(1) / (d * d).sum(1)
 
 
 # ------------------------------------------------------------------ data
-def targets_from_record(rec, far_target):
+def targets_from_record(rec, s, far_target):
     """Training targets [n, 2] from hit records [3, n] (t_first, t_last,
-    terminated) of the plain tracer."""
+    terminated) of the plain tracer; s [n] are the rays' closest-approach
+    offsets and far_target the t - s of "no far clip"."""
     t_first, t_last, term = rec[0], rec[1], rec[2]
     hit = torch.isfinite(t_first)
     near = torch.where(hit, t_first, torch.full_like(t_first, -1.0))
-    far = torch.where(hit & (term > 0.5), t_last, torch.full_like(t_last, far_target))
+    far = torch.where(hit & (term > 0.5), t_last, s + far_target)
     return torch.stack([near, far], 1)
 
 
-def collect(tracer, scene, views, far_target=None, bg=None):
+def collect(prop, tracer, scene, views, far_target=None, bg=None):
     """Traces `views` (list of (ray_o, ray_d) [H, W, 3]) with the plain
     tracer and returns (rays [N, 6], targets [N, 2], far_target). `scene` is
-    a dict of device tensors: verts, sigma, npts, cums, shs, opac, P."""
+    a dict of device tensors: verts, sigma, npts, cums, shs, opac, P. Without
+    a far_target, 0.5 beyond the last hit seen (relative to s) is used."""
     dev = tracer.device
     bg = torch.zeros(3, device=dev) if bg is None else bg
     rays, recs = [], []
@@ -193,10 +212,11 @@ def collect(tracer, scene, views, far_target=None, bg=None):
             recs.append(rec.reshape(3, -1))
     rays = torch.cat(rays, 0).contiguous()
     rec = torch.cat(recs, 1)
+    s = prop.offsets(rays)
     if far_target is None:
         hit = torch.isfinite(rec[1])
-        far_target = float(rec[1][hit].max().item()) + 0.5 if bool(hit.any()) else 6.0
-    return rays, targets_from_record(rec, far_target).contiguous(), far_target
+        far_target = float((rec[1] - s)[hit].max().item()) + 0.5 if bool(hit.any()) else 3.0
+    return rays, targets_from_record(rec, s, far_target).contiguous(), far_target
 
 
 def fit(prop, rays, targets, epochs=20, batch=65536, lr=1e-3, near_weight=8.0, far_weight=3.0, seed=0,
@@ -224,18 +244,27 @@ def fit(prop, rays, targets, epochs=20, batch=65536, lr=1e-3, near_weight=8.0, f
     return losses.cpu().numpy()
 
 
-def interval_stats(pred, targets, far_target, margin_near, margin_far, far_cap):
-    """Miss rates of intervals [t_near - m_n, t_far + m_f] against targets:
-    near misses (t_near beyond the first hit: hits skipped) and far misses
-    (a terminated ray's last hit beyond t_far: continuation)."""
-    tn = pred[:, 0] - margin_near
-    tf = pred[:, 1] + margin_far
-    tf = torch.where(tf >= far_cap, torch.full_like(tf, float("inf")), tf)
+def interval_stats(prop, rays, targets, margin_near=None, margin_far=None, far_cap=None):
+    """How intervals [t_near - m_n, t_far + m_f] of `prop` fit the targets:
+    near misses (t_near beyond the first hit: hits skipped, among rays with
+    hits), far misses (a terminated ray's last hit beyond a finite t_far: a
+    continuation, among terminated rays), false far clips (a ray that does not
+    terminate given a finite t_far: a continuation, among those rays) and the
+    share of terminated rays whose t_far is finite."""
+    mn = prop.margin_near if margin_near is None else margin_near
+    mf = prop.margin_far if margin_far is None else margin_far
+    cap = prop.far_cap if far_cap is None else far_cap
+    pred = prop.predict(rays)
+    s = prop.offsets(rays)
+    tn = pred[:, 0] - mn
+    clip = (pred[:, 1] - s + mf) < cap
     hit = targets[:, 0] >= 0
-    term = targets[:, 1] < far_target
-    near_miss = (hit & (tn > targets[:, 0])).float().mean().item()
-    far_miss = (term & (tf < targets[:, 1])).float().mean().item()
-    clipped_far = torch.isfinite(tf).float().mean().item()
-    return {"near_miss": near_miss, "far_miss": far_miss, "far_clipped": clipped_far,
-            "near_err": (pred[:, 0] - targets[:, 0])[hit].abs().mean().item(),
-            "far_err": (pred[:, 1] - targets[:, 1])[term].abs().mean().item() if bool(term.any()) else 0.0}
+    term = (targets[:, 1] - s) < prop.far_target - 1e-3
+    f = lambda x: float(x.float().mean().item()) if x.numel() else 0.0
+    return {"near_miss": f((tn > targets[:, 0])[hit]),
+            "far_miss": f((clip & (pred[:, 1] + mf < targets[:, 1]))[term]),
+            "false_far_clip": f(clip[~term]),
+            "far_clipped": f(clip[term]),
+            "far_err_median": float((pred[:, 1] - targets[:, 1])[term].abs().median().item()) if bool(term.any())
+            else 0.0,
+            "terminated": f(term)}

@@ -239,13 +239,15 @@ int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, i
 /* ---------------------------------------------------------------------------
  * Proposal network (no reference counterpart). A small MLP maps each ray to
  * the interval [t_near, t_far] holding the hits its march visits; the trace
- * is clipped to it through tt_view.interval. Inputs (80): the ray origin
- * scaled by origin_scale and the direction, sin and cos of 2^k pi x over
- * those 6 coordinates for k = 0..5, a constant 1 and a zero. Layers: 80 -> 64
- * -> 64 -> 64 (ReLU, each output again followed by a constant-1 input) -> 16,
- * of which outputs 0 and 1 are (t_near - t_shift) / t_scale and
- * (t_far - t_shift) / t_scale. Every layer runs on the tensor cores (BF16
- * operands, FP32 accumulation).
+ * is clipped to it through tt_view.interval. The ray origin o is first
+ * moved along the ray to the closest approach of the ray's line to `center`
+ * (o' = o + s d, s = -(o - center).d / d.d), so the inputs depend on the line
+ * only. Inputs (80): (o' - center) * origin_scale and the direction, sin and
+ * cos of 2^k pi x over those 6 coordinates for k = 0..5, a constant 1 and a
+ * zero. Layers: 80 -> 64 -> 64 -> 64 (ReLU, each output again followed by a
+ * constant-1 input) -> 16, of which outputs 0 and 1 are
+ * (t_near - s - t_shift) / t_scale and (t_far - s - t_shift) / t_scale.
+ * Every layer runs on the tensor cores (BF16 operands, FP32 accumulation).
  *
  * The arrays are device memory owned by the caller:
  *   master, adam_m, adam_v  float[TT_MLP_PARAMS]: W1 [64][80], W2 [64][80],
@@ -268,9 +270,10 @@ typedef struct tt_mlp {
   float* adam_v;
   float* partial;
   int partial_ctas;
-  float origin_scale; /* origins are multiplied by this before encoding */
-  float t_shift;      /* t = output * t_scale + t_shift */
+  float origin_scale; /* closest-approach origins are multiplied by this before encoding */
+  float t_shift;      /* t = output * t_scale + t_shift + s */
   float t_scale;
+  float center[3];    /* scene centre */
 } tt_mlp;
 
 /* One Adam step on a batch. Loss per ray: w0 e0^2 + w1 e1^2 on the scaled
@@ -296,8 +299,9 @@ int tt_mlp_train_step(tt_tracer* h, const tt_mlp* net, const tt_mlp_step* st, co
 int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, float* out, void* stream);
 /* Proposed intervals for the rays of up to 32 views (ray_o / ray_d of each
  * view; other view fields ignored): intervals[i] is [2][H][W] of view i,
- * [t_near - margin_near, t_far + margin_far], t_far = +inf when the predicted
- * t_far + margin_far >= far_cap. */
+ * [t_near - margin_near, t_far + margin_far], with t_far = +inf when
+ * t_far + margin_far - s >= far_cap (far_cap is measured from the ray's
+ * closest approach to the centre). */
 int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int n_views, float* const* intervals,
                      float margin_near, float margin_far, float far_cap, void* stream);
 

@@ -3,8 +3,10 @@ diff-triangle-tracer_b200/csrc/proposal.cu (no counterpart in the reference,
 which traces every ray to the far plane). Used only by tests to check the
 tensor-core kernels.
 
-Network: 80 inputs (origin * origin_scale and direction, sin / cos of
-2^k pi x for k = 0..5 over those 6 coordinates, a constant 1, a zero) ->
+Network: the ray origin o is moved along the ray to the closest approach of
+its line to the centre c (o' = o + s d, s = -(o - c).d / d.d); 80 inputs
+((o' - c) * origin_scale and the direction, sin / cos of 2^k pi x for
+k = 0..5 over those 6 coordinates, a constant 1, a zero) ->
 64 -> 64 -> 64 (ReLU, each followed by a constant-1 input) -> 16 outputs (the
 first two used). Weights W1 [64][80], W2 [64][80], W3 [64][80], W4 [16][80]
 flattened in that order; a layer's bias is the weight column fed by the
@@ -37,10 +39,20 @@ def layers(params):
     return [p[OFF[l]:OFF[l] + ROWS[l] * IN].reshape(ROWS[l], IN) for l in range(4)]
 
 
-def encode(rays, origin_scale):
+def closest_offset(rays, center=(0.0, 0.0, 0.0)):
+    """s of each ray and its centred closest-approach origin o + s d - c."""
+    rays = np.asarray(rays, np.float64)
+    o = rays[:, :3] - np.asarray(center, np.float64)
+    d = rays[:, 3:6]
+    s = -np.sum(o * d, 1) / np.sum(d * d, 1)
+    return s, o + s[:, None] * d
+
+
+def encode(rays, origin_scale, center=(0.0, 0.0, 0.0)):
     """rays [n, 6] -> inputs [n, 80] (float64)."""
     rays = np.asarray(rays, np.float64)
-    v = np.concatenate([rays[:, :3] * np.float32(origin_scale), rays[:, 3:6]], 1).astype(np.float32).astype(np.float64)
+    _, o = closest_offset(rays, center)
+    v = np.concatenate([o * origin_scale, rays[:, 3:6]], 1).astype(np.float32).astype(np.float64)
     f = [v]
     for k in range(6):
         a = v * float(1 << k)
@@ -61,10 +73,10 @@ def _ext(h):
     return np.concatenate([h, np.ones((n, 1)), np.zeros((n, IN - HID - 1))], 1)
 
 
-def forward(params, rays, origin_scale, bf16_ops=True):
+def forward(params, rays, origin_scale, center=(0.0, 0.0, 0.0), bf16_ops=True):
     """Returns (raw outputs [n, 16], activations [act0..act3])."""
     W = [_r(w, bf16_ops) for w in layers(params)]
-    act = [_r(encode(rays, origin_scale), bf16_ops)]
+    act = [_r(encode(rays, origin_scale, center), bf16_ops)]
     for l in range(3):
         z = act[l] @ W[l].T
         act.append(_ext(_r(np.maximum(z, 0.0), bf16_ops)))
@@ -72,21 +84,25 @@ def forward(params, rays, origin_scale, bf16_ops=True):
     return y, act
 
 
-def predict(params, rays, origin_scale, t_shift, t_scale, bf16_ops=True):
-    y, _ = forward(params, rays, origin_scale, bf16_ops)
-    return y[:, :2] * t_scale + t_shift
+def predict(params, rays, origin_scale, t_shift, t_scale, center=(0.0, 0.0, 0.0), bf16_ops=True):
+    """(t_near, t_far) [n, 2] in t along the ray from its origin."""
+    y, _ = forward(params, rays, origin_scale, center, bf16_ops)
+    s, _ = closest_offset(rays, center)
+    return y[:, :2] * t_scale + t_shift + s[:, None]
 
 
-def loss_and_grad(params, rays, targets, origin_scale, t_shift, t_scale, near_weight, far_weight, bf16_ops=True):
+def loss_and_grad(params, rays, targets, origin_scale, t_shift, t_scale, near_weight, far_weight,
+                  center=(0.0, 0.0, 0.0), bf16_ops=True):
     """Mean asymmetric loss and its gradient with respect to the flattened
     parameters (the kernels' training step before Adam). A t_near above its
     target weighs near_weight, a t_far below its target far_weight; a ray
     whose t_near target is negative (no hit) has no t_near term."""
     W = [_r(w, bf16_ops) for w in layers(params)]
-    y, act = forward(params, rays, origin_scale, bf16_ops)
+    y, act = forward(params, rays, origin_scale, center, bf16_ops)
     n = rays.shape[0]
     raw = np.asarray(targets, np.float32).astype(np.float64)
-    tg = (raw - t_shift) / t_scale
+    s, _ = closest_offset(rays, center)
+    tg = (raw - s[:, None] - t_shift) / t_scale
     e0, e1 = y[:, 0] - tg[:, 0], y[:, 1] - tg[:, 1]
     w0 = np.where(raw[:, 0] >= 0, np.where(e0 > 0, near_weight, 1.0), 0.0)
     w1 = np.where(e1 < 0, far_weight, 1.0)

@@ -6,10 +6,10 @@
 * training step: the kernels' weight gradients (the per-CTA sums left in the
   partial buffer) within 2 % (L2) of the oracle's, the loss within 1e-3, and
   the Adam update exact to FP32 rounding;
-* training on the tracer's own records lowers the loss and gives intervals
-  that miss few hits; the clipped trace then reproduces the plain image
-  within a small RMSE and with fewer node visits (the trained network's gain),
-  and exactly when the margins cover every ray.
+* training on the tracer's own records lowers the loss; on held-out views
+  the far clip of the learned intervals leaves the image bit-identical to the
+  plain trace (a short interval only costs a continuation); the counters
+  show what the clip saves and what its continuations cost.
 """
 import numpy as np
 import pytest
@@ -40,7 +40,7 @@ def tracer():
 
 
 def make_prop(tracer, seed=3):
-    p = proposal.Proposal(tracer, seed=seed)
+    p = proposal.Proposal(tracer, seed=seed, center=(0.1, -0.2, 0.05))
     # a non-trivial network: perturb the output layer and the biases too
     rng = np.random.default_rng(seed)
     m = p.master.cpu().numpy()
@@ -60,7 +60,7 @@ def test_inference_matches_oracle(tracer):
     rays = random_rays(3000, 1)  # not a multiple of the 128-ray tile
     got = p.predict(T(rays)).cpu().numpy()
     tracer.device_status()
-    ref = OP.predict(p.master.cpu().numpy(), rays, p.origin_scale, p.t_shift, p.t_scale)
+    ref = OP.predict(p.master.cpu().numpy(), rays, p.origin_scale, p.t_shift, p.t_scale, p.center)
     err = np.abs(got - ref)
     print("inference |err| mean %.2e max %.2e, output spread %.2e" % (err.mean(), err.max(), ref.std()))
     assert ref.std() > 0.1
@@ -71,14 +71,22 @@ def test_intervals_layout(tracer):
     p = make_prop(tracer)
     views = [scenes.camera_rays(scenes.look_at_camera([0.3, 0.4, 3.0], H, W, fov_deg=20.0)) for H, W in
              ((20, 24), (7, 130))]
-    ivs = p.intervals([(T(ro), T(rd)) for ro, rd in views], margin_near=0.1, margin_far=0.2, far_cap=3.4)
+    cap = 0.9
+    ivs = p.intervals([(T(ro), T(rd)) for ro, rd in views], margin_near=0.1, margin_far=0.2, far_cap=cap)
+    n_inf = n_all = 0
     for (ro, rd), iv in zip(views, ivs):
         rays = np.concatenate([ro.reshape(-1, 3), rd.reshape(-1, 3)], 1)
         raw = p.predict(T(rays)).cpu().numpy()
+        s = p.offsets(T(rays)).cpu().numpy()
         got = iv.cpu().numpy().reshape(2, -1)
         np.testing.assert_allclose(got[0], raw[:, 0] - 0.1, rtol=0, atol=1e-5)
-        far = raw[:, 1] + 0.2
-        np.testing.assert_allclose(got[1], np.where(far >= 3.4, np.inf, far), rtol=0, atol=1e-5)
+        rel = raw[:, 1] - s + 0.2  # far_cap is measured from the closest approach
+        keep = np.abs(rel - cap) > 1e-4  # rounding may decide rays right at the cap either way
+        want = np.where(rel >= cap, np.inf, raw[:, 1] + 0.2)
+        np.testing.assert_allclose(got[1][keep], want[keep], rtol=0, atol=1e-5)
+        n_inf += int(np.isinf(want).sum())
+        n_all += want.size
+    assert 0 < n_inf < n_all
 
 
 def test_train_step_matches_oracle(tracer):
@@ -97,7 +105,7 @@ def test_train_step_matches_oracle(tracer):
     per = -(-ntiles // p.partial.shape[0])
     ctas = -(-ntiles // per)
     g_gpu = p.partial[:ctas, :proposal.PARAMS].sum(0).double().cpu().numpy() / n
-    l_ref, g_ref = OP.loss_and_grad(m0, rays, targets, p.origin_scale, p.t_shift, p.t_scale, 8.0, 3.0)
+    l_ref, g_ref = OP.loss_and_grad(m0, rays, targets, p.origin_scale, p.t_shift, p.t_scale, 8.0, 3.0, p.center)
     e = rel_norm(g_gpu, g_ref)
     print(f"loss gpu {loss.item():.6f} oracle {l_ref:.6f}; gradient rel L2 {e:.2e}")
     assert abs(loss.item() - l_ref) <= 1e-3 * l_ref
@@ -119,46 +127,51 @@ def scene_dict(sc):
 
 
 def test_learned_intervals_on_tracer_records():
-    sc = scenes.make_scene(20000, seed=11, center_std=0.3, edge_range=(0.02, 0.1))
+    """Train on the plain tracer's records of 36 views, test on 4 others."""
+    # optically thick enough that many rays end on the transmittance cut-off
+    sc = scenes.make_scene(20000, seed=11, center_std=0.25, edge_range=(0.06, 0.25))
     s = scene_dict(sc)
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
     tr.build_tri_accel(s["verts"], s["cums"], sc.P, True)
-    cams = scenes.sphere_cameras(40, 96, 96, seed=4)
+    cams = scenes.sphere_cameras(40, 96, 96, seed=4, fov_deg=20.0)
     views = [tuple(T(a) for a in scenes.camera_rays(c)) for c in cams]
     train, held = views[:36], views[36:]
     p = proposal.Proposal(tr, seed=0)
-    rays, targets, far_target = proposal.collect(tr, s, train)
-    p.far_target, p.far_cap = far_target, far_target - 0.5
-    losses = proposal.fit(p, rays, targets, epochs=30, batch=16384, lr=3e-3)
+    rays, targets, far_target = proposal.collect(p, tr, s, train)
+    p.far_target, p.far_cap = far_target, far_target - 0.25
+    losses = proposal.fit(p, rays, targets, epochs=40, batch=16384, lr=3e-3)
     tr.device_status()
     first, last = losses[:5].mean(), losses[-5:].mean()
     print(f"loss {first:.4f} -> {last:.4f} over {len(losses)} steps")
     assert last < 0.2 * first
-    hrays, htargets, _ = proposal.collect(tr, s, held, far_target=far_target)
-    st = proposal.interval_stats(p.predict(hrays), htargets, far_target, 0.1, 0.1, p.far_cap)
+    hrays, htargets, _ = proposal.collect(p, tr, s, held, far_target=far_target)
+    st = proposal.interval_stats(p, hrays, htargets)
     print("held-out", st)
-    assert st["near_miss"] < 0.05
-    # clipped trace vs plain on the held-out views
+    assert st["near_miss"] == 0.0  # the near clip is off by default
+    assert st["terminated"] > 0.1 and st["far_clipped"] > 0.5 and st["far_err_median"] < 0.3
     bg = torch.zeros(3, device=DEV)
-    ivs = p.intervals(held, margin_near=0.1, margin_far=0.1)
+
     def render(intervals):
         outs, _ = tr.trace_forward_views(held, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3,
                                          s["opac"], torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), bg,
                                          2, intervals=intervals)
         return torch.stack([c for c, _ in outs]).cpu().numpy()
+
     tr.reset_stats()
     plain = render(None)
     st_plain = tr.stats()
-    tr.reset_stats()
-    clipped = render(ivs)
-    st_clip = tr.stats()
-    rmse = float(np.sqrt(np.mean((clipped - plain) ** 2)))
-    print(f"image RMSE clipped vs plain {rmse:.2e}; node visits/ray {st_plain['node_visits'] / st_plain['rays']:.1f}"
-          f" -> {st_clip['node_visits'] / st_clip['rays']:.1f}; continuations {st_clip['interval_continuations']},"
-          f" re-traces {st_clip['interval_retraces']}")
-    assert rmse < 1e-2  # small scene, short training; the benchmark states the real figure
-    assert st_clip["node_visits"] < st_plain["node_visits"]  # what the network gains
-    # margins that cover every ray reproduce the plain image exactly
-    wide = p.intervals(held, margin_near=100.0, margin_far=0.0)
-    np.testing.assert_array_equal(render(wide), plain)
+    for mf in (0.05, 0.2):
+        tr.reset_stats()
+        clipped = render(p.intervals(held, margin_far=mf))
+        st_clip = tr.stats()
+        print(f"margin_far {mf}: node visits/ray {st_plain['node_visits'] / st_plain['rays']:.1f} -> "
+              f"{st_clip['node_visits'] / st_clip['rays']:.1f}; triangle tests/ray "
+              f"{st_plain['triangle_tests'] / st_plain['rays']:.1f} -> "
+              f"{st_clip['triangle_tests'] / st_clip['rays']:.1f}; continuations "
+              f"{st_clip['interval_continuations']}, re-traces {st_clip['interval_retraces']}")
+        # the far clip never changes the result: a short interval only costs a continuation
+        np.testing.assert_array_equal(clipped, plain)
+    # with the near clip on, hits before t_near go missing: a small image error
+    rmse = float(np.sqrt(np.mean((render(p.intervals(held, margin_near=0.05)) - plain) ** 2)))
+    print(f"near clip on (margin 0.05): image RMSE {rmse:.2e}")
     tr.device_status()
