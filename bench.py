@@ -217,6 +217,111 @@ def algorithmic_bytes(rays, evals, blends):
     return fwd, bwd
 
 
+def proposal_leg(dev, steps=3, seed=0, small=False):
+    """The learned proposal against the plain traversal on the 3M-triangle
+    workload: 64 training views of 256x256 (4.2M rays traced by the plain
+    tracer), Adam on the tensor-core kernels, then forward + adjoint of 8
+    held-out 1920x1080 views (one batched launch each) with and without the
+    proposal's intervals, and with the perfect intervals of the plain
+    tracer's own hit records (the clip's upper bound)."""
+    import time
+
+    import torch
+
+    from diff_tritracer import _C, proposal, scenes
+
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    # small: the same protocol at profiling size (200k triangles, 16 x 128^2 training views, 2 x 540x960)
+    P, n_train, side, n_held, hh, ww = (200_000, 16, 128, 2, 540, 960) if small else (3_000_000, 64, 256, 8, 1080, 1920)
+    sc = scenes.make_scene(P, seed=seed)
+    S = dict(verts=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), npts=T(sc.num_points), cums=T(sc.cumsum),
+             shs=T(sc.shs), opac=T(sc.opacities), P=sc.P)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.set_traversal("packets", 32)
+    tr.build_tri_accel(S["verts"], S["cums"], sc.P, True)
+    train = [tuple(T(a) for a in scenes.camera_rays(c))
+             for c in scenes.sphere_cameras(n_train, side, side, seed=1000)]
+    held = [tuple(T(a) for a in scenes.camera_rays(c)) for c in scenes.sphere_cameras(n_held, hh, ww, seed=2000)]
+    ups = [tuple(T(a) for a in scenes.upstream_grads(hh, ww, seed=3000 + i)) for i in range(n_held)]
+    bg = torch.zeros(3, device=dev)
+    R = sum(ro.shape[0] * ro.shape[1] for ro, _ in held)
+
+    def fwd_bwd(intervals, records=None):
+        z1, z2 = torch.zeros(sc.P, device=dev), torch.zeros(sc.P, device=dev)
+        outs, _ = tr.trace_forward_views(held, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"], 3,
+                                         S["opac"], z1, z2, bg, 2, intervals=intervals, records=records)
+        g = tr.trace_backward_views(held, outs, ups, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"],
+                                    3, S["opac"], bg, intervals=intervals)
+        return outs, g
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_plain = timed(lambda: fwd_bwd(None))
+    recs = [torch.empty((3, ro.shape[0], ro.shape[1]), device=dev) for ro, _ in held]
+    ref_outs, ref_g = fwd_bwd(None, recs)
+    ref_col = torch.stack([c for c, _ in ref_outs]).clone()
+    ref_g = [x.clone() for x in ref_g]
+    # perfect intervals: the plain tracer's own first hit and (for terminated rays) last hit
+    perfect = [torch.stack([torch.where(torch.isfinite(r[0]), r[0], torch.zeros_like(r[0])),
+                            torch.where(r[2] > 0.5, r[1], torch.full_like(r[1], float("inf")))]) for r in recs]
+    perfect_far = [torch.stack([torch.zeros_like(p[0]), p[1]]) for p in perfect]
+    ms_perfect = timed(lambda: fwd_bwd(perfect))
+    ms_perfect_far = timed(lambda: fwd_bwd(perfect_far))
+
+    center = tuple(float(x) for x in sc.verts.reshape(-1, 3).mean(0))
+    prop = proposal.Proposal(tr, seed=seed, center=center)
+    t0 = time.time()
+    rays, targets, far_target = proposal.collect(prop, tr, S, train)
+    torch.cuda.synchronize()
+    t_collect = time.time() - t0
+    prop.far_target, prop.far_cap, prop.margin_far = far_target, far_target - 0.75, 0.3
+    t0 = time.time()
+    losses = proposal.fit(prop, rays, targets, epochs=30, batch=65536, lr=1e-3)
+    torch.cuda.synchronize()
+    t_fit = time.time() - t0
+    n_steps = len(losses)
+    ivs = prop.intervals(held)
+    ms_infer = timed(lambda: prop.intervals(held, out=ivs))
+    ms_prop = timed(lambda: fwd_bwd(ivs))
+    tr.reset_stats()
+    outs, g = fwd_bwd(ivs)
+    st = tr.stats()
+    tr.device_status()
+    col = torch.stack([c for c, _ in outs])
+    rmse = float(((col - ref_col) ** 2).mean().sqrt())
+    grad_rel = max(float((a - b).norm() / b.norm()) for a, b in zip(g, ref_g))
+    hr, ht, _ = proposal.collect(prop, tr, S, held[:2], far_target=far_target)
+    stats = proposal.interval_stats(prop, hr, ht)
+    flops_ray = 2 * (3 * 80 * 64 + 80 * 16)
+    return {
+        "workload": f"{P} triangles; train {n_train} views {side}x{side} ({int(rays.shape[0])} rays); "
+                    f"test {n_held} held-out views {ww}x{hh}",
+        "plain_mrays": R / ms_plain / 1e3,
+        "proposal_mrays": R / (ms_prop + ms_infer) / 1e3,
+        "speedup": ms_plain / (ms_prop + ms_infer),
+        "perfect_interval_mrays": R / ms_perfect / 1e3,
+        "perfect_far_only_mrays": R / ms_perfect_far / 1e3,
+        "image_rmse_vs_plain": rmse, "grad_rel_err_vs_plain": grad_rel,
+        "intervals": {k: round(v, 4) for k, v in stats.items()},
+        "continuations_per_ray": st["interval_continuations"] / max(st["rays"], 1),
+        "margin_far": prop.margin_far, "far_cap": prop.far_cap, "near_clip": "off",
+        "train": {"steps": n_steps, "batch": 65536, "lr": 1e-3, "seconds": t_fit, "collect_s": t_collect,
+                  "loss_first": float(losses[:5].mean()), "loss_last": float(losses[-5:].mean()),
+                  "tflops": 3 * flops_ray * 65536 * n_steps / max(t_fit, 1e-9) / 1e12},
+        "inference": {"ms": ms_infer, "tflops": flops_ray * R / (ms_infer / 1e3) / 1e12},
+    }
+
+
 def run_views(args, world, rank, local, dev):
     """Batched uneven views: every step is one CUDA-graph replay of refit +
     forward + adjoint over all 16 views (ViewBatch), after autotuning."""
@@ -304,6 +409,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-budget", type=float, default=3.0, help="seconds of CPU work per reference step")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default traversal configuration")
+    ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal leg")
+    ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
+    ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
+                    help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -370,7 +479,12 @@ def main():
         return float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
 
     tuned = None
-    if not args.no_autotune:
+    if args.traversal:
+        mode, num = args.traversal.rstrip("0123456789"), int(args.traversal.lstrip("acdeklnpst"))
+        tr.set_traversal(mode, k=num if mode == "packets" else 16, stack_depth=num if mode == "lanes" else 32)
+        tuned = {"traversal": mode, "k": num if mode == "packets" else 16,
+                 "stack_depth": num if mode == "lanes" else 32}
+    elif not args.no_autotune:
         tuned = autotune(tr, step, key=f"{name}", iters=2)
     for _ in range(max(3, args.warmup)):
         step()
@@ -465,6 +579,10 @@ def main():
     d2h = color_h.numel() * 4
 
     # ---------------- CPU baseline (rank 0, N = 1)
+    prop = None
+    if rank == 0 and world == 1 and not args.no_proposal:
+        prop = proposal_leg(dev, small=args.proposal_small)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(name, sc, ro_np, rd_np, g_np, go_np)[0]
@@ -496,6 +614,7 @@ def main():
                      "forward_ms": fwd_ms, "adjoint_ms": bwd_ms,
                      "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
         "cpu_baseline": cpu,
+        "proposal": prop,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
