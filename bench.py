@@ -322,6 +322,59 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
     }
 
 
+def secondary_leg(dev, steps=3, seed=0):
+    """Secondary-ray passes on their benchmark configuration: 500k
+    triangles, 20 % dielectric (IOR ~ U[1.3, 1.6]), a 512x1024 lat-long
+    environment map (U[0, 1] noise box-filtered 9x9), 2 views of 800x800
+    stacked into one [1600, 800] image, up to 2 bounces; forward + adjoint
+    through the device ray queue."""
+    import torch
+
+    from diff_tritracer import _C, scenes
+
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    P = 500_000
+    sc = scenes.make_scene(P, seed=seed)
+    sec = scenes.secondary_inputs(P, seed=seed)
+    cams = scenes.sphere_cameras(2, 800, 800, seed=seed + 3)
+    rays = [scenes.camera_rays(c) for c in cams]
+    ro = T(np.concatenate([r[0] for r in rays], 0))
+    rd = T(np.concatenate([r[1] for r in rays], 0))
+    g, go = scenes.upstream_grads(1600, 800, seed=seed)
+    g, go = T(g), T(go)
+    verts, sig, npts, cums = T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum)
+    shs, opac = T(sc.shs), T(sc.opacities)
+    mat, ior, env = T(sec["material"]), T(sec["ior"]), T(sec["env"])
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.build_tri_accel(verts, cums, P, True)
+    scaling, density = torch.zeros(P, device=dev), torch.zeros(P, device=dev)
+
+    def step():
+        color, others, _ = tr.trace_forward_secondary(ro, rd, verts, sig, npts, cums, P, shs, 3, opac, scaling,
+                                                      density, mat, ior, env, 2, 2)
+        tr.trace_backward_secondary(ro, rd, verts, sig, npts, cums, color, others, P, shs, 3, opac, g, go, mat,
+                                    ior, env, 2)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    tr.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = tr.stats()
+    tr.device_status()
+    R = 1600 * 800
+    return {"workload": "500k triangles, 20% dielectric, env 512x1024, 2 views 800x800, 2 bounces",
+            "pixels_per_step": R, "rays_per_step": st["rays"] / steps, "ms_per_step": ms,
+            "primary_mrays": R / ms / 1e3, "all_rays_mrays": st["rays"] / steps / ms / 1e3,
+            "step": "forward (3 trace levels + 3 resolves) + adjoint (all levels, one launch)"}
+
+
 def run_views(args, world, rank, local, dev):
     """Batched uneven views: every step is one CUDA-graph replay of refit +
     forward + adjoint over all 16 views (ViewBatch), after autotuning."""
@@ -411,6 +464,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default traversal configuration")
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
                     help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
@@ -582,6 +636,9 @@ def main():
     prop = None
     if rank == 0 and world == 1 and not args.no_proposal:
         prop = proposal_leg(dev, small=args.proposal_small)
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        secondary = secondary_leg(dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -615,6 +672,7 @@ def main():
                      "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
         "cpu_baseline": cpu,
         "proposal": prop,
+        "secondary": secondary,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

@@ -20,7 +20,11 @@ struct tt_tracer {
   int cfg_id = tt::kCfgPackets16;
   std::string err;
   tt::Bvh bvh;
-  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[kNumStats] from byte 16
+  tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[kNumStats] from byte 16,
+                       // int[3] secondary-ray queue counters from byte kSecCountOffset
+  tt::DevBuf sec_rec;  // secondary-ray queue: R * (2^(depth+1) - 1) records
+  int sec_R = 0, sec_depth = -1;  // the ray tree the last tt_forward_secondary left
+  int sec_trace_grid = 0, sec_bwd_grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
@@ -28,6 +32,8 @@ struct tt_tracer {
 };
 
 namespace {
+
+constexpr int kSecCountOffset = 96;
 
 int fail(tt_tracer* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -105,6 +111,8 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
   }
+  h->sec_trace_grid = h->num_sms * tt::sec_blocks_per_sm(0);
+  h->sec_bwd_grid = h->num_sms * tt::sec_blocks_per_sm(1);
   if (tt_set_traversal(h, h->cfg.traversal, h->cfg.k, h->cfg.stack_depth) != TT_OK) {
     delete h;
     return TT_ERR_INVALID;
@@ -141,6 +149,7 @@ int tt_destroy(tt_tracer* h) {
   if (!h) return TT_ERR_INVALID;
   h->bvh.release();
   h->scratch.release();
+  h->sec_rec.release();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   delete h;
@@ -560,6 +569,186 @@ int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int 
   p.nsets = n_views;
   p.ntiles = (int)tiles;
   return mlp_infer(h, net, p, margin_near, margin_far, far_cap, as_stream(stream));
+}
+
+// ---------------------------------------------------------------- secondary rays
+static int check_secondary(tt_tracer* h, const tt_secondary* sec, int P) {
+  TT_REQUIRE(h, sec != nullptr, "null secondary-ray description");
+  TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "secondary-ray passes need the plain program");
+  TT_REQUIRE(h, sec->max_depth >= 0 && sec->max_depth <= TT_MAX_BOUNCES, "max_depth must be in [0, 2]");
+  TT_REQUIRE(h, sec->env && sec->env_h > 0 && sec->env_w > 0, "need an environment map [env_h][env_w][3]");
+  TT_REQUIRE(h, P == 0 || (sec->material && sec->ior), "need material and ior per triangle");
+  return TT_OK;
+}
+
+static void sec_layout(tt::SecParams& sp, const tt_secondary* sec, tt::SecRecord* rec, int R, int* count) {
+  sp.material = sec->material;
+  sp.ior = sec->ior;
+  sp.env = sec->env;
+  sp.env_h = sec->env_h;
+  sp.env_w = sec->env_w;
+  sp.max_depth = sec->max_depth;
+  sp.rec = rec;
+  sp.count = count;
+  for (int l = 0; l <= tt::kMaxSecDepth; ++l) {
+    sp.base[l] = R * ((1 << l) - 1);
+    sp.cap[l] = R << l;
+  }
+}
+
+int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary* sec, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+  int rc = check_secondary(h, sec, a->P);
+  if (rc != TT_OK) return rc;
+  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->out_color && a->out_others, "null ray or output pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->scaling && a->density_factor && a->max_blending &&
+                              a->num_points),
+             "null per-triangle pointer");
+  rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  if (rc != TT_OK) return rc;
+  const long long R = (long long)a->H * a->W;
+  const long long nrec = R * ((2ll << sec->max_depth) - 1);
+  TT_REQUIRE(h, nrec < (1ll << 31), "too many rays for the secondary-ray queue");
+  const cudaStream_t s = as_stream(stream);
+  tt::TraceParams p = base_params(h);
+  tt_view v;
+  std::memset(&v, 0, sizeof(v));
+  v.H = a->H;
+  v.W = a->W;
+  v.ray_o = a->ray_o;
+  v.ray_d = a->ray_d;
+  v.out_color = a->out_color;
+  v.out_others = a->out_others;
+  rc = add_view(h, p, v);
+  if (rc != TT_OK) return rc;
+  rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
+  if (rc != TT_OK) return rc;
+  TT_CUDA(h, h->sec_rec.reserve((size_t)nrec * sizeof(tt::SecRecord)));
+  p.bvh = h->bvh.view();
+  p.verts = a->vertices;
+  p.cumsum = a->cumsum;
+  p.num_points = a->num_points;
+  p.shs = a->shs;
+  p.sh_degree = a->sh_degree;
+  p.M = a->M;
+  p.opac = a->opacities;
+  p.sigma = a->sigma;
+  p.bg = a->bg;
+  p.scaling = a->scaling;
+  p.density = a->density_factor;
+  p.max_blending = a->max_blending;
+  int* count = reinterpret_cast<int*>(h->scratch.as<char>() + kSecCountOffset);
+  sec_layout(p.sec, sec, h->sec_rec.as<tt::SecRecord>(), (int)R, count);
+  h->sec_depth = -1;  // no valid tree until this call's launches are enqueued
+  if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
+  TT_CUDA(h, cudaMemsetAsync(count, 0, (tt::kMaxSecDepth + 1) * sizeof(int), s));
+  if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  for (int level = 0; level <= sec->max_depth; ++level) {
+    p.sec.level = level;
+    TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+    TT_CUDA(h, tt::launch_sec_trace(p, h->sec_trace_grid, s));
+    ++h->trace_launches;
+  }
+  for (int level = sec->max_depth; level >= 0; --level) {
+    p.sec.level = level;
+    TT_CUDA(h, tt::launch_sec_resolve(p, s));
+    ++h->trace_launches;
+  }
+  if (a->debug) {
+    TT_CUDA(h, cudaEventRecord(h->ev1, s));
+    TT_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (a->gpu_time_ms) *a->gpu_time_ms = ms;
+  }
+  h->sec_R = (int)R;
+  h->sec_depth = sec->max_depth;
+  return TT_OK;
+}
+
+int tt_secondary_tree(tt_tracer* h, void* dst, unsigned long long dst_bytes, int* counts, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, counts != nullptr, "null counts");
+  if (h->sec_depth < 0) return fail(h, TT_ERR_STATE, "no secondary-ray forward on this handle");
+  const cudaStream_t s = as_stream(stream);
+  int dev_counts[tt::kMaxSecDepth + 1] = {0, 0, 0};
+  TT_CUDA(h, cudaMemcpyAsync(dev_counts, h->scratch.as<char>() + kSecCountOffset, sizeof(dev_counts),
+                             cudaMemcpyDeviceToHost, s));
+  const unsigned long long total =
+      (unsigned long long)h->sec_R * ((2ull << h->sec_depth) - 1) * sizeof(tt::SecRecord);
+  if (dst && dst_bytes)
+    TT_CUDA(h, cudaMemcpyAsync(dst, h->sec_rec.p, dst_bytes < total ? dst_bytes : total, cudaMemcpyDeviceToDevice, s));
+  TT_CUDA(h, cudaStreamSynchronize(s));
+  counts[0] = h->sec_R;
+  for (int l = 1; l <= tt::kMaxSecDepth; ++l) counts[l] = l <= h->sec_depth ? dev_counts[l] : 0;
+  return TT_OK;
+}
+
+int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary* sec, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
+  int rc = check_secondary(h, sec, a->P);
+  if (rc != TT_OK) return rc;
+  TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
+  TT_REQUIRE(h, a->ray_o && a->ray_d && a->others && a->dL_dpixels && a->dL_dothers,
+             "null ray, forward-output or upstream-gradient pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->cumsum && a->vertices), "null per-triangle pointer");
+  TT_REQUIRE(h, a->P == 0 || (a->dL_dtriangle && a->dL_dsigma && a->dL_dopacity && a->dL_dsh),
+             "null gradient output");
+  rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  if (rc != TT_OK) return rc;
+  if (!h->bvh.built() || h->bvh.P() != a->P) return fail(h, TT_ERR_STATE, "backward before a matching forward");
+  if (h->sec_depth != sec->max_depth || h->sec_R != a->H * a->W)
+    return fail(h, TT_ERR_STATE, "secondary backward without a matching tt_forward_secondary on this handle");
+  const cudaStream_t s = as_stream(stream);
+  tt::TraceParams p = base_params(h);
+  tt_view v;
+  std::memset(&v, 0, sizeof(v));
+  v.H = a->H;
+  v.W = a->W;
+  v.ray_o = a->ray_o;
+  v.ray_d = a->ray_d;
+  v.colors = a->colors;
+  v.others = a->others;
+  v.dL_dpixels = a->dL_dpixels;
+  v.dL_dothers = a->dL_dothers;
+  rc = add_view(h, p, v);
+  if (rc != TT_OK) return rc;
+  if (a->P > 0) {
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dtriangle, 0, (size_t)a->num_vertices * 3 * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dsigma, 0, (size_t)a->P * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dopacity, 0, (size_t)a->P * sizeof(float), s));
+    TT_CUDA(h, cudaMemsetAsync(a->dL_dsh, 0, (size_t)a->P * a->M * 3 * sizeof(float), s));
+  }
+  p.verts = a->vertices;
+  p.cumsum = a->cumsum;
+  p.num_points = a->num_points;
+  p.shs = a->shs;
+  p.sh_degree = a->sh_degree;
+  p.M = a->M;
+  p.opac = a->opacities;
+  p.sigma = a->sigma;
+  p.bg = a->bg;
+  p.d_tri = a->dL_dtriangle;
+  p.d_sigma = a->dL_dsigma;
+  p.d_opac = a->dL_dopacity;
+  p.d_sh = a->dL_dsh;
+  int* count = reinterpret_cast<int*>(h->scratch.as<char>() + kSecCountOffset);
+  sec_layout(p.sec, sec, h->sec_rec.as<tt::SecRecord>(), h->sec_R, count);
+  TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+  if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  TT_CUDA(h, tt::launch_sec_backward(p, h->sec_bwd_grid, s));
+  ++h->trace_launches;
+  if (a->debug) {
+    TT_CUDA(h, cudaEventRecord(h->ev1, s));
+    TT_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (a->gpu_time_ms) *a->gpu_time_ms = ms;
+  }
+  return TT_OK;
 }
 
 }  // extern "C"

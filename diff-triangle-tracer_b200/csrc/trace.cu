@@ -18,6 +18,7 @@
 //    (the FP32 hit point loses ~4 digits on small triangles far from the
 //    camera); SH, compositing and the side outputs are FP32 like the
 //    reference; the adjoint re-traverses instead of storing hit lists.
+#include <algorithm>
 #include <cfloat>
 
 #include "trace.cuh"
@@ -1329,6 +1330,504 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __
   run<CFG>(p, sh, cnt);
 }
 
+// ---------------------------------------------------------------- secondary rays
+// Secondary-ray passes over a device ray queue (no reference counterpart; the
+// reference bends rays only at one analytic sphere). Per pixel a tree of
+// rays: the first blended hit of a ray of depth < max_depth on a triangle of
+// material 1 spawns a reflected and (unless totally reflected) a refracted
+// ray from the exact hit point, and that hit's colour is
+// F L(reflected) + (1 - F) L(refracted) instead of its SH colour; rays that
+// leave the scene see a lat-long environment map in place of bg. One launch
+// per level traces the level's rays from its queue and appends their
+// children to the next level's queue (atomic slot counter); resolve launches
+// then add each child's radiance to its parent, deepest level first, and
+// write the pixel colours. The adjoint traces every ray of every level in one
+// launch with upstream gradient tau dL/dpixel, taking the spawning hit's
+// colour from the children's resolved radiance.
+
+// Per-lane persistent driver over `total` queue items (item order = record
+// order); lanes refill as their rays finish.
+template <int SD, class Shader>
+__device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm, Shader& sh, Counters& cnt,
+                                            int total) {
+  constexpr int K = kChunk;
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  bool have = false, exhausted = false;
+  Cursor cur = first_cursor(p.tmin_inclusive);
+  float3 o = make_float3(0.f, 0.f, 0.f), d = o;
+  for (;;) {
+    const unsigned need = __ballot_sync(full, !have && !exhausted);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(p.work, __popc(need));
+      base = __shfl_sync(full, base, leader);
+      if (!have && !exhausted) {
+        const int item = base + __popc(need & lt);
+        if (item >= total) {
+          exhausted = true;
+        } else {
+          sh.begin_item(item, o, d);
+          cur = first_cursor(p.tmin_inclusive);
+          have = true;
+        }
+      }
+    }
+    if (__ballot_sync(full, have) == 0) {
+      if (__all_sync(full, exhausted)) break;
+      continue;
+    }
+    float t_drop = INFINITY;
+    if (have) {
+      const RayW r = make_ray(o, d);
+      unsigned long long kb[kChunk];
+      query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
+#pragma unroll
+      for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+    }
+    __syncwarp();
+    if (have) {
+      bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);
+      if (!done && ++cur.chunks >= kMaxChunks) {
+        atomicOr(p.status, kStatusTimeout);
+        done = true;
+      }
+      if (done) {
+        sh.end();
+        have = false;
+      }
+    }
+  }
+}
+
+// FP64 with explicit round-to-nearest operations (no contraction), in the
+// oracle's operation order, so both spawn the same FP32 rays.
+namespace sd {
+struct V {
+  double x, y, z;
+};
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ V vsub(V a, V b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
+__device__ __forceinline__ V vadd(V a, V b) { return {add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)}; }
+__device__ __forceinline__ V vscale(V a, double s) { return {mul(a.x, s), mul(a.y, s), mul(a.z, s)}; }
+__device__ __forceinline__ double dot(V a, V b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+__device__ __forceinline__ V cross(V a, V b) {
+  return {sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)), sub(mul(a.x, b.y), mul(a.y, b.x))};
+}
+__device__ __forceinline__ V from(float4 v) { return {(double)v.x, (double)v.y, (double)v.z}; }
+__device__ __forceinline__ V from(float3 v) { return {(double)v.x, (double)v.y, (double)v.z}; }
+__device__ __forceinline__ float3 to_f(V v) {
+  return make_float3(__double2float_rn(v.x), __double2float_rn(v.y), __double2float_rn(v.z));
+}
+}  // namespace sd
+
+struct SpawnDev {
+  float3 o, r, t;
+  bool refracts;
+  float F;
+};
+
+// Reflected / refracted rays at the hit of (o, d) on the triangle (a, b, c)
+// with index of refraction ior: Schlick's Fresnel term, the exact hit point
+// of an FP64 plane solve.
+__device__ __noinline__ SpawnDev spawn_rays(float4 a4, float4 b4, float4 c4, float3 of, float3 df, float ior_f) {
+  using namespace sd;
+  const V A = from(a4), B = from(b4), C = from(c4), o = from(of), d = from(df);
+  const V nc = cross(vsub(B, A), vsub(C, A));
+  const double te = __ddiv_rn(dot(vsub(A, o), nc), dot(d, nc));
+  const V x = vadd(o, vscale(d, te));
+  const V n = vscale(nc, __ddiv_rn(1.0, __dsqrt_rn(dot(nc, nc))));
+  const V du = vscale(d, __ddiv_rn(1.0, __dsqrt_rn(dot(d, d))));
+  const double ior = (double)ior_f;
+  const double cosi = dot(du, n);
+  const bool entering = cosi < 0.0;
+  const V nf = entering ? n : V{-n.x, -n.y, -n.z};
+  const double c = entering ? -cosi : cosi;
+  const double ei = entering ? 1.0 : ior, et = entering ? ior : 1.0;
+  const double eta = __ddiv_rn(ei, et);
+  const double q = __ddiv_rn(sub(ei, et), add(ei, et));
+  const double r0 = mul(q, q);
+  const double k = sub(1.0, mul(mul(eta, eta), sub(1.0, mul(c, c))));
+  SpawnDev sp;
+  sp.o = to_f(x);
+  sp.r = to_f(vadd(du, vscale(nf, mul(2.0, c))));
+  sp.refracts = k >= 0.0;
+  double F = 1.0;
+  V t = du;
+  if (sp.refracts) {
+    const double m = sub(1.0, c);
+    const double m2 = mul(m, m);
+    F = add(r0, mul(sub(1.0, r0), mul(mul(m2, m2), m)));
+    t = vadd(vscale(du, eta), vscale(nf, sub(mul(eta, c), __dsqrt_rn(k))));
+  }
+  sp.t = to_f(t);
+  sp.F = __double2float_rn(F);
+  return sp;
+}
+
+// Lat-long lookup: longitude atan2(d.z, d.x) over the columns (wrapping),
+// colatitude acos(d.y) over the rows (clamped), bilinear between texel centres.
+__device__ __forceinline__ float3 env_lookup(const SecParams& s, float3 d) {
+  const float kPi = 3.14159265358979f;
+  const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+  const float u = atan2f(d.z, d.x) * (0.5f / kPi) + 0.5f;
+  const float v = acosf(fminf(1.f, fmaxf(-1.f, d.y / len))) * (1.0f / kPi);
+  float fx = u * (float)s.env_w - 0.5f, fy = v * (float)s.env_h - 0.5f;
+  if (!(fabsf(fx) <= (float)s.env_w)) fx = 0.f;  // NaN direction: any texel, never out of bounds
+  if (!(fabsf(fy) <= (float)s.env_h)) fy = 0.f;
+  const float x0f = floorf(fx), y0f = floorf(fy);
+  const float ax = fx - x0f, ay = fy - y0f;
+  const int W = s.env_w, H = s.env_h;
+  const int x0 = (((int)x0f % W) + W) % W, x1 = (x0 + 1) % W;
+  const int y0 = max(0, min(H - 1, (int)y0f)), y1 = max(0, min(H - 1, (int)y0f + 1));
+  const float* e = s.env;
+  float out[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float t00 = __ldg(e + ((size_t)y0 * W + x0) * 3 + c), t01 = __ldg(e + ((size_t)y0 * W + x1) * 3 + c);
+    const float t10 = __ldg(e + ((size_t)y1 * W + x0) * 3 + c), t11 = __ldg(e + ((size_t)y1 * W + x1) * 3 + c);
+    out[c] = (1.f - ay) * ((1.f - ax) * t00 + ax * t01) + ay * ((1.f - ax) * t10 + ax * t11);
+  }
+  return make_float3(out[0], out[1], out[2]);
+}
+
+// The rays of one level: trace, composite, spawn children into the next level.
+struct SecShader {
+  const TraceParams& p;
+  const ViewDesc* v;
+  int ridx, pix, level;
+  float3 o, d;
+  float C0, C1, C2, N0, N1, N2, T, tau;
+  bool spawned;
+  unsigned n_rays = 0, n_eval = 0, n_blend = 0;
+
+  __device__ explicit SecShader(const TraceParams& params) : p(params), v(&params.views[0]), level(params.sec.level) {}
+
+  __device__ __forceinline__ void begin_item(int i, float3& ro, float3& rd) {
+    const SecParams& s = p.sec;
+    ridx = s.base[level] + i;
+    SecRecord* r = s.rec + ridx;
+    if (level == 0) {
+      pix = i;
+      ro = make_float3(v->ray_o[3 * pix], v->ray_o[3 * pix + 1], v->ray_o[3 * pix + 2]);
+      rd = make_float3(v->ray_d[3 * pix], v->ray_d[3 * pix + 1], v->ray_d[3 * pix + 2]);
+      tau = 1.0f;
+      r->pixel = pix;
+      r->tau = 1.0f;
+    } else {
+      ro = make_float3(r->o[0], r->o[1], r->o[2]);
+      rd = make_float3(r->d[0], r->d[1], r->d[2]);
+      pix = r->pixel;
+      tau = r->tau;
+    }
+    r->child_r = r->child_t = -1;
+    r->F = r->w = 0.f;
+    o = ro;
+    d = rd;
+    C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
+    T = 1.0f;
+    spawned = false;
+    ++n_rays;
+  }
+
+  __device__ __forceinline__ void prepare() {}
+
+  __device__ __forceinline__ int push_child(float3 co, float3 cd, float ctau) {
+    const SecParams& s = p.sec;
+    const int slot = atomicAdd(s.count + level + 1, 1);
+    if (slot >= s.cap[level + 1]) {
+      atomicOr(p.status, kStatusStack);
+      return -1;
+    }
+    SecRecord* c = s.rec + s.base[level + 1] + slot;
+    c->o[0] = co.x;
+    c->o[1] = co.y;
+    c->o[2] = co.z;
+    c->d[0] = cd.x;
+    c->d[1] = cd.y;
+    c->d[2] = cd.z;
+    c->pixel = pix;
+    c->tau = ctau;
+    return slot;
+  }
+
+  __device__ __forceinline__ bool visit(uint32_t prim, float) {
+    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
+    const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+    const Geom g = window_fn(a, b, c, o, d, __ldg(p.sigma + prim));
+    ++n_eval;
+    const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
+    if (alpha < kAlphaMin) return false;
+    const float test_T = T * (1.0f - alpha);
+    if (test_T < kTMin) return true;
+    ++n_blend;
+    const float w = alpha * T;
+    if (level == 0) {
+      p.density[prim] = 1.0f;
+      compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
+      atomicMax(reinterpret_cast<int*>(p.max_blending) + prim, __float_as_int(w));
+      N0 += g.n.x * w;
+      N1 += g.n.y * w;
+      N2 += g.n.z * w;
+    }
+    const SecParams& s = p.sec;
+    if (!spawned && level < s.max_depth && __ldg(s.material + prim) == 1) {
+      // the hit's colour comes from its children at the resolve
+      spawned = true;
+      const SpawnDev sp = spawn_rays(a, b, c, o, d, __ldg(s.ior + prim));
+      SecRecord* r = s.rec + ridx;
+      r->F = sp.F;
+      r->w = w;
+      r->child_r = push_child(sp.o, sp.r, tau * w * sp.F);
+      if (sp.refracts) r->child_t = push_child(sp.o, sp.t, tau * w * (1.0f - sp.F));
+    } else {
+      float B[16];
+      sh_basis(unit(d), p.sh_degree, B);
+      const float3 col = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+      C0 += fmaxf(col.x, 0.f) * w;
+      C1 += fmaxf(col.y, 0.f) * w;
+      C2 += fmaxf(col.z, 0.f) * w;
+    }
+    T = test_T;
+    return false;
+  }
+
+  __device__ __forceinline__ void end() {
+    const float3 e = env_lookup(p.sec, d);
+    SecRecord* r = p.sec.rec + ridx;
+    r->L[0] = C0 + T * e.x;
+    r->L[1] = C1 + T * e.y;
+    r->L[2] = C2 + T * e.z;
+    if (level == 0) {
+      const int HW = v->H * v->W;
+      v->out_others[kDepthCh * HW + pix] = 0.0f;
+      v->out_others[kAlphaCh * HW + pix] = 1.0f - T;
+      v->out_others[(kNormalCh + 0) * HW + pix] = N0;
+      v->out_others[(kNormalCh + 1) * HW + pix] = N1;
+      v->out_others[(kNormalCh + 2) * HW + pix] = N2;
+      v->out_others[kMidDepthCh * HW + pix] = 0.0f;
+      v->out_others[kDistortionCh * HW + pix] = 0.0f;
+    }
+  }
+};
+
+__device__ __forceinline__ int sec_level_size(const TraceParams& p, int level) {
+  return level == 0 ? p.views[0].H * p.views[0].W : min(__ldcg(p.sec.count + level), p.sec.cap[level]);
+}
+
+__global__ void __launch_bounds__(kTraceThreads, 4) k_sec_trace(const __grid_constant__ TraceParams p) {
+  Counters cnt;
+  SecShader sh(p);
+  drive_items<32>(p, thread_smem<32>(), sh, cnt, sec_level_size(p, p.sec.level));
+  add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
+}
+
+// Adds each record's children's radiance to it (their level is complete) and,
+// for level 0, writes the pixel colours.
+__global__ void k_sec_resolve(const __grid_constant__ TraceParams p) {
+  const SecParams& s = p.sec;
+  const int level = s.level;
+  const int n = sec_level_size(p, level);
+  const ViewDesc& v = p.views[0];
+  const int HW = v.H * v.W;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    SecRecord* r = s.rec + s.base[level] + i;
+    float L0 = r->L[0], L1 = r->L[1], L2 = r->L[2];
+    if (r->child_r >= 0 || r->child_t >= 0) {
+      float lr[3] = {0.f, 0.f, 0.f}, lt[3] = {0.f, 0.f, 0.f};
+      if (r->child_r >= 0) {
+        const SecRecord* c = s.rec + s.base[level + 1] + r->child_r;
+        lr[0] = c->L[0];
+        lr[1] = c->L[1];
+        lr[2] = c->L[2];
+      }
+      if (r->child_t >= 0) {
+        const SecRecord* c = s.rec + s.base[level + 1] + r->child_t;
+        lt[0] = c->L[0];
+        lt[1] = c->L[1];
+        lt[2] = c->L[2];
+      }
+      const float F = r->F, w = r->w;
+      L0 += w * (F * lr[0] + (1.0f - F) * lt[0]);
+      L1 += w * (F * lr[1] + (1.0f - F) * lt[1]);
+      L2 += w * (F * lr[2] + (1.0f - F) * lt[2]);
+      r->L[0] = L0;
+      r->L[1] = L1;
+      r->L[2] = L2;
+    }
+    if (level == 0) {
+      v.out_color[i] = L0;
+      v.out_color[HW + i] = L1;
+      v.out_color[2 * HW + i] = L2;
+    }
+  }
+}
+
+// Adjoint of every ray of every level (backward.cu's per-hit formulas with
+// upstream gradient tau dL/dpixel; the spawning hit's colour is the
+// children's resolved radiance and it has no SH gradient).
+struct SecBwdShader {
+  const TraceParams& p;
+  const ViewDesc* v;
+  int ridx, pix, level;
+  float3 o, d;
+  float Cf0, Cf1, Cf2, Df, Nf0, Nf1, Nf2;
+  float g0, g1, g2, gD, gN0, gN1, gN2;
+  float C0, C1, C2, N0, N1, N2, D, T;
+  bool spawned;
+
+  __device__ explicit SecBwdShader(const TraceParams& params) : p(params), v(&params.views[0]) {}
+
+  __device__ __forceinline__ void begin_item(int item, float3& ro, float3& rd) {
+    const SecParams& s = p.sec;
+    level = 0;
+    int i = item;
+    while (level < s.max_depth && i >= sec_level_size(p, level)) {
+      i -= sec_level_size(p, level);
+      ++level;
+    }
+    ridx = s.base[level] + i;
+    const SecRecord* r = s.rec + ridx;
+    const int HW = v->H * v->W;
+    float tau;
+    if (level == 0) {
+      pix = i;
+      ro = make_float3(v->ray_o[3 * pix], v->ray_o[3 * pix + 1], v->ray_o[3 * pix + 2]);
+      rd = make_float3(v->ray_d[3 * pix], v->ray_d[3 * pix + 1], v->ray_d[3 * pix + 2]);
+      tau = 1.0f;
+      Df = __ldg(v->others + kDepthCh * HW + pix);
+      Nf0 = __ldg(v->others + (kNormalCh + 0) * HW + pix);
+      Nf1 = __ldg(v->others + (kNormalCh + 1) * HW + pix);
+      Nf2 = __ldg(v->others + (kNormalCh + 2) * HW + pix);
+      gD = __ldg(v->dL_doth + kDepthCh * HW + pix);
+      gN0 = __ldg(v->dL_doth + (kNormalCh + 0) * HW + pix);
+      gN1 = __ldg(v->dL_doth + (kNormalCh + 1) * HW + pix);
+      gN2 = __ldg(v->dL_doth + (kNormalCh + 2) * HW + pix);
+    } else {
+      ro = make_float3(r->o[0], r->o[1], r->o[2]);
+      rd = make_float3(r->d[0], r->d[1], r->d[2]);
+      pix = r->pixel;
+      tau = r->tau;
+      Df = Nf0 = Nf1 = Nf2 = gD = gN0 = gN1 = gN2 = 0.f;
+    }
+    Cf0 = r->L[0];
+    Cf1 = r->L[1];
+    Cf2 = r->L[2];
+    g0 = tau * __ldg(v->dL_dpix + pix);
+    g1 = tau * __ldg(v->dL_dpix + HW + pix);
+    g2 = tau * __ldg(v->dL_dpix + 2 * HW + pix);
+    o = ro;
+    d = rd;
+    C0 = C1 = C2 = N0 = N1 = N2 = D = 0.f;
+    T = 1.0f;
+    spawned = false;
+  }
+
+  __device__ __forceinline__ void prepare() {}
+
+  __device__ __forceinline__ bool visit(uint32_t prim, float) {
+    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
+    const float sig = __ldg(p.sigma + prim);
+    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
+    const float opacity = __ldg(p.opac + prim);
+    const float alpha = fminf(kAlphaMax, opacity * g.Cx);
+    if (alpha < kAlphaMin) return false;
+    const float test_T = T * (1.0f - alpha);
+    if (test_T < kTMin) return true;
+    const float w = alpha * T;
+    const SecParams& s = p.sec;
+    float c0, c1, c2;
+    float raw0 = 0.f, raw1 = 0.f, raw2 = 0.f;
+    float B[16];
+    const bool spawn = !spawned && level < s.max_depth && __ldg(s.material + prim) == 1;
+    if (spawn) {
+      spawned = true;
+      const SecRecord* r = s.rec + ridx;
+      const float F = r->F;
+      float lr[3] = {0.f, 0.f, 0.f}, lt[3] = {0.f, 0.f, 0.f};
+      if (r->child_r >= 0) {
+        const SecRecord* c = s.rec + s.base[level + 1] + r->child_r;
+        lr[0] = c->L[0];
+        lr[1] = c->L[1];
+        lr[2] = c->L[2];
+      }
+      if (r->child_t >= 0) {
+        const SecRecord* c = s.rec + s.base[level + 1] + r->child_t;
+        lt[0] = c->L[0];
+        lt[1] = c->L[1];
+        lt[2] = c->L[2];
+      }
+      c0 = F * lr[0] + (1.0f - F) * lt[0];
+      c1 = F * lr[1] + (1.0f - F) * lt[1];
+      c2 = F * lr[2] + (1.0f - F) * lt[2];
+    } else {
+      sh_basis(unit(d), p.sh_degree, B);
+      const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+      raw0 = raw.x;
+      raw1 = raw.y;
+      raw2 = raw.z;
+      c0 = fmaxf(raw.x, 0.f);
+      c1 = fmaxf(raw.y, 0.f);
+      c2 = fmaxf(raw.z, 0.f);
+    }
+    C0 += c0 * w;
+    C1 += c1 * w;
+    C2 += c2 * w;
+    N0 += g.n.x * w;
+    N1 += g.n.y * w;
+    N2 += g.n.z * w;
+    D += w * g.t;
+    const float inv1a = 1.0f / (1.0f - alpha);
+    float dL_dalpha = g0 * (T * c0 - (Cf0 - C0) * inv1a) + g1 * (T * c1 - (Cf1 - C1) * inv1a) +
+                      g2 * (T * c2 - (Cf2 - C2) * inv1a);
+    dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
+    dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
+                 gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
+    red_add(p.d_opac + prim, dL_dalpha * g.Cx);
+    const float dL_dC = opacity * dL_dalpha;
+    if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
+    const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
+    float3 gv[3];
+    window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
+    float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      red_add(dt + 3 * k + 0, gv[k].x);
+      red_add(dt + 3 * k + 1, gv[k].y);
+      red_add(dt + 3 * k + 2, gv[k].z);
+    }
+    if (!spawn) {
+      const float e0 = raw0 < 0.f ? 0.f : g0 * w, e1 = raw1 < 0.f ? 0.f : g1 * w, e2 = raw2 < 0.f ? 0.f : g2 * w;
+      float* dsh = p.d_sh + (size_t)prim * p.M * 3;
+      const int n = sh_count(p.sh_degree);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k < n) {
+          red_add(dsh + 3 * k + 0, B[k] * e0);
+          red_add(dsh + 3 * k + 1, B[k] * e1);
+          red_add(dsh + 3 * k + 2, B[k] * e2);
+        }
+      }
+    }
+    T = test_T;
+    return false;
+  }
+
+  __device__ __forceinline__ void end() {}
+};
+
+__global__ void __launch_bounds__(kTraceThreads, 4) k_sec_backward(const __grid_constant__ TraceParams p) {
+  Counters cnt;
+  SecBwdShader sh(p);
+  int total = 0;
+  for (int l = 0; l <= p.sec.max_depth; ++l) total += sec_level_size(p, l);
+  drive_items<32>(p, thread_smem<32>(), sh, cnt, total);
+}
+
 // ---------------------------------------------------------------- hit stream
 __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p) {
   const Stack st = thread_smem<kStackDepth>().st;
@@ -1423,6 +1922,33 @@ cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
     case kCfgLanes24: k_backward<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
     default: k_backward<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
   }
+  return cudaGetLastError();
+}
+
+int sec_blocks_per_sm(int which) {
+  int n = 0;
+  const void* fn = which == 0 ? (const void*)k_sec_trace : (const void*)k_sec_backward;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem_bytes_for<kCfgLanes32>()) !=
+      cudaSuccess)
+    n = 1;
+  return n > 0 ? n : 1;
+}
+
+cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s) {
+  k_sec_trace<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s) {
+  const long long cap = p.sec.level == 0 ? (long long)p.views[0].H * p.views[0].W : p.sec.cap[p.sec.level];
+  const int grid = (int)std::min<long long>((cap + 255) / 256, 4096);
+  if (grid == 0) return cudaSuccess;
+  k_sec_resolve<<<grid, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sec_backward(const TraceParams& p, int grid, cudaStream_t s) {
+  k_sec_backward<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
   return cudaGetLastError();
 }
 

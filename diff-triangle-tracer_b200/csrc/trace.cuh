@@ -24,6 +24,36 @@ struct ViewDesc {
   int H, W, ntx, tile_begin;
 };
 
+// Secondary-ray passes: one record per ray of each pixel's ray tree
+// (64 bytes). Level 0 holds the primary rays (record i = pixel i of view 0;
+// their origin/direction fields are unused), level k + 1 the rays spawned by
+// level k.
+struct SecRecord {
+  float o[3];
+  int pixel;
+  float d[3];
+  float tau;   // product of the spawn weights along the path (the adjoint's scale)
+  float L[3];  // radiance: without the spawn term after the trace, complete after the resolve
+  float F;     // Fresnel share of the reflected child
+  float w;     // blending weight of the spawning hit
+  int child_r, child_t;  // records of the children in the next level, or -1
+  int pad;
+};
+
+constexpr int kMaxSecDepth = 2;
+
+struct SecParams {
+  const int* material;  // [P], 1 = dielectric interface
+  const float* ior;     // [P]
+  const float* env;     // [env_h][env_w][3] lat-long radiance
+  int env_h, env_w, max_depth;
+  SecRecord* rec;
+  int level;                       // level traced / resolved by this launch
+  int base[kMaxSecDepth + 1];      // first record of each level
+  int cap[kMaxSecDepth + 1];       // records each level can hold
+  int* count;                      // [kMaxSecDepth + 1] records per level, levels >= 1 (device)
+};
+
 struct TraceParams {
   BvhView bvh;
   int nviews;
@@ -55,6 +85,7 @@ struct TraceParams {
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)
+  SecParams sec;              // secondary-ray passes only
 };
 
 struct HitStreamParams {
@@ -89,5 +120,11 @@ int trace_blocks_per_sm(int which /*0 forward, 1 adjoint, 2 variant*/, int cfg);
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);
+// Secondary-ray passes (views[0] only): trace level p.sec.level, resolve it,
+// or run the adjoint of every ray of every level.
+int sec_blocks_per_sm(int which /*0 trace, 1 adjoint*/);
+cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s);
+cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s);
+cudaError_t launch_sec_backward(const TraceParams& p, int grid, cudaStream_t s);
 
 }  // namespace tt

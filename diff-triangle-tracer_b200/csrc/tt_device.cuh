@@ -139,7 +139,10 @@ __device__ __forceinline__ bool isect_tri(const RayW& r, float4 a, float4 b, flo
   const float Bz = __fmul_rn(r.Sz, Bkz);
   const float Cz = __fmul_rn(r.Sz, Ckz);
   const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
-  t = __fdiv_rn(T, det);
+  // + 0 turns a -0 distance (a ray starting on the triangle's plane, e.g. a
+  // spawned secondary ray) into +0: hit keys are built from the float's
+  // bits, where -0 would sort after every other hit
+  t = __fadd_rn(__fdiv_rn(T, det), 0.0f);
   return true;
 }
 

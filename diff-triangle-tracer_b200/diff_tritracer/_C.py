@@ -277,6 +277,99 @@ class OptixTracer:
         a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
         return a, (verts, sig, npts, cums, sh, opac, bg)
 
+    # ------------------------------------------------------------------ secondary rays
+    def _secondary(self, material, ior, env, max_depth):
+        dev = self.device
+        mat = _i32(material, "material", dev)
+        io = _f32(ior, "ior", dev)
+        ev = _f32(env, "env", dev)
+        if ev.dim() != 3 or ev.shape[2] != 3:
+            raise RuntimeError("env must be [env_h, env_w, 3]")
+        sec = _lib.TtSecondary(_ptr(mat), _ptr(io), _ptr(ev), int(ev.shape[0]), int(ev.shape[1]), int(max_depth))
+        return sec, (mat, io, ev)
+
+    def trace_forward_secondary(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
+                                cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities, scaling,
+                                density_factor, material, ior, env, max_depth=2, rebuild_gas_opt=0, debug=False):
+        """Secondary-ray passes (dielectric triangles spawn reflected and
+        refracted rays up to max_depth bounces, an environment map lights
+        escaping rays). Returns (color [3,H,W], others [7,H,W], max_blending
+        [P]); scaling and density_factor are updated in place."""
+        dev = self.device
+        P = int(number_of_points)
+        ro, rd = _f32(ray_o, "ray_o", dev), _f32(ray_d, "ray_d", dev)
+        H, W = int(ro.shape[0]), int(ro.shape[1])
+        max_blending = torch.empty((P,), dtype=torch.float32, device=dev)
+        bg = torch.zeros(3, device=dev)
+        a, keep = self._scene_fwd_args(triangles_points, sigma, num_points_per_triangle,
+                                       cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities,
+                                       scaling, density_factor, bg, rebuild_gas_opt, max_blending)
+        color = torch.empty((3, H, W), dtype=torch.float32, device=dev)
+        others = torch.empty((7, H, W), dtype=torch.float32, device=dev)
+        ms = ctypes.c_float(0.0)
+        a.H, a.W, a.ray_o, a.ray_d = H, W, _ptr(ro), _ptr(rd)
+        a.out_color, a.out_others = _ptr(color), _ptr(others)
+        a.debug = 1 if debug else 0
+        a.gpu_time_ms = ctypes.pointer(ms)
+        sec, skeep = self._secondary(material, ior, env, max_depth)
+        check(self._h, lib.tt_forward_secondary(self._h, ctypes.byref(a), ctypes.byref(sec), _stream()))
+        self._keep = keep + skeep + (ro, rd)
+        self.last_gpu_time_ms = ms.value
+        return color, others, max_blending
+
+    def secondary_tree(self):
+        """Test hook: (records [N, 16] float32 view of the last secondary
+        forward's ray records, counts per level). Record fields: o[3],
+        pixel (int bits), d[3], tau, L[3], F, w, child_r, child_t (int bits)."""
+        counts = (ctypes.c_int * 3)()
+        check(self._h, lib.tt_secondary_tree(self._h, None, 0, counts, _stream()))
+        depth = sum(1 for c in counts[1:] if c > 0)
+        R = counts[0]
+        n = R * (2 ** (len(counts)) - 1)
+        buf = torch.zeros((n, 16), dtype=torch.float32, device=self.device)
+        check(self._h, lib.tt_secondary_tree(self._h, _ptr(buf), buf.numel() * 4, counts, _stream()))
+        return buf, list(counts)
+
+    def trace_backward_secondary(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
+                                 cumsum_of_points_per_triangle, colors, others, number_of_points, shs, sh_degree,
+                                 opacities, dL_dpixels, dL_dothers, material, ior, env, max_depth=2):
+        """Adjoint of the last trace_forward_secondary (same rays and scene):
+        (dL_dtriangle [V,3], dL_dsigma, dL_dopacity, dL_dsh [P,M,3])."""
+        dev = self.device
+        P = int(number_of_points)
+        ro, rd = _f32(ray_o, "ray_o", dev), _f32(ray_d, "ray_d", dev)
+        H, W = int(ro.shape[0]), int(ro.shape[1])
+        verts = _f32(triangles_points, "triangles_points", dev)
+        sig = _f32(sigma, "sigma", dev)
+        npts = _i32(num_points_per_triangle, "num_points_per_triangle", dev)
+        cums = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", dev)
+        col, oth = _f32(colors, "colors", dev), _f32(others, "others", dev)
+        sh = _f32(shs, "shs", dev)
+        M = int(sh.shape[1]) if sh.dim() >= 2 and sh.shape[0] != 0 else 0
+        opac = _f32(opacities, "opacities", dev)
+        g, go = _f32(dL_dpixels, "dL_dpixels", dev), _f32(dL_dothers, "dL_dothers", dev)
+        V = verts.numel() // 3
+        grads = (torch.empty((V, 3), dtype=torch.float32, device=dev),
+                 torch.empty_like(sigma, memory_format=torch.contiguous_format),
+                 torch.empty_like(opacities, memory_format=torch.contiguous_format),
+                 torch.empty((P, M, 3), dtype=torch.float32, device=dev))
+        bg = torch.zeros(3, device=dev)
+        a = _lib.TtBwdArgs()
+        a.H, a.W = H, W
+        a.ray_o, a.ray_d, a.bg = _ptr(ro), _ptr(rd), _ptr(bg)
+        a.vertices, a.num_vertices = _ptr(verts), V
+        a.sigma, a.num_points, a.cumsum = _ptr(sig), _ptr(npts), _ptr(cums)
+        a.colors, a.others, a.P = _ptr(col), _ptr(oth), P
+        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
+        a.opacities, a.dL_dpixels, a.dL_dothers = _ptr(opac), _ptr(g), _ptr(go)
+        a.scaling = ctypes.c_void_p(0)
+        a.dL_dtriangle, a.dL_dsigma, a.dL_dopacity, a.dL_dsh = [_ptr(x) for x in grads]
+        a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        sec, skeep = self._secondary(material, ior, env, max_depth)
+        check(self._h, lib.tt_backward_secondary(self._h, ctypes.byref(a), ctypes.byref(sec), _stream()))
+        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg) + skeep
+        return grads
+
     def trace_forward_views(self, rays, triangles_points, sigma, num_points_per_triangle,
                             cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities, scaling,
                             density_factor, bg_color, rebuild_gas_opt, outputs=None, max_blending=None,

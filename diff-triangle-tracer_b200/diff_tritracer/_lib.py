@@ -100,11 +100,16 @@ class TtMlpStep(ctypes.Structure):
                 ("far_weight", ctypes.c_float)]
 
 
+class TtSecondary(ctypes.Structure):
+    _fields_ = [("material", _vp), ("ior", _vp), ("env", _vp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
+                ("max_depth", ctypes.c_int)]
+
+
 EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
     "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
-    "tt_mlp_intervals",
+    "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree",
 )
 
 
@@ -128,6 +133,9 @@ def _load():
     lib.tt_get_stats.argtypes = [_vp, ctypes.POINTER(TtStats), _vp]
     lib.tt_reset_stats.argtypes = [_vp, _vp]
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+    lib.tt_forward_secondary.argtypes = [_vp, ctypes.POINTER(TtFwdArgs), ctypes.POINTER(TtSecondary), _vp]
+    lib.tt_backward_secondary.argtypes = [_vp, ctypes.POINTER(TtBwdArgs), ctypes.POINTER(TtSecondary), _vp]
+    lib.tt_secondary_tree.argtypes = [_vp, _vp, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_int), _vp]
     lib.tt_mlp_update.argtypes = [_vp, ctypes.POINTER(TtMlp), _vp]
     lib.tt_mlp_train_step.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtMlpStep), _vp, _vp, ctypes.c_int,
                                       _vp, _vp]

@@ -134,3 +134,28 @@ def upstream_grads(H: int, W: int, seed: int = 0, others_std: float = 0.0):
         go[0] = rng.normal(0, others_std, size=(H, W))
         go[2:5] = rng.normal(0, others_std, size=(3, H, W))
     return g, go
+
+
+def box_filter_latlong(img: np.ndarray, k: int) -> np.ndarray:
+    """k x k box filter of a lat-long map [h, w, c]: wraps in longitude,
+    clamps (edge-replicates) in latitude."""
+    r = k // 2
+    pad = np.pad(img, ((r, r), (0, 0), (0, 0)), mode="edge")
+    pad = np.concatenate([pad[:, -r:], pad, pad[:, :r]], axis=1).astype(np.float64)
+    c = np.cumsum(np.cumsum(pad, 0), 1)
+    c = np.pad(c, ((1, 0), (1, 0), (0, 0)))
+    h, w = img.shape[:2]
+    out = c[k:k + h, k:k + w] - c[:h, k:k + w] - c[k:k + h, :w] + c[:h, :w]
+    return (out / (k * k)).astype(np.float32)
+
+
+def secondary_inputs(P: int, seed: int = 0, p_dielectric: float = 0.2, ior_range=(1.3, 1.6),
+                     env_shape=(512, 1024), box: int = 9, max_depth: int = 2) -> dict:
+    """Per-triangle dielectric mask (Bernoulli), IOR (uniform) and a lat-long
+    environment map (uniform noise, box-filtered) for the secondary-ray
+    passes."""
+    rng = np.random.default_rng(seed + 31337)
+    material = (rng.random(P) < p_dielectric).astype(np.int32)
+    ior = rng.uniform(ior_range[0], ior_range[1], P).astype(np.float32)
+    env = box_filter_latlong(rng.random((env_shape[0], env_shape[1], 3), dtype=np.float32), box)
+    return {"material": material, "ior": ior, "env": env, "max_depth": max_depth}

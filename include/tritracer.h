@@ -305,6 +305,40 @@ int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, fl
 int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int n_views, float* const* intervals,
                      float margin_near, float margin_far, float far_cap, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Secondary-ray passes (no reference counterpart: the reference bends rays
+ * only at the analytic sphere of its reflect/refract/envlight programs).
+ * Per pixel a tree of rays, traced level by level from a device ray queue
+ * owned by the handle: the first blended hit of a ray of depth < max_depth on
+ * a triangle with material[prim] == 1 (a dielectric interface with index of
+ * refraction ior[prim]) spawns a reflected and, unless totally reflected, a
+ * refracted ray from the exact hit point, and that hit's colour is
+ * F L(reflected) + (1 - F) L(refracted) (Schlick's Fresnel term) instead of
+ * its SH colour. Every other hit shades as in tt_forward. A ray's
+ * transmittance left at the end sees the lat-long environment map env
+ * (longitude atan2(d.z, d.x) over the columns, colatitude acos(d.y) over the
+ * rows, bilinear) in place of bg. out_color = radiance of the primary ray;
+ * out_others, density_factor, scaling and max_blending come from the primary
+ * rays only. The adjoint differentiates every ray of the tree with the spawn
+ * geometry (directions, F) held constant, and uses the ray tree of the last
+ * tt_forward_secondary on the handle (same rays, scene and max_depth).
+ * One view per call (H, W, rays and outputs of the argument block). */
+#define TT_MAX_BOUNCES 2
+typedef struct tt_secondary {
+  const int* material; /* [P]: 1 = dielectric interface, 0 = plain */
+  const float* ior;    /* [P] */
+  const float* env;    /* [env_h][env_w][3] */
+  int env_h, env_w;
+  int max_depth;       /* 0..TT_MAX_BOUNCES */
+} tt_secondary;
+int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary* s, void* stream);
+int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary* s, void* stream);
+/* Test hook: synchronises `stream`, writes the number of rays of each level
+ * of the last tt_forward_secondary into counts[0..2] (host) and copies up to
+ * dst_bytes of its 64-byte ray records (level 0 first, each level's records
+ * at offset R * (2^level - 1)) into dst (device). */
+int tt_secondary_tree(tt_tracer* h, void* dst, unsigned long long dst_bytes, int* counts, void* stream);
+
 /* Forward trace that allocates nothing. No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: an operator plugin that only

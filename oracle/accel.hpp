@@ -84,7 +84,7 @@ inline bool isect_tri(const RayPre& r, const float* v0, const float* v1, const f
   const float Bz = r.Sz * B[r.kz];
   const float Cz = r.Sz * C[r.kz];
   const float T = (U * Az + V * Bz) + W * Cz;
-  *t_out = T / det;
+  *t_out = T / det + 0.0f;  // a -0 distance (ray starting on the plane) counts as +0, like the GPU's keys
   return true;
 }
 

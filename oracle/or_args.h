@@ -37,5 +37,10 @@ struct or_args {
   float* margin;    // [H*W]
   // optional proposed interval per ray, [2][H*W] (t_near plane, t_far plane)
   const float* interval;
+  // secondary rays (or_*_secondary only)
+  const int* material;
+  const float* ior;
+  const float* env;
+  int env_h, env_w, max_depth;
 };
 }

@@ -124,6 +124,78 @@ extern "C" int or_backward_f64(void* s, const or_args* a, double* dtri, double* 
   return backward_impl<double>(s, a, dtri, dsigma, dopac, dsh);
 }
 
+static SecInputs to_sec(const or_args* a) {
+  SecInputs s;
+  s.material = a->material;
+  s.ior = a->ior;
+  s.env = a->env;
+  s.env_h = a->env_h;
+  s.env_w = a->env_w;
+  s.max_depth = a->max_depth;
+  return s;
+}
+
+template <class R>
+static int forward_sec_impl(void* scene, const or_args* a, R* scaling, R* density, R* color, R* others, R* maxb) {
+  const Scene& sc = *static_cast<Scene*>(scene);
+  const Inputs in = to_inputs(a);
+  const SecInputs sec = to_sec(a);
+  const Opts opt = to_opts(a, sizeof(R) == 8);
+  FwdOut<R> out{scaling, density, color, others, maxb};
+  parallel_rows(a, [&](int pix) {
+    RayRecord rec;
+    RayRecord* rp = nullptr;
+    if (a->rec_count) {
+      rec.max_rec = a->max_rec;
+      rec.ids = a->rec_ids + (size_t)pix * a->max_rec;
+      rp = &rec;
+    }
+    sec_radiance<R>(sc, in, sec, in.ray_o + 3 * (size_t)pix, in.ray_d + 3 * (size_t)pix, 0, opt, &out, pix, rp);
+    if (rp) {
+      a->rec_count[pix] = rec.count;
+      if (a->margin) a->margin[pix] = (float)rec.margin;
+    }
+  });
+  return 0;
+}
+
+template <class R>
+static int backward_sec_impl(void* scene, const or_args* a, R* dtri, R* dsigma, R* dopac, R* dsh) {
+  const Scene& sc = *static_cast<Scene*>(scene);
+  const Inputs in = to_inputs(a);
+  const SecInputs sec = to_sec(a);
+  const Opts opt = to_opts(a, sizeof(R) == 8);
+  const R* others = static_cast<const R*>(a->others);
+  BwdOut<R> bo{dtri, dsigma, dopac, dsh};
+  const int HW = a->H * a->W;
+  parallel_rows(a, [&](int pix) {
+    const R gL[3] = {(R)a->dL_dpixels[pix], (R)a->dL_dpixels[HW + pix], (R)a->dL_dpixels[2 * HW + pix]};
+    const R go[4] = {(R)a->dL_dothers[kDepth * HW + pix], (R)a->dL_dothers[(kNormal + 0) * HW + pix],
+                     (R)a->dL_dothers[(kNormal + 1) * HW + pix], (R)a->dL_dothers[(kNormal + 2) * HW + pix]};
+    const R fo[4] = {others[kDepth * HW + pix], others[(kNormal + 0) * HW + pix], others[(kNormal + 1) * HW + pix],
+                     others[(kNormal + 2) * HW + pix]};
+    sec_backward<R>(sc, in, sec, in.ray_o + 3 * (size_t)pix, in.ray_d + 3 * (size_t)pix, 0, opt, gL, go, fo, bo);
+  });
+  return 0;
+}
+
+extern "C" int or_forward_secondary_f64(void* s, const or_args* a, double* scaling, double* density, double* color,
+                                        double* others, double* maxb) {
+  return forward_sec_impl<double>(s, a, scaling, density, color, others, maxb);
+}
+extern "C" int or_forward_secondary_f32(void* s, const or_args* a, float* scaling, float* density, float* color,
+                                        float* others, float* maxb) {
+  return forward_sec_impl<float>(s, a, scaling, density, color, others, maxb);
+}
+extern "C" int or_backward_secondary_f64(void* s, const or_args* a, double* dtri, double* dsigma, double* dopac,
+                                         double* dsh) {
+  return backward_sec_impl<double>(s, a, dtri, dsigma, dopac, dsh);
+}
+extern "C" int or_backward_secondary_f32(void* s, const or_args* a, float* dtri, float* dsigma, float* dopac,
+                                         float* dsh) {
+  return backward_sec_impl<float>(s, a, dtri, dsigma, dopac, dsh);
+}
+
 // Every triangle hit in [0, tmax] of each ray, ordered by (t, primitive id),
 // truncated to max_hits: the stream the chunked k-closest query walks through.
 extern "C" int or_hit_stream(void* scene, const float* ray_o, const float* ray_d, int R, float tmax, int max_hits,

@@ -916,4 +916,247 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
       [](const Hit&) {}, t_near, t_far);
 }
 
+// ---------------------------------------------------------------- secondary rays
+// Secondary-ray passes with per-triangle dielectric interfaces and an
+// environment map. No reference counterpart (the reference bends rays only
+// at one analytic sphere, reflect.cu / refract.cu / envlight.cu); these are
+// the semantics the GPU's ray-queue passes implement:
+//  * every ray marches as forward.cu does (window function, alpha, the
+//    1/255 floor, the 1e-4 transmittance cut-off, SH colour, front-to-back
+//    compositing); its radiance is L = sum_i w_i c_i + T_final env(d), with
+//    a lat-long environment map in place of bg;
+//  * the first blended hit of a ray of depth < max_depth on a triangle of
+//    material 1 spawns a reflected and (unless totally reflected) a
+//    refracted ray from the exact hit point (FP64 plane solve), and that
+//    hit's colour is F L(reflected) + (1 - F) L(refracted) instead of its SH
+//    colour (Schlick's Fresnel term with the triangle's IOR; set-up in FP64
+//    without contraction, so GPU and CPU spawn the same FP32 rays);
+//  * pixel colour = L(primary); alpha, normal, density, scaling and
+//    max_blending come from the primary ray only;
+//  * adjoint: the same march for every ray of the tree with upstream
+//    gradient tau dL/dpixel, tau the product of the spawn weights (w F or
+//    w (1 - F)) along the path; the spawn geometry (directions, F) is held
+//    constant, as the reference's vertex gradient ignores how hit points
+//    move.
+struct SecInputs {
+  const int* material = nullptr;  // [P], 1 = dielectric interface
+  const float* ior = nullptr;     // [P]
+  const float* env = nullptr;     // [env_h][env_w][3]
+  int env_h = 0, env_w = 0;
+  int max_depth = 2;
+};
+
+// Lat-long lookup: longitude atan2(d.z, d.x) over the columns (wrapping),
+// colatitude acos(d.y) over the rows (clamped), bilinear between texel
+// centres.
+template <class R>
+inline V3<R> env_lookup(const SecInputs& s, V3<R> d) {
+  const double kPi = 3.14159265358979323846;
+  const double dx = d.x, dy = d.y, dz = d.z;
+  const double len = std::sqrt(dx * dx + dy * dy + dz * dz);
+  const double u = std::atan2(dz, dx) / (2.0 * kPi) + 0.5;
+  const double v = std::acos(std::fmax(-1.0, std::fmin(1.0, dy / len))) / kPi;
+  const double fx = u * s.env_w - 0.5, fy = v * s.env_h - 0.5;
+  const double x0f = std::floor(fx), y0f = std::floor(fy);
+  const double ax = fx - x0f, ay = fy - y0f;
+  const int W = s.env_w, H = s.env_h;
+  const int x0 = (((int)x0f % W) + W) % W, x1 = (x0 + 1) % W;
+  const int y0 = std::max(0, std::min(H - 1, (int)y0f)), y1 = std::max(0, std::min(H - 1, (int)y0f + 1));
+  double out[3];
+  for (int c = 0; c < 3; ++c) {
+    auto tx = [&](int x, int y) { return (double)s.env[((size_t)y * W + x) * 3 + c]; };
+    out[c] = (1 - ay) * ((1 - ax) * tx(x0, y0) + ax * tx(x1, y0)) + ay * ((1 - ax) * tx(x0, y1) + ax * tx(x1, y1));
+  }
+  return V3<R>{(R)out[0], (R)out[1], (R)out[2]};
+}
+
+struct Spawn {
+  float o[3];   // exact hit point
+  float r[3];   // reflected direction
+  float t[3];   // refracted direction (if refracts)
+  bool refracts;
+  double F;     // reflected share
+};
+
+// Reflected / refracted rays at the hit of ray (of, df) on triangle prim.
+inline Spawn spawn_rays(const Inputs& in, int prim, const float* of, const float* df, double ior) {
+  const int off = in.cumsum[prim];
+  const V3<double> A = from_f<double>(in.verts + 3 * (size_t)off);
+  const V3<double> B = from_f<double>(in.verts + 3 * (size_t)(off + 1));
+  const V3<double> C = from_f<double>(in.verts + 3 * (size_t)(off + 2));
+  const V3<double> o = from_f<double>(of), d = from_f<double>(df);
+  const V3<double> nc = cross(B - A, C - A);
+  const double te = dot(A - o, nc) / dot(d, nc);
+  const V3<double> x = o + te * d;
+  const V3<double> n = nc / std::sqrt(dot(nc, nc));
+  const V3<double> du = d / std::sqrt(dot(d, d));
+  const double cosi = dot(du, n);
+  const bool entering = cosi < 0.0;
+  const V3<double> nf = entering ? n : -n;
+  const double c = entering ? -cosi : cosi;
+  const double ei = entering ? 1.0 : ior, et = entering ? ior : 1.0;
+  const double eta = ei / et;
+  const double r0 = ((ei - et) / (ei + et)) * ((ei - et) / (ei + et));
+  const double k = 1.0 - eta * eta * (1.0 - c * c);
+  Spawn sp;
+  const V3<double> r = du + (2.0 * c) * nf;
+  sp.refracts = k >= 0.0;
+  V3<double> t = du;
+  if (sp.refracts) {
+    const double m = 1.0 - c;
+    const double m2 = m * m;
+    sp.F = r0 + (1.0 - r0) * (m2 * m2 * m);
+    t = eta * du + (eta * c - std::sqrt(k)) * nf;
+  } else {
+    sp.F = 1.0;
+  }
+  const double xs[3] = {x.x, x.y, x.z}, rs[3] = {r.x, r.y, r.z}, ts[3] = {t.x, t.y, t.z};
+  for (int i = 0; i < 3; ++i) {
+    sp.o[i] = (float)xs[i];
+    sp.r[i] = (float)rs[i];
+    sp.t[i] = (float)ts[i];
+  }
+  return sp;
+}
+
+// Radiance of one ray of the tree (recursive over its spawned rays). For the
+// primary ray (out != nullptr) also the side outputs of pixel pix.
+template <class R>
+inline V3<R> sec_radiance(const Scene& sc, const Inputs& in, const SecInputs& s, const float* of, const float* df,
+                          int depth, const Opts& opt, FwdOut<R>* out, int pix, RayRecord* rec) {
+  const V3<R> o = from_f<R>(of), d = from_f<R>(df);
+  const RayPre rp = ray_pre(of, df);
+  V3<R> C = mk<R>(0, 0, 0), N = mk<R>(0, 0, 0);
+  R T = 1;
+  bool spawned = false;
+  march(
+      sc, rp, opt,
+      [&](uint32_t prim, float t) -> bool {
+        const V3<R> hp = hit_point(in, (int)prim, o, d, t, opt);
+        const Window<R> w = window_fn(in, (int)prim, hp);
+        const R alpha = std::fmin(R(kAlphaMax), (R)in.opacities[prim] * w.Cx);
+        if (rec) rec->near((double)alpha, (double)kAlphaMin);
+        if (alpha < R(kAlphaMin)) return false;
+        const R test_T = T * (R(1) - alpha);
+        if (rec) rec->near((double)test_T, (double)kTMin);
+        if (test_T < R(kTMin)) return true;
+        const R bw = alpha * T;
+        if (out) {
+          out->density[prim] = R(1);
+          compute_scaling(in, (int)prim, o, out->scaling, opt.mt);
+          atomic_max(&out->max_blending[prim], bw, opt.mt);
+          N = N + w.n * bw;
+        }
+        V3<R> col;
+        if (!spawned && depth < s.max_depth && s.material[prim] == 1) {
+          spawned = true;
+          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim]);
+          const V3<R> Lr = sec_radiance<R>(sc, in, s, sp.o, sp.r, depth + 1, opt, nullptr, pix, rec);
+          const V3<R> Lt = sp.refracts ? sec_radiance<R>(sc, in, s, sp.o, sp.t, depth + 1, opt, nullptr, pix, rec)
+                                       : mk<R>(0, 0, 0);
+          col = R(sp.F) * Lr + R(1.0 - sp.F) * Lt;
+        } else {
+          col = sh_color(in, (int)prim, d, nullptr);
+        }
+        C = C + col * bw;
+        T = test_T;
+        return false;
+      },
+      [&](const Hit& h) {
+        if (rec && out) rec->add(h);
+      });
+  const V3<R> L = C + T * env_lookup<R>(s, d);
+  if (out) {
+    const int HW = in.H * in.W;
+    out->color[pix] = L.x;
+    out->color[HW + pix] = L.y;
+    out->color[2 * HW + pix] = L.z;
+    out->others[pix + kDepth * HW] = R(0);
+    out->others[pix + kAlphaOff * HW] = R(1) - T;
+    out->others[pix + (kNormal + 0) * HW] = N.x;
+    out->others[pix + (kNormal + 1) * HW] = N.y;
+    out->others[pix + (kNormal + 2) * HW] = N.z;
+    out->others[pix + kMidDepth * HW] = R(0);
+    out->others[pix + kDistortion * HW] = R(0);
+  }
+  return L;
+}
+
+// Adjoint of one ray of the tree with upstream dL/dL = gL (and, for the
+// primary ray, dL/d(depth, normal) and its final side outputs).
+template <class R>
+inline void sec_backward(const Scene& sc, const Inputs& in, const SecInputs& s, const float* of, const float* df,
+                         int depth, const Opts& opt, const R gL[3], const R* g_others, const R* f_others,
+                         BwdOut<R>& bo) {
+  const V3<R> o = from_f<R>(of), d = from_f<R>(df);
+  const RayPre rp = ray_pre(of, df);
+  const V3<R> Lf = sec_radiance<R>(sc, in, s, of, df, depth, opt, nullptr, 0, nullptr);
+  const R final_color[3] = {Lf.x, Lf.y, Lf.z};
+  const R gD = g_others ? g_others[0] : R(0);
+  const V3<R> gN = g_others ? mk<R>(g_others[1], g_others[2], g_others[3]) : mk<R>(0, 0, 0);
+  const R final_depth = f_others ? f_others[0] : R(0);
+  const V3<R> final_normal = f_others ? mk<R>(f_others[1], f_others[2], f_others[3]) : mk<R>(0, 0, 0);
+  R C[3] = {0, 0, 0};
+  V3<R> N = mk<R>(0, 0, 0);
+  R D = 0, T = 1;
+  bool spawned = false;
+  march(
+      sc, rp, opt,
+      [&](uint32_t prim, float t) -> bool {
+        const V3<R> hp = hit_point(in, (int)prim, o, d, t, opt);
+        const R hit_t = hit_dist(in, (int)prim, o, d, t, opt);
+        const Window<R> w = window_fn(in, (int)prim, hp);
+        const R opacity = (R)in.opacities[prim];
+        const R alpha = std::fmin(R(kAlphaMax), opacity * w.Cx);
+        if (alpha < R(kAlphaMin)) return false;
+        const R test_T = T * (R(1) - alpha);
+        if (test_T < R(kTMin)) return true;
+        const R bw = alpha * T;
+        bool clamped[3] = {false, false, false};
+        V3<R> col;
+        bool spawn = false;
+        if (!spawned && depth < s.max_depth && s.material[prim] == 1) {
+          spawned = spawn = true;
+          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim]);
+          const V3<R> Lr = sec_radiance<R>(sc, in, s, sp.o, sp.r, depth + 1, opt, nullptr, 0, nullptr);
+          V3<R> Lt = mk<R>(0, 0, 0);
+          const R gr[3] = {gL[0] * bw * R(sp.F), gL[1] * bw * R(sp.F), gL[2] * bw * R(sp.F)};
+          sec_backward<R>(sc, in, s, sp.o, sp.r, depth + 1, opt, gr, nullptr, nullptr, bo);
+          if (sp.refracts) {
+            Lt = sec_radiance<R>(sc, in, s, sp.o, sp.t, depth + 1, opt, nullptr, 0, nullptr);
+            const R ft = R(1.0 - sp.F);
+            const R gt[3] = {gL[0] * bw * ft, gL[1] * bw * ft, gL[2] * bw * ft};
+            sec_backward<R>(sc, in, s, sp.o, sp.t, depth + 1, opt, gt, nullptr, nullptr, bo);
+          }
+          col = R(sp.F) * Lr + R(1.0 - sp.F) * Lt;
+        } else {
+          col = sh_color(in, (int)prim, d, clamped);
+        }
+        const R c[3] = {col.x, col.y, col.z};
+        for (int ch = 0; ch < 3; ++ch) C[ch] += c[ch] * bw;
+        N = N + w.n * bw;
+        D += bw * hit_t;
+        const R inv_1_alpha = R(1) / (R(1) - alpha);
+        R dL_dalpha = R(0);
+        R dL_dcolor[3];
+        for (int ch = 0; ch < 3; ++ch) {
+          dL_dcolor[ch] = gL[ch] * bw;
+          dL_dalpha += gL[ch] * (T * c[ch] - (final_color[ch] - C[ch]) * inv_1_alpha);
+        }
+        if (g_others) {
+          dL_dalpha += gD * (T * hit_t - (final_depth - D) * inv_1_alpha);
+          dL_dalpha += sum3(vmul(gN, T * w.n - (final_normal - N) * inv_1_alpha));
+        }
+        atomic_add(&bo.dopac[prim], dL_dalpha * w.Cx, opt.mt);
+        const R dL_dC = opacity * dL_dalpha;
+        if (w.phi_final > R(0)) atomic_add(&bo.dsigma[prim], dL_dC * w.Cx * fast_log<R>(w.phi_final), opt.mt);
+        const R dL_dphi_x = (R)in.sigma[prim] / w.phi_max * dL_dC * w.Cx;
+        window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, gN * bw, bo.dtri, opt.mt);
+        if (!spawn) sh_color_bwd(in, (int)prim, d, clamped, dL_dcolor, bo.dsh, opt.mt);
+        T = test_T;
+        return false;
+      },
+      [](const Hit&) {});
+}
+
 }  // namespace tto

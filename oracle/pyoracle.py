@@ -39,6 +39,8 @@ class OrArgs(ctypes.Structure):
         ("dL_dpixels", _fp), ("dL_dothers", _fp),
         ("max_rec", ctypes.c_int), ("rec_ids", _ip), ("rec_count", _ip), ("margin", _fp),
         ("interval", _fp),
+        ("material", _ip), ("ior", _fp), ("env", _fp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
+        ("max_depth", ctypes.c_int),
     ]
 
 
@@ -130,11 +132,25 @@ class _Runner:
             raise ValueError("interval must be [2, H, W]")
         a.interval = _ptr(keep["interval"])
 
+    @staticmethod
+    def _secondary(a, keep, secondary):
+        """Secondary-ray inputs: dict(material [P] int, ior [P], env [h, w, 3], max_depth)."""
+        if secondary is None:
+            return ""
+        keep["material"] = _c(secondary["material"], np.int32)
+        keep["ior"] = _c(secondary["ior"], np.float32)
+        keep["env"] = _c(secondary["env"], np.float32)
+        a.material, a.ior, a.env = _ptr(keep["material"], _ip), _ptr(keep["ior"]), _ptr(keep["env"])
+        a.env_h, a.env_w = keep["env"].shape[0], keep["env"].shape[1]
+        a.max_depth = int(secondary.get("max_depth", 2))
+        return "secondary_"
+
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
                 canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None,
-                interval=None):
+                interval=None, secondary=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, extra, variant, tmin_inclusive, canonical, exact, nthreads, rows)
         self._interval(a, keep, interval)
+        sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64
         H, W, P = a.H, a.W, scene.P
         scaling = np.zeros(P, dt) if scaling is None else _c(scaling, dt).reshape(-1).copy()
@@ -153,7 +169,7 @@ class _Runner:
             assert precision == 32
             fn = self.lib.ref_forward
         else:
-            fn = self.lib.or_forward_f32 if precision == 32 else self.lib.or_forward_f64
+            fn = getattr(self.lib, f"or_forward_{sec}f{precision}")
         fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrArgs)] + [t] * 5
         rc = fn(self._scene(scene)[1], ctypes.byref(a), _ptr(scaling, t), _ptr(density, t), _ptr(color, t),
                 _ptr(others, t), _ptr(maxb, t))
@@ -162,9 +178,11 @@ class _Runner:
         return FwdResult(color, others, scaling, density, maxb, rec_ids, rec_count, margin)
 
     def backward(self, scene, ray_o, ray_d, colors, others, dL_dpixels, dL_dothers, bg=None, precision=32,
-                 tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None):
+                 tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None,
+                 secondary=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, None, 0, tmin_inclusive, canonical, exact, nthreads, rows)
         self._interval(a, keep, interval)
+        sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64
         keep["colors"] = _c(colors, dt)
         keep["others"] = _c(others, dt)
@@ -184,7 +202,7 @@ class _Runner:
             assert precision == 32
             fn = self.lib.ref_backward
         else:
-            fn = self.lib.or_backward_f32 if precision == 32 else self.lib.or_backward_f64
+            fn = getattr(self.lib, f"or_backward_{sec}f{precision}")
         fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrArgs)] + [t] * 4
         rc = fn(self._scene(scene)[1], ctypes.byref(a), _ptr(dtri, t), _ptr(dsigma, t), _ptr(dopac, t), _ptr(dsh, t))
         if rc != 0:

@@ -1,0 +1,124 @@
+"""Secondary-ray passes on the GPU (device ray queue: dielectric triangles
+reflect and refract, an environment map lights escaping rays) against the
+FP64 oracle's restatement of the same semantics (oracle.hpp sec_radiance /
+sec_backward), through the C ABI:
+
+* colour and side outputs within |d| <= 1e-5 |ref| + 1e-6 per pixel for
+  every pixel whose ray tree makes no decision within 1e-5 (relative) of a
+  threshold; the spawned rays are bit-identical (FP64 set-up without
+  contraction on both sides);
+* all four gradients within 1e-4 relative (L2);
+* without dielectric triangles and with a constant environment the passes
+  reproduce the plain trace with bg = that constant.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from diff_tritracer import _C, scenes  # noqa: E402
+from diff_tritracer.secondary import SecondaryTracer  # noqa: E402
+from gpu_helpers import DEV, MARGIN, T, flagged_prims, rel_norm  # noqa: E402
+from scenes_for_tests import dense_scene, dense_view  # noqa: E402
+
+RTOL, ATOL = 1e-5, 1e-6
+H, W = 48, 64
+
+
+@pytest.fixture(scope="module")
+def setup():
+    sc = dense_scene(seed=7, P=3000)
+    ro, rd = dense_view(H=H, W=W)
+    sec = scenes.secondary_inputs(sc.P, seed=7, p_dielectric=0.3, env_shape=(32, 64), box=5)
+    return sc, ro, rd, sec
+
+
+def gpu_secondary(tr, sc, ro, rd, sec, g=None, go=None, max_depth=2):
+    color, others, maxb = tr.trace_forward_secondary(
+        T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P, T(sc.shs), 3,
+        T(sc.opacities), scaling := torch.zeros(sc.P, device=DEV), density := torch.zeros(sc.P, device=DEV),
+        T(sec["material"]), T(sec["ior"]), T(sec["env"]), max_depth)
+    out = dict(color=color, others=others, max_blending=maxb, scaling=scaling, density=density)
+    if g is not None:
+        out["grads"] = tr.trace_backward_secondary(
+            T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), color, others, sc.P,
+            T(sc.shs), 3, T(sc.opacities), T(g), T(go), T(sec["material"]), T(sec["ior"]), T(sec["env"]),
+            max_depth)
+    torch.cuda.synchronize()
+    tr.device_status()
+    return {k: (v.cpu().numpy() if torch.is_tensor(v) else [x.cpu().numpy() for x in v]) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("max_depth", [1, 2])
+def test_forward_and_adjoint_vs_fp64_oracle(oracle, setup, max_depth):
+    sc, ro, rd, sec = setup
+    sec = dict(sec, max_depth=max_depth)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.reset_stats()
+    g, go = scenes.upstream_grads(H, W, seed=11, others_std=1.0)
+    ref = oracle.forward(sc, ro, rd, precision=64, exact=True, canonical=True, record=256, nthreads=8, secondary=sec)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    assert ok.mean() > 0.95, ok.mean()
+    g, go = g * ok[None], go * ok[None]
+    got = gpu_secondary(tr, sc, ro, rd, sec, g, go, max_depth)
+    st = tr.stats()
+    assert st["rays"] > H * W * 1.5  # the queue really held spawned rays
+    for key in ("color", "others"):
+        a, b = got[key][:, ok], getattr(ref, key)[:, ok]
+        err = np.abs(a - b)
+        worst = float((err / (RTOL * np.abs(b) + ATOL)).max())
+        print(f"depth {max_depth} {key}: max abs {err.max():.2e}, worst/tol {worst:.3f}")
+        assert np.all(err <= RTOL * np.abs(b) + ATOL), (key, worst)
+    skip = np.zeros(sc.P, bool)
+    skip[flagged_prims(ref, H, W, ok)] = True
+    np.testing.assert_array_equal(got["density"][~skip], ref.density[~skip])
+    np.testing.assert_allclose(got["max_blending"][~skip], ref.max_blending[~skip], rtol=RTOL, atol=ATOL)
+    rb = oracle.backward(sc, ro, rd, ref.color, ref.others, g, go, precision=64, exact=True, canonical=True,
+                         nthreads=8, secondary=sec)
+    for key, x in zip(("dtri", "dsigma", "dopac", "dsh"), got["grads"]):
+        e = rel_norm(x, getattr(rb, key))
+        print(f"depth {max_depth} {key}: rel L2 {e:.2e}")
+        assert np.linalg.norm(getattr(rb, key)) > 0
+        assert e < 1e-4, (key, e)
+
+
+def test_reduces_to_plain(setup):
+    sc, ro, rd, sec = setup
+    bg = np.array([0.2, 0.4, 0.6], np.float32)
+    flat = dict(sec, material=np.zeros(sc.P, np.int32), env=np.broadcast_to(bg, (4, 8, 3)).copy())
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    got = gpu_secondary(tr, sc, ro, rd, flat)
+    res = tr.trace_forward(T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P,
+                           T(sc.shs), 3, torch.empty(0, device=DEV), T(sc.opacities), torch.zeros(sc.P, device=DEV),
+                           torch.zeros(sc.P, device=DEV), T(bg), torch.zeros(5, device=DEV), 2, False).data
+    np.testing.assert_allclose(got["color"], res[0].cpu().numpy(), rtol=1e-6, atol=1e-7)
+    np.testing.assert_array_equal(got["others"], res[1].cpu().numpy())
+
+
+def test_autograd_module_and_state(setup):
+    sc, ro, rd, sec = setup
+    mod = SecondaryTracer(max_depth=2)
+    verts = T(sc.verts.reshape(-1)).requires_grad_(True)
+    opac = T(sc.opacities).requires_grad_(True)
+    shs = T(sc.shs).requires_grad_(True)
+    sigma = T(sc.sigma).requires_grad_(True)
+    args = (T(ro), T(rd), verts, sigma, T(sc.num_points), T(sc.cumsum), sc.P, opac, shs, T(sec["material"]),
+            T(sec["ior"]), T(sec["env"]))
+    for _ in range(2):  # build, then refit
+        color, others, maxb, scaling, density = mod(*args)
+        color.sum().backward()
+    torch.cuda.synchronize()
+    assert verts.grad.shape == verts.shape and shs.grad.shape == shs.shape
+    assert torch.isfinite(shs.grad).all() and shs.grad.abs().sum() > 0
+    # an adjoint without its forward is refused
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    with pytest.raises(RuntimeError, match="without a matching"):
+        tr.build_tri_accel(T(sc.verts), T(sc.cumsum), sc.P, True)
+        tr.trace_backward_secondary(T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points),
+                                    T(sc.cumsum), color.detach(), others, sc.P, T(sc.shs), 3, T(sc.opacities),
+                                    torch.zeros_like(color), torch.zeros_like(others), T(sec["material"]),
+                                    T(sec["ior"]), T(sec["env"]), 2)
