@@ -99,7 +99,8 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
   def.variant = TT_VARIANT_PLAIN;
   def.tmin_inclusive = 1;
   h->cfg = cfg ? *cfg : def;
-  if (h->cfg.variant < TT_VARIANT_PLAIN || h->cfg.variant > TT_VARIANT_ENVLIGHT) {
+  if (h->cfg.variant < TT_VARIANT_PLAIN || h->cfg.variant > TT_VARIANT_ENVLIGHT ||
+      (h->cfg.exact_adjoint != 0 && h->cfg.variant != TT_VARIANT_PLAIN)) {
     delete h;
     return TT_ERR_INVALID;
   }
@@ -169,6 +170,7 @@ static tt::TraceParams base_params(tt_tracer* h) {
   std::memset(&p, 0, sizeof(p));
   p.bvh = h->bvh.view();
   p.tmin_inclusive = h->cfg.tmin_inclusive;
+  p.exact = h->cfg.exact_adjoint;
   p.variant = h->cfg.variant;
   p.cfg = h->cfg_id;
   p.work = h->scratch.as<int>();
@@ -575,6 +577,7 @@ int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int 
 static int check_secondary(tt_tracer* h, const tt_secondary* sec, int P) {
   TT_REQUIRE(h, sec != nullptr, "null secondary-ray description");
   TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "secondary-ray passes need the plain program");
+  TT_REQUIRE(h, h->cfg.exact_adjoint == 0, "secondary-ray passes have the reference-style adjoint only");
   TT_REQUIRE(h, sec->max_depth >= 0 && sec->max_depth <= TT_MAX_BOUNCES, "max_depth must be in [0, 2]");
   TT_REQUIRE(h, sec->env && sec->env_h > 0 && sec->env_w > 0, "need an environment map [env_h][env_w][3]");
   TT_REQUIRE(h, P == 0 || (sec->material && sec->ior), "need material and ior per triangle");

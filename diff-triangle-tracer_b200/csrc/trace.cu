@@ -866,13 +866,17 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned ra
   }
 }
 
-// forward.cu:109-152 per hit and :204-214 per ray.
+// forward.cu:109-152 per hit and :204-214 per ray. EXACT (no reference
+// counterpart) also accumulates the depth channel, sum of w t, which the
+// reference leaves at 0.
+template <bool EXACT>
 struct FwdShader {
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
   float3 o, d;
   float C0, C1, C2, N0, N1, N2, T;
+  float D;  // EXACT only
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
   unsigned first_eval = 0;  // value of n_eval at the ray's first hit (record only)
 
@@ -884,6 +888,7 @@ struct FwdShader {
     o = ro;
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
+    D = 0.f;
     T = 1.0f;
     ++n_rays;
     if (v->record) {
@@ -926,6 +931,7 @@ struct FwdShader {
     N0 += g.n.x * w;
     N1 += g.n.y * w;
     N2 += g.n.z * w;
+    if (EXACT) D += w * g.t;
     float B[16];
     sh_basis(unit(d), p.sh_degree, B);
     const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
@@ -941,7 +947,7 @@ struct FwdShader {
     v->out_color[pix] = C0 + T * p.bg[0];
     v->out_color[HW + pix] = C1 + T * p.bg[1];
     v->out_color[2 * HW + pix] = C2 + T * p.bg[2];
-    v->out_others[kDepthCh * HW + pix] = 0.0f;  // the reference never accumulates depth
+    v->out_others[kDepthCh * HW + pix] = EXACT ? D : 0.0f;  // the reference never accumulates depth
     v->out_others[kAlphaCh * HW + pix] = 1.0f - T;
     v->out_others[(kNormalCh + 0) * HW + pix] = N0;
     v->out_others[(kNormalCh + 1) * HW + pix] = N1;
@@ -951,10 +957,10 @@ struct FwdShader {
   }
 };
 
-template <int CFG>
+template <int CFG, bool EXACT>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
   Counters cnt;
-  FwdShader sh(p);
+  FwdShader<EXACT> sh(p);
   run<CFG>(p, sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
@@ -1205,8 +1211,93 @@ __device__ __forceinline__ void window_bwd(const Geom& g, float dL_dphi, float3 
   }
 }
 
+// Exact adjoint of the window function (no reference counterpart), written
+// from its definition in A-relative coordinates (P0 = 0, P1 = e1, P2 = e2,
+// hit point q): edge k's unit normal en_k = s_k normalize(nc x (P_k - P_k+1))
+// with nc = e1 x e2, d_k = en_k . (q - P_k), phi = max d_k,
+// dist = en_0 . (I - P0), I the incenter, phi_final = phi / dist; the face
+// normal normalize(nc); q = o - A + t dir with t solving q . nc = 0. Inputs:
+// dL/dphi, dL/dCx sigma Cx (for dist), dL/dn and the depth term dL/dt.
+__device__ __noinline__ void window_bwd_exact(const Geom& g, float3 dir, float dL_dphi, float G, float3 dL_dn3,
+                                              float dL_dt_depth, float3 (&gv)[3]) {
+  const float3 P[3] = {make_float3(0.f, 0.f, 0.f), g.e1, g.e2};
+  const float3 nc = fcross(g.e1, g.e2);
+  const float la = flen(g.e1 - g.e2), lb = flen(g.e2), lc = flen(g.e1), sum = la + lb + lc;
+  const float3 inc = (lb * g.e1 + lc * g.e2) * (1.0f / sum);
+  float3 en[3];
+  en[0] = fnormalize(fcross(nc, -g.e1));
+  float dist = fdot(en[0], inc);
+  const bool flip0 = dist > 0.0f;
+  if (flip0) {
+    en[0] = -en[0];
+    dist = -dist;
+  }
+  en[1] = fnormalize(fcross(nc, g.e1 - g.e2));
+  en[2] = fnormalize(fcross(nc, g.e2));
+  const float dL_ddist = -G / dist;
+  gv[0] = gv[1] = gv[2] = make_float3(0.f, 0.f, 0.f);
+  float3 g_nc = make_float3(0.f, 0.f, 0.f);
+  auto edge_bwd = [&](int k, float3 g_en) {
+    const float3 e = P[k] - P[(k + 1) % 3];
+    const float3 ne = fcross(nc, e);
+    const float inv = 1.0f / flen(ne);
+    const float3 raw = ne * inv;
+    const float3 gr = (k == 0 && flip0) ? -g_en : g_en;
+    const float3 v = (gr - raw * fdot(raw, gr)) * inv;  // dL/d(ne)
+    g_nc = g_nc + fcross(e, v);
+    const float3 ge = fcross(v, nc);
+    gv[k] = gv[k] + ge;
+    gv[(k + 1) % 3] = gv[(k + 1) % 3] - ge;
+  };
+  float3 g_p = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (fabsf(g.d[k] - g.phi_max) > 1e-6f) continue;
+    edge_bwd(k, dL_dphi * (g.q - P[k]));
+    g_p = g_p + dL_dphi * en[k];
+    gv[k] = gv[k] - dL_dphi * en[k];
+  }
+  {
+    edge_bwd(0, dL_ddist * inc);
+    const float3 gI = dL_ddist * en[0];
+    gv[0] = gv[0] - gI;
+    gv[0] = gv[0] + (la / sum) * gI;
+    gv[1] = gv[1] + (lb / sum) * gI;
+    gv[2] = gv[2] + (lc / sum) * gI;
+    const float ga = fdot(gI, P[0] - inc) / sum, gb = fdot(gI, P[1] - inc) / sum, gc = fdot(gI, P[2] - inc) / sum;
+    const float3 bc = P[1] - P[2], ca = P[2] - P[0], ab = P[0] - P[1];
+    gv[1] = gv[1] + (ga / la) * bc;
+    gv[2] = gv[2] - (ga / la) * bc;
+    gv[2] = gv[2] + (gb / lb) * ca;
+    gv[0] = gv[0] - (gb / lb) * ca;
+    gv[0] = gv[0] + (gc / lc) * ab;
+    gv[1] = gv[1] - (gc / lc) * ab;
+  }
+  {
+    const float inv = 1.0f / flen(nc);
+    const float3 n = nc * inv;
+    g_nc = g_nc + (dL_dn3 - n * fdot(n, dL_dn3)) * inv;
+  }
+  {
+    const float dL_dt = fdot(g_p, dir) + dL_dt_depth;
+    const float sc = -dL_dt / fdot(dir, nc);
+    const float3 fB = fcross(g.e2, g.q), fC = fcross(g.q, g.e1);
+    gv[0] = gv[0] + sc * (-nc - fB - fC);
+    gv[1] = gv[1] + sc * fB;
+    gv[2] = gv[2] + sc * fC;
+  }
+  {
+    const float3 g1 = fcross(g.e2, g_nc), g2 = fcross(g_nc, g.e1);
+    gv[1] = gv[1] + g1;
+    gv[2] = gv[2] + g2;
+    gv[0] = gv[0] - g1 - g2;
+  }
+}
+
 // backward.cu:191-350: the same march, running C/N/D that include the current
-// hit, dL/dalpha from the final values, scattered gradients.
+// hit, dL/dalpha from the final values, scattered gradients. EXACT: the full
+// chain rule of window_bwd_exact, and no gradient through a clamped alpha.
+template <bool EXACT>
 struct BwdShader {
   const TraceParams& p;
   const ViewDesc* v;
@@ -1278,12 +1369,16 @@ struct BwdShader {
     dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
     dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
                  gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
-    red_add(p.d_opac + prim, dL_dalpha * g.Cx);
-    const float dL_dC = opacity * dL_dalpha;
+    const bool live = !EXACT || opacity * g.Cx < kAlphaMax;
+    const float dL_dC = live ? opacity * dL_dalpha : 0.0f;
+    if (live) red_add(p.d_opac + prim, dL_dalpha * g.Cx);
     if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
     const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
     float3 gv[3];
-    window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
+    if (EXACT)
+      window_bwd_exact(g, d, dL_dphi, dL_dC * sig * g.Cx, make_float3(gN0 * w, gN1 * w, gN2 * w), gD * w, gv);
+    else
+      window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
     float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -1323,10 +1418,10 @@ struct BwdShader {
   __device__ __forceinline__ void end() {}
 };
 
-template <int CFG>
+template <int CFG, bool EXACT>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
   Counters cnt;
-  BwdShader sh(p);
+  BwdShader<EXACT> sh(p);
   run<CFG>(p, sh, cnt);
 }
 
@@ -1880,9 +1975,9 @@ size_t trace_smem_bytes(int cfg) {
 
 namespace {
 template <int CFG>
-const void* fwd_fn() { return (const void*)k_forward<CFG>; }
+const void* fwd_fn() { return (const void*)k_forward<CFG, false>; }
 template <int CFG>
-const void* bwd_fn() { return (const void*)k_backward<CFG>; }
+const void* bwd_fn() { return (const void*)k_backward<CFG, false>; }
 const void* kernel_for(int which, int cfg) {
   switch (cfg) {
     case kCfgPackets16: return which == 0 ? fwd_fn<kCfgPackets16>() : bwd_fn<kCfgPackets16>();
@@ -1901,28 +1996,38 @@ int trace_blocks_per_sm(int which, int cfg) {
   return n > 0 ? n : 1;
 }
 
+template <bool EXACT>
+cudaError_t launch_forward_t(const TraceParams& p, int grid, cudaStream_t s) {
+  switch (p.cfg) {
+    case kCfgPackets16: k_forward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_forward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_forward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_forward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+  }
+  return cudaGetLastError();
+}
+
+template <bool EXACT>
+cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
+  switch (p.cfg) {
+    case kCfgPackets16: k_backward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_backward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_backward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_backward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {
   if (p.variant != 0) {
     k_variant<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
     return cudaGetLastError();
   }
-  switch (p.cfg) {
-    case kCfgPackets16: k_forward<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
-    case kCfgPackets32: k_forward<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
-    case kCfgLanes24: k_forward<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
-    default: k_forward<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
-  }
-  return cudaGetLastError();
+  return p.exact ? launch_forward_t<true>(p, grid, s) : launch_forward_t<false>(p, grid, s);
 }
 
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
-  switch (p.cfg) {
-    case kCfgPackets16: k_backward<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
-    case kCfgPackets32: k_backward<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
-    case kCfgLanes24: k_backward<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
-    default: k_backward<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
-  }
-  return cudaGetLastError();
+  return p.exact ? launch_backward_t<true>(p, grid, s) : launch_backward_t<false>(p, grid, s);
 }
 
 int sec_blocks_per_sm(int which) {

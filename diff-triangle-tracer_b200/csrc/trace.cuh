@@ -81,6 +81,7 @@ struct TraceParams {
   float sph_r, sph_cx, sph_cy, sph_cz;
   int samples;
   int tmin_inclusive;
+  int exact;    // 1: exact adjoint (and depth accumulated by the forward)
   int cfg;      // traversal configuration, kCfg*
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits

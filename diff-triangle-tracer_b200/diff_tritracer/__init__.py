@@ -105,9 +105,11 @@ class Tracer(nn.Module):
     in the reference ("forward.ptx", "reflect.ptx", "refract.ptx",
     "envlight.ptx" / "backward.ptx"); nothing is read from disk."""
 
-    def __init__(self, forwad_ptx="forward.ptx", backward_ptx="backward.ptx", tmin_inclusive: bool = True) -> None:
+    def __init__(self, forwad_ptx="forward.ptx", backward_ptx="backward.ptx", tmin_inclusive: bool = True,
+                 exact_adjoint: bool = False) -> None:
         super().__init__()
-        self.tracer = _C.OptixTracer("", forwad_ptx, backward_ptx, tmin_inclusive=tmin_inclusive)
+        self.tracer = _C.OptixTracer("", forwad_ptx, backward_ptx, tmin_inclusive=tmin_inclusive,
+                                     exact_adjoint=exact_adjoint)
 
     def forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,
                 number_of_points, opacities, scaling, density_factor, shs, colors_precomp,

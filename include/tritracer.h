@@ -68,7 +68,12 @@ typedef struct tt_config {
   int k;              /* hits gathered per traversal: 16 (0 = default) or 32 (packets
                          only); compositing keeps the reference's 16-hit chunks */
   int stack_depth;    /* per-lane traversal stack: 32 (0 = default) or 24 (lanes only) */
-  int reserved[3];    /* zero */
+  int exact_adjoint;  /* 0 (default): the reference's gradients (backward.cu), whose vertex
+                         gradient leaves out how the incenter distance, the hit point and t
+                         move; 1: the full chain rule, no gradient through a clamped alpha, and
+                         the forward accumulates depth (out_others channel 0 = sum w t). No
+                         reference counterpart; plain program only */
+  int reserved[2];    /* zero */
 } tt_config;
 
 /* Arguments of the forward trace: OptixTracer::trace_fwd

@@ -42,5 +42,6 @@ struct or_args {
   const float* ior;
   const float* env;
   int env_h, env_w, max_depth;
+  int exact_adjoint;  // 1: full chain rule + forward depth (FP64 with exact geometry)
 };
 }

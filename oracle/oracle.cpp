@@ -49,6 +49,7 @@ static Opts to_opts(const or_args* a, bool fp64) {
   o.canonical_ties = a->canonical_ties != 0;
   o.exact_geometry = fp64 && a->exact_geometry != 0;
   o.mt = a->nthreads > 1;
+  o.exact_adjoint = fp64 && a->exact_adjoint != 0;
   return o;
 }
 

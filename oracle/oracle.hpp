@@ -250,6 +250,7 @@ inline void atomic_max(R* p, R v, bool mt) {
 
 // ---------------------------------------------------------------- options
 struct Opts {
+  bool exact_adjoint = false;   // full chain rule + depth accumulation (no reference counterpart)
   bool tmin_inclusive = true;   // optixTrace's closed [tmin, tmax]
   bool canonical_ties = false;  // order equal-t hits by primitive id
   bool exact_geometry = false;  // hit point from an FP64 plane intersection
@@ -401,6 +402,9 @@ struct Window {
   V3<R> n;
   R phi_final, phi_max;
   R d[3];
+  R dist;         // signed distance of the incenter to edge 0
+  V3<R> incenter;
+  V3<R> en[3];    // edge normals as used (edge 0 oriented by the incenter)
 };
 
 template <class R>
@@ -430,7 +434,10 @@ inline Window<R> window_fn(const Inputs& in, int prim, V3<R> hit_p) {
     const R ed = dot(en, hit_p) + offset;
     phi = std::fmax(phi, ed);
     w.d[i] = ed;
+    w.en[i] = en;
   }
+  w.dist = dist;
+  w.incenter = incenter;
   w.phi_max = phi;
   w.phi_final = phi / dist;
   w.Cx = std::fmax(R(0), fast_pow<R>(w.phi_final, (R)in.sigma[prim]));
@@ -545,7 +552,7 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
   ray_interval(in, pix, t_near, t_far);
   R C[3] = {0, 0, 0}, N[3] = {0, 0, 0};
   R T = 1;
-  const R D = 0;  // the reference never accumulates depth in the forward pass
+  R D = 0;  // the reference never accumulates depth; the exact adjoint's forward does
   march(
       sc, rp, opt,
       [&](uint32_t prim, float t) -> bool {
@@ -564,6 +571,7 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
         N[0] += w.n.x * bw;
         N[1] += w.n.y * bw;
         N[2] += w.n.z * bw;
+        if (opt.exact_adjoint) D += bw * hit_dist(in, (int)prim, o, d, t, opt);
         const V3<R> col = sh_color(in, (int)prim, d, nullptr);
         C[0] += col.x * bw;
         C[1] += col.y * bw;
@@ -844,6 +852,90 @@ inline void window_bwd(const Inputs& in, int prim, V3<R> hit_p, R dL_dphi_x, R p
   }
 }
 
+// Exact adjoint (no reference counterpart): the complete chain rule of the
+// window function, written from its definition (not from backward.cu's
+// partial Jacobians). nc = (B - A) x (C - A); edge k's unit normal
+// en_k = s_k normalize(nc x (P_k - P_k+1)) (s_0 orients edge 0 by the
+// incenter); d_k = en_k . (p - P_k); phi = max d_k; dist = en_0 . (I - A),
+// I = (a A + b B + c C) / (a + b + c); phi_final = phi / dist; the face
+// normal n = normalize(nc); the hit point p = o + t d with t solving
+// (p - A) . nc = 0, so dt/dX = -(df/dX) / (d . nc). Inputs: dL/dphi,
+// dL/ddist, dL/dn and the depth term dL/dt = dL/dD w.
+template <class R>
+inline void window_bwd_exact(const Inputs& in, int prim, V3<R> dir, V3<R> hit_p, const Window<R>& w, R dL_dphi,
+                             R dL_ddist, V3<R> dL_dn, R dL_dt_depth, R* dtri, bool mt) {
+  const int off = in.cumsum[prim];
+  const V3<R> P[3] = {vert<R>(in, off), vert<R>(in, off + 1), vert<R>(in, off + 2)};
+  const V3<R> e1 = P[1] - P[0], e2 = P[2] - P[0];
+  const V3<R> nc = cross(e1, e2);
+  V3<R> gP[3] = {mk<R>(0, 0, 0), mk<R>(0, 0, 0), mk<R>(0, 0, 0)};
+  V3<R> g_nc = mk<R>(0, 0, 0);
+  // unit normal of edge k, given dL/d(en_k)
+  auto edge_bwd = [&](int k, V3<R> g_en) {
+    const V3<R> e = P[k] - P[(k + 1) % 3];
+    const V3<R> ne = cross(nc, e);
+    const R len = length(ne);
+    const V3<R> raw = ne * (R(1) / len);
+    const R sgn = dot(raw, w.en[k]) < R(0) ? R(-1) : R(1);
+    const V3<R> gr = sgn * g_en;
+    const V3<R> v = (gr - raw * dot(raw, gr)) * (R(1) / len);  // dL/d(ne)
+    g_nc = g_nc + cross(e, v);
+    const V3<R> ge = cross(v, nc);
+    gP[k] = gP[k] + ge;
+    gP[(k + 1) % 3] = gP[(k + 1) % 3] - ge;
+  };
+  // phi = d_m at every edge at the maximum
+  V3<R> g_p = mk<R>(0, 0, 0);
+  for (int k = 0; k < 3; ++k) {
+    if (std::fabs(w.d[k] - w.phi_max) > R(1e-6f)) continue;
+    edge_bwd(k, dL_dphi * (hit_p - P[k]));
+    g_p = g_p + dL_dphi * w.en[k];
+    gP[k] = gP[k] - dL_dphi * w.en[k];
+  }
+  // dist = en_0 . (I - A)
+  {
+    edge_bwd(0, dL_ddist * (w.incenter - P[0]));
+    const V3<R> gI = dL_ddist * w.en[0];
+    gP[0] = gP[0] - gI;
+    const R a = length(P[1] - P[2]), b = length(P[2] - P[0]), c = length(P[0] - P[1]), sum = a + b + c;
+    const V3<R> I = w.incenter;
+    gP[0] = gP[0] + (a / sum) * gI;
+    gP[1] = gP[1] + (b / sum) * gI;
+    gP[2] = gP[2] + (c / sum) * gI;
+    const R ga = dot(gI, P[0] - I) / sum, gb = dot(gI, P[1] - I) / sum, gc = dot(gI, P[2] - I) / sum;
+    gP[1] = gP[1] + (ga / a) * (P[1] - P[2]);
+    gP[2] = gP[2] - (ga / a) * (P[1] - P[2]);
+    gP[2] = gP[2] + (gb / b) * (P[2] - P[0]);
+    gP[0] = gP[0] - (gb / b) * (P[2] - P[0]);
+    gP[0] = gP[0] + (gc / c) * (P[0] - P[1]);
+    gP[1] = gP[1] - (gc / c) * (P[0] - P[1]);
+  }
+  // face normal n = nc / |nc|
+  {
+    const R len = length(nc);
+    const V3<R> n = nc * (R(1) / len);
+    g_nc = g_nc + (dL_dn - n * dot(n, dL_dn)) * (R(1) / len);
+  }
+  // t from the plane, with dL/dt from the hit point and the depth
+  {
+    const R dL_dt = dot(g_p, dir) + dL_dt_depth;
+    const V3<R> u = hit_p - P[0];
+    const R s = -dL_dt / dot(dir, nc);
+    const V3<R> fB = cross(e2, u), fC = cross(u, e1);
+    gP[0] = gP[0] + s * (-nc - fB - fC);
+    gP[1] = gP[1] + s * fB;
+    gP[2] = gP[2] + s * fC;
+  }
+  // nc = e1 x e2
+  {
+    const V3<R> g1 = cross(e2, g_nc), g2 = cross(g_nc, e1);
+    gP[1] = gP[1] + g1;
+    gP[2] = gP[2] + g2;
+    gP[0] = gP[0] - g1 - g2;
+  }
+  for (int k = 0; k < 3; ++k) add3(dtri, off + k, gP[k], mt);
+}
+
 // backward.cu:191-350: re-march with the forward's decisions, keeping running
 // C/N/D that include the current hit, and take each hit's alpha gradient from
 // the difference to the final values.
@@ -901,14 +993,23 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
         dL_dalpha += dL_ddepth * (T * hit_t - (final_depth - D) * inv_1_alpha);
         const V3<R> Nf = mk<R>(N[0], N[1], N[2]);
         dL_dalpha += sum3(vmul(dL_dnormal2D, T * w.n - (final_normal - Nf) * inv_1_alpha));
-        atomic_add(&bo.dopac[prim], dL_dalpha * w.Cx, opt.mt);
-        const R dL_dC = opacity * dL_dalpha;
+        // the exact adjoint honours the alpha clamp (no gradient through a
+        // clamped alpha); the reference differentiates through it
+        const bool live = !opt.exact_adjoint || opacity * w.Cx < R(kAlphaMax);
+        const R dL_dC = live ? opacity * dL_dalpha : R(0);
+        if (live) atomic_add(&bo.dopac[prim], dL_dalpha * w.Cx, opt.mt);
         if (w.phi_final > R(0)) {
           atomic_add(&bo.dsigma[prim], dL_dC * w.Cx * fast_log<R>(w.phi_final), opt.mt);
         }
         const R dL_dphi_x = (R)in.sigma[prim] / w.phi_max * dL_dC * w.Cx;
         const V3<R> dL_dnormal = dL_dnormal2D * bw;
-        window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, dL_dnormal, bo.dtri, opt.mt);
+        if (opt.exact_adjoint) {
+          const R dL_ddist = -dL_dC * (R)in.sigma[prim] * w.Cx / w.dist;
+          window_bwd_exact(in, (int)prim, d, hp, w, dL_dphi_x, dL_ddist, dL_dnormal, dL_ddepth * bw, bo.dtri,
+                           opt.mt);
+        } else {
+          window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, dL_dnormal, bo.dtri, opt.mt);
+        }
         sh_color_bwd(in, (int)prim, d, clamped, dL_dcolor, bo.dsh, opt.mt);
         T = test_T;
         return false;

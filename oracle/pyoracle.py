@@ -40,7 +40,7 @@ class OrArgs(ctypes.Structure):
         ("max_rec", ctypes.c_int), ("rec_ids", _ip), ("rec_count", _ip), ("margin", _fp),
         ("interval", _fp),
         ("material", _ip), ("ior", _fp), ("env", _fp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
-        ("max_depth", ctypes.c_int),
+        ("max_depth", ctypes.c_int), ("exact_adjoint", ctypes.c_int),
     ]
 
 
@@ -147,8 +147,9 @@ class _Runner:
 
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
                 canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None,
-                interval=None, secondary=None):
+                interval=None, secondary=None, exact_adjoint=False):
         a, keep = self._args(scene, ray_o, ray_d, bg, extra, variant, tmin_inclusive, canonical, exact, nthreads, rows)
+        a.exact_adjoint = int(exact_adjoint)
         self._interval(a, keep, interval)
         sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64
@@ -179,8 +180,9 @@ class _Runner:
 
     def backward(self, scene, ray_o, ray_d, colors, others, dL_dpixels, dL_dothers, bg=None, precision=32,
                  tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None,
-                 secondary=None):
+                 secondary=None, exact_adjoint=False):
         a, keep = self._args(scene, ray_o, ray_d, bg, None, 0, tmin_inclusive, canonical, exact, nthreads, rows)
+        a.exact_adjoint = int(exact_adjoint)
         self._interval(a, keep, interval)
         sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64

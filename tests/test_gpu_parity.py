@@ -260,3 +260,34 @@ def test_sphere_variants_vs_fp64_oracle(oracle, prog, variant):
     g, go = scenes.upstream_grads(H, W, seed=3)
     grads = gpu_backward(tr, sc, ro, rd, settings(bg=bg), out["color"], out["others"], g, go)
     assert all(np.isfinite(v).all() for v in grads.values())
+
+
+@pytest.mark.parametrize("traversal", ["packets", "lanes"])
+def test_exact_adjoint_vs_fp64_oracle(oracle, traversal):
+    """exact_adjoint=True: the forward accumulates depth and the adjoint is the
+    full chain rule (checked against finite differences on the CPU oracle in
+    test_oracle_fd.py); the GPU's FP32 evaluation against the FP64 oracle."""
+    sc, (ro, rd) = dense_scene(seed=1, P=3000), dense_view(H=48, W=64)
+    H, W = ro.shape[:2]
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal=traversal, exact_adjoint=True)
+    kw = dict(precision=64, exact=True, canonical=True, nthreads=8, exact_adjoint=True)
+    ref = oracle.forward(sc, ro, rd, record=256, **kw)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    g, go = scenes.upstream_grads(H, W, seed=12, others_std=1.0)
+    g, go = g * ok[None], go * ok[None]
+    out = gpu_forward(tr, sc, ro, rd, settings())
+    assert np.abs(out["others"][0]).max() > 1.0  # depth is accumulated
+    a, b = out["others"][:, ok], ref.others[:, ok]
+    assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + ATOL)
+    grads = gpu_backward(tr, sc, ro, rd, settings(), out["color"], out["others"], g, go)
+    tr.device_status()
+    rb = oracle.backward(sc, ro, rd, ref.color, ref.others, g, go, **kw)
+    for key, tol in (("dtri", 1e-3), ("dsigma", GRAD_RTOL), ("dopac", GRAD_RTOL), ("dsh", GRAD_RTOL)):
+        e = rel_norm(grads[key], getattr(rb, key))
+        print(f"exact {traversal} {key}: rel L2 {e:.2e}")
+        assert e < tol, (key, e)
+    # and it differs from the reference's partial vertex gradient
+    plain = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal=traversal)
+    pout = gpu_forward(plain, sc, ro, rd, settings())
+    pg = gpu_backward(plain, sc, ro, rd, settings(), pout["color"], pout["others"], g, go)
+    assert rel_norm(pg["dtri"], grads["dtri"]) > 0.1
