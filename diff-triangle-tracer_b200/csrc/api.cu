@@ -77,11 +77,11 @@ int accel_step(tt_tracer* h, const float* verts, int num_vertices, const int* cu
   return TT_OK;
 }
 
-int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P) {
+int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P, const float* cols = nullptr) {
+  if (cols && !shs) return TT_OK;  // precomputed colours in place of SH
   TT_REQUIRE(h, deg >= 0 && deg <= 3, "sh_degree must be in [0, 3]");
   TT_REQUIRE(h, M >= (deg + 1) * (deg + 1), "shs has fewer coefficients per triangle than sh_degree needs");
-  TT_REQUIRE(h, P == 0 || shs != nullptr,
-             "shs is empty: the reference path evaluates SH only (colors_precomp is never read)");
+  TT_REQUIRE(h, P == 0 || shs != nullptr, "shs is empty and no colors_precomp was given");
   return TT_OK;
 }
 
@@ -217,7 +217,9 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
                               a->num_points),
              "null per-triangle pointer");
   TT_REQUIRE(h, a->bg, "null background");
-  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  const float* cols = a->shs ? nullptr : a->colors_precomp;
+  TT_REQUIRE(h, !cols || h->cfg.variant == TT_VARIANT_PLAIN, "colors_precomp needs the plain program");
+  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P, cols);
   if (rc != TT_OK) return rc;
   float ex[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   if (h->cfg.variant != TT_VARIANT_PLAIN) {
@@ -241,6 +243,7 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   p.shs = a->shs;
   p.sh_degree = a->sh_degree;
   p.M = a->M;
+  p.cols = cols;
   p.opac = a->opacities;
   p.sigma = a->sigma;
   p.bg = a->bg;
@@ -296,9 +299,11 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
     TT_REQUIRE(h, views[i].colors && views[i].others && views[i].dL_dpixels && views[i].dL_dothers,
                "null forward-output or upstream-gradient pointer in a view");
   TT_REQUIRE(h, a->P == 0 || (a->opacities && a->sigma && a->cumsum && a->vertices), "null per-triangle pointer");
-  TT_REQUIRE(h, a->P == 0 || (a->dL_dtriangle && a->dL_dsigma && a->dL_dopacity && a->dL_dsh),
+  const float* cols = a->shs ? nullptr : a->colors_precomp;
+  TT_REQUIRE(h, a->P == 0 || (a->dL_dtriangle && a->dL_dsigma && a->dL_dopacity && (a->dL_dsh || cols)),
              "null gradient output");
-  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P);
+  TT_REQUIRE(h, !cols || a->dL_dcolors, "colors_precomp needs a dL_dcolors output");
+  int rc = check_sh(h, a->shs, a->sh_degree, a->M, a->P, cols);
   if (rc != TT_OK) return rc;
   if (!h->bvh.built()) return fail(h, TT_ERR_STATE, "backward before any forward/build");
   if (h->bvh.P() != a->P) return fail(h, TT_ERR_STATE, "backward with a different triangle count than the forward");
@@ -311,7 +316,8 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
     TT_CUDA(h, cudaMemsetAsync(a->dL_dtriangle, 0, (size_t)a->num_vertices * 3 * sizeof(float), s));
     TT_CUDA(h, cudaMemsetAsync(a->dL_dsigma, 0, (size_t)a->P * sizeof(float), s));
     TT_CUDA(h, cudaMemsetAsync(a->dL_dopacity, 0, (size_t)a->P * sizeof(float), s));
-    TT_CUDA(h, cudaMemsetAsync(a->dL_dsh, 0, (size_t)a->P * a->M * 3 * sizeof(float), s));
+    if (a->dL_dsh && a->M > 0) TT_CUDA(h, cudaMemsetAsync(a->dL_dsh, 0, (size_t)a->P * a->M * 3 * sizeof(float), s));
+    if (cols) TT_CUDA(h, cudaMemsetAsync(a->dL_dcolors, 0, (size_t)a->P * 3 * sizeof(float), s));
   }
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
@@ -319,6 +325,8 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
   p.shs = a->shs;
   p.sh_degree = a->sh_degree;
   p.M = a->M;
+  p.cols = cols;
+  p.d_cols = a->dL_dcolors;
   p.opac = a->opacities;
   p.sigma = a->sigma;
   p.bg = a->bg;
@@ -751,6 +759,30 @@ int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary
     TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (a->gpu_time_ms) *a->gpu_time_ms = ms;
   }
+  return TT_OK;
+}
+
+// ---------------------------------------------------------------- BVH files
+int tt_bvh_save(tt_tracer* h, void* dst, unsigned long long capacity, unsigned long long* bytes, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, bytes != nullptr, "null size pointer");
+  if (!h->bvh.built() || h->bvh.P() <= 0) return fail(h, TT_ERR_STATE, "no acceleration structure to save");
+  size_t n = 0;
+  const cudaError_t e = h->bvh.save(dst, (size_t)capacity, &n, as_stream(stream));
+  *bytes = n;
+  if (e == cudaErrorInvalidValue) return fail(h, TT_ERR_INVALID, "destination buffer too small");
+  if (e != cudaSuccess) return cuda_fail(h, e, "bvh save");
+  return TT_OK;
+}
+
+int tt_bvh_load(tt_tracer* h, const void* src, unsigned long long bytes, const float* vertices, int num_vertices,
+                const int* cumsum, int P, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, src && vertices && cumsum && P > 0 && num_vertices >= 3, "need a blob, vertices and cumsum");
+  cudaError_t e = cudaSuccess;
+  if (h->bvh.load(src, (size_t)bytes, vertices, cumsum, P, as_stream(stream), &e) != 0)
+    return fail(h, TT_ERR_INVALID, "not a BVH blob for this triangle count");
+  if (e != cudaSuccess) return cuda_fail(h, e, "bvh load");
   return TT_OK;
 }
 

@@ -14,6 +14,8 @@
 // A refit re-runs prep/records/bottom-up/boxes over the same topology.
 #include <cstdio>
 
+#include <cstring>
+
 #include "bvh.cuh"
 
 namespace tt {
@@ -598,6 +600,95 @@ cudaError_t Bvh::refit(const float* verts, const int* cumsum, int P, cudaStream_
   k_records<<<blocks_for(P), kBlock, 0, s>>>(vals_.as<uint32_t>(), tri_prim_.as<float4>(), P,
                                              tri_sorted_.as<float4>());
   return boxes(s);
+}
+
+namespace {
+struct BlobHeader {
+  char magic[8];  // "TTBVH\0\0\1"
+  int P, nw;      // triangles, wide nodes
+  long long pad;
+};
+constexpr char kBlobMagic[8] = {'T', 'T', 'B', 'V', 'H', 0, 0, 1};
+
+size_t blob_bytes(int P, int nw) {
+  const size_t p = (size_t)P, b = P > 1 ? (size_t)P - 1 : 1;
+  return sizeof(BlobHeader) + p * 4 + b * sizeof(BinNode) + b * 4 + p * 4 + (size_t)nw * kWide * 4 +
+         (size_t)nw * kNodeF4 * sizeof(float4);
+}
+}  // namespace
+
+cudaError_t Bvh::save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s) {
+  if (!built_ || P_ <= 0) {
+    *bytes = 0;
+    return cudaSuccess;
+  }
+  int cnt[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(cnt, counters_.p, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  const int nw = cnt[0];
+  *bytes = blob_bytes(P_, nw);
+  if (!dst) return cudaSuccess;
+  if (capacity < *bytes) return cudaErrorInvalidValue;
+  const size_t p = (size_t)P_, b = P_ > 1 ? (size_t)P_ - 1 : 1;
+  char* o = static_cast<char*>(dst);
+  BlobHeader hd;
+  std::memcpy(hd.magic, kBlobMagic, 8);
+  hd.P = P_;
+  hd.nw = nw;
+  hd.pad = 0;
+  std::memcpy(o, &hd, sizeof(hd));
+  o += sizeof(hd);
+  auto d2h = [&](const DevBuf& buf, size_t n) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(o, buf.p, n, cudaMemcpyDeviceToHost, s);
+    o += n;
+  };
+  d2h(vals_, p * 4);
+  d2h(bnode_, b * sizeof(BinNode));
+  d2h(bparent_, b * 4);
+  d2h(lparent_, p * 4);
+  d2h(wsrc_, (size_t)nw * kWide * 4);
+  d2h(wnodes_, (size_t)nw * kNodeF4 * sizeof(float4));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
+
+int Bvh::load(const void* src, size_t bytes, const float* verts, const int* cumsum, int P, cudaStream_t s,
+              cudaError_t* err) {
+  *err = cudaSuccess;
+  BlobHeader hd;
+  if (!src || bytes < sizeof(hd)) return 1;
+  std::memcpy(&hd, src, sizeof(hd));
+  if (std::memcmp(hd.magic, kBlobMagic, 8) != 0 || hd.P != P || P <= 0 || hd.nw < 1 ||
+      hd.nw > (P > 1 ? P - 1 : 1) || bytes != blob_bytes(P, hd.nw))
+    return 1;
+  built_ = false;
+  if ((*err = reserve(P)) != cudaSuccess) return 0;
+  const size_t p = (size_t)P, b = P > 1 ? (size_t)P - 1 : 1;
+  const char* in = static_cast<const char*>(src) + sizeof(hd);
+  cudaError_t e = cudaSuccess;
+  auto h2d = [&](DevBuf& buf, size_t n) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf.p, in, n, cudaMemcpyHostToDevice, s);
+    in += n;
+  };
+  h2d(vals_, p * 4);
+  h2d(bnode_, b * sizeof(BinNode));
+  h2d(bparent_, b * 4);
+  h2d(lparent_, p * 4);
+  h2d(wsrc_, (size_t)hd.nw * kWide * 4);
+  h2d(wnodes_, (size_t)hd.nw * kNodeF4 * sizeof(float4));
+  const int cnt[4] = {hd.nw, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(counters_.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s);
+  // the host blob and cnt may go away on return
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    *err = e;
+    return 0;
+  }
+  P_ = P;
+  built_ = true;
+  *err = refit(verts, cumsum, P, s);  // triangle records and boxes from the vertices
+  return 0;
 }
 
 void Bvh::release() {

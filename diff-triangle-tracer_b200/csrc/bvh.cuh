@@ -38,6 +38,14 @@ class Bvh {
   const int* counters() const { return counters_.as<int>(); }
   // kernels enqueued by build/refit so far
   unsigned long long launches() const { return launches_; }
+  // Serialised topology: a host blob of the Morton order, the binary and
+  // 8-wide hierarchies (not the triangle records or boxes, which load()
+  // rebuilds from the vertices with a refit). save() synchronises `s`; with
+  // dst == nullptr it only reports the size.
+  cudaError_t save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s);
+  // 1: bad blob (magic, version, size or triangle count), else a CUDA error
+  int load(const void* src, size_t bytes, const float* verts, const int* cumsum, int P, cudaStream_t s,
+           cudaError_t* err);
 
  private:
   cudaError_t reserve(int P);

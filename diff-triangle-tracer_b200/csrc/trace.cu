@@ -932,12 +932,18 @@ struct FwdShader {
     N1 += g.n.y * w;
     N2 += g.n.z * w;
     if (EXACT) D += w * g.t;
-    float B[16];
-    sh_basis(unit(d), p.sh_degree, B);
-    const float3 c = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
-    C0 += fmaxf(c.x, 0.f) * w;
-    C1 += fmaxf(c.y, 0.f) * w;
-    C2 += fmaxf(c.z, 0.f) * w;
+    float3 c;
+    if (p.cols) {  // precomputed colours in place of SH
+      c = make_float3(__ldg(p.cols + 3 * prim), __ldg(p.cols + 3 * prim + 1), __ldg(p.cols + 3 * prim + 2));
+    } else {
+      float B[16];
+      sh_basis(unit(d), p.sh_degree, B);
+      const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+      c = make_float3(fmaxf(raw.x, 0.f), fmaxf(raw.y, 0.f), fmaxf(raw.z, 0.f));
+    }
+    C0 += c.x * w;
+    C1 += c.y * w;
+    C2 += c.z * w;
     T = test_T;
     return false;
   }
@@ -1352,9 +1358,15 @@ struct BwdShader {
     if (test_T < kTMin) return true;
     const float w = alpha * T;
     float B[16];
-    sh_basis(unit(d), p.sh_degree, B);
-    const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
-    const float c0 = fmaxf(raw.x, 0.f), c1 = fmaxf(raw.y, 0.f), c2 = fmaxf(raw.z, 0.f);
+    float3 raw;
+    if (p.cols) {  // precomputed colours in place of SH
+      raw = make_float3(__ldg(p.cols + 3 * prim), __ldg(p.cols + 3 * prim + 1), __ldg(p.cols + 3 * prim + 2));
+    } else {
+      sh_basis(unit(d), p.sh_degree, B);
+      raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+    }
+    const float c0 = p.cols ? raw.x : fmaxf(raw.x, 0.f), c1 = p.cols ? raw.y : fmaxf(raw.y, 0.f),
+                c2 = p.cols ? raw.z : fmaxf(raw.z, 0.f);
     C0 += c0 * w;
     C1 += c1 * w;
     C2 += c2 * w;
@@ -1385,6 +1397,13 @@ struct BwdShader {
       red_add(dt + 3 * k + 0, gv[k].x);
       red_add(dt + 3 * k + 1, gv[k].y);
       red_add(dt + 3 * k + 2, gv[k].z);
+    }
+    if (p.cols) {
+      red_add(p.d_cols + 3 * prim + 0, g0 * w);
+      red_add(p.d_cols + 3 * prim + 1, g1 * w);
+      red_add(p.d_cols + 3 * prim + 2, g2 * w);
+      T = test_T;
+      return false;
     }
     // SH: dRGB/dsh_k = B_k, masked where the colour was clamped at 0
     const float e0 = raw.x < 0.f ? 0.f : g0 * w, e1 = raw.y < 0.f ? 0.f : g1 * w, e2 = raw.z < 0.f ? 0.f : g2 * w;

@@ -64,6 +64,8 @@ struct TraceParams {
   const int* num_points;
   const float* shs;
   int sh_degree, M;
+  const float* cols;  // [P][3] precomputed colours in place of SH (shs NULL), or NULL
+  float* d_cols;      // their gradient (adjoint)
   const float* opac;
   const float* sigma;
   const float* bg;

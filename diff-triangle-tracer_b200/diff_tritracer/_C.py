@@ -114,6 +114,34 @@ class OptixTracer:
         check(self._h, lib.tt_build(self._h, _ptr(verts), verts.numel() // 3, _ptr(cumsum), int(number_of_points),
                                     mode, _stream()))
 
+    def save_bvh(self, path=None):
+        """Serialises the acceleration structure's topology (bytes; also
+        written to `path` when given). No reference counterpart."""
+        n = ctypes.c_ulonglong(0)
+        check(self._h, lib.tt_bvh_save(self._h, None, 0, ctypes.byref(n), _stream()))
+        buf = ctypes.create_string_buffer(n.value)
+        check(self._h, lib.tt_bvh_save(self._h, buf, n.value, ctypes.byref(n), _stream()))
+        blob = buf.raw[:n.value]
+        if path is not None:
+            with open(path, "wb") as f:
+                f.write(blob)
+        return blob
+
+    def load_bvh(self, blob_or_path, triangles_points, cumsum_of_points_per_triangle, number_of_points):
+        """Restores a saved topology and refits it to these vertices (the
+        same triangles), instead of building: the next trace may use
+        rebuild_gas = 2 (keep) or 1 (refit)."""
+        blob = blob_or_path
+        if not isinstance(blob, (bytes, bytearray)):
+            with open(blob_or_path, "rb") as f:
+                blob = f.read()
+        verts = _f32(triangles_points, "triangles_points", self.device)
+        cumsum = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", self.device)
+        buf = ctypes.create_string_buffer(bytes(blob), len(blob))
+        check(self._h, lib.tt_bvh_load(self._h, buf, len(blob), _ptr(verts), verts.numel() // 3, _ptr(cumsum),
+                                       int(number_of_points), _stream()))
+        self._keep = (verts, cumsum)
+
     def trace_forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
                       cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, colors_precomp, opacities,
                       scaling, density_factor, bg_color, extra, rebuild_gas_opt, debug):
@@ -149,8 +177,11 @@ class OptixTracer:
         a.ray_o, a.ray_d = _ptr(ro), _ptr(rd)
         a.vertices, a.num_vertices = _ptr(verts), verts.numel() // 3
         a.num_points, a.cumsum, a.P = _ptr(npts), _ptr(cums), P
-        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
-        a.colors_precomp = ctypes.c_void_p(0)
+        a.shs, a.sh_degree, a.M = (_ptr(sh) if sh.numel() else ctypes.c_void_p(0)), int(sh_degree), M
+        cp = None
+        if sh.numel() == 0 and isinstance(colors_precomp, torch.Tensor) and colors_precomp.numel():
+            cp = _f32(colors_precomp, "colors_precomp", dev)  # [P, 3] in place of SH
+        a.colors_precomp = _ptr(cp) if cp is not None else ctypes.c_void_p(0)
         a.opacities, a.sigma = _ptr(opac), _ptr(sig)
         a.scaling, a.density_factor = _ptr(sc), _ptr(de)
         a.bg = _ptr(bg)
@@ -176,14 +207,16 @@ class OptixTracer:
         if debug:
             gpu_time.fill_(ms.value)
         # the arrays the kernels read must outlive the asynchronous launch
-        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de, iv)
+        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de, iv, cp)
         return FwdTraceResult((out_color, out_others, gpu_time, scaling, density_factor, max_blending))
 
     def trace_backward(self, ray_o, ray_d, background, triangles_points, sigma, num_points_per_triangle,
                        cumsum_of_points_per_triangle, colors, others, number_of_points, shs, sh_degree, opacities,
-                       dL_dpixels, dL_dothers, scaling, debug):
+                       dL_dpixels, dL_dothers, scaling, debug, colors_precomp=None):
         """tracer.cpp:144-228: returns BwdTraceResult((dL_dtriangle [V,3],
-        dL_dsigma like sigma, dL_dopacity like opacities, dL_dsh [P,M,3]))."""
+        dL_dsigma like sigma, dL_dopacity like opacities, dL_dsh [P,M,3])).
+        With empty shs and colors_precomp [P, 3] (the forward's colours) the
+        result also carries .dL_dcolors [P, 3]."""
         dev = self.device
         P = int(number_of_points)
         ro = _f32(ray_o, "ray_o", dev)
@@ -212,7 +245,12 @@ class OptixTracer:
         a.vertices, a.num_vertices = _ptr(verts), V
         a.sigma, a.num_points, a.cumsum = _ptr(sig), _ptr(npts), _ptr(cums)
         a.colors, a.others, a.P = _ptr(col), _ptr(oth), P
-        a.shs, a.sh_degree, a.M = _ptr(sh), int(sh_degree), M
+        a.shs, a.sh_degree, a.M = (_ptr(sh) if sh.numel() else ctypes.c_void_p(0)), int(sh_degree), M
+        cp = dcols = None
+        if sh.numel() == 0 and isinstance(colors_precomp, torch.Tensor) and colors_precomp.numel():
+            cp = _f32(colors_precomp, "colors_precomp", dev)
+            dcols = torch.empty((P, 3), dtype=torch.float32, device=dev)
+            a.colors_precomp, a.dL_dcolors = _ptr(cp), _ptr(dcols)
         a.opacities, a.dL_dpixels, a.dL_dothers = _ptr(opac), _ptr(g), _ptr(go)
         a.scaling = ctypes.c_void_p(0)
         a.debug = 1 if debug else 0
@@ -229,8 +267,10 @@ class OptixTracer:
         else:
             iv = None
             check(self._h, lib.tt_backward(self._h, ctypes.byref(a), _stream()))
-        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg, iv)
-        return BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
+        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg, iv, cp)
+        res = BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
+        res.dL_dcolors = dcols
+        return res
 
     # ------------------------------------------------------------------
     def set_proposal(self, proposal, margin_near=None, margin_far=None, far_cap=None):

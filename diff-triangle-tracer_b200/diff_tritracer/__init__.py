@@ -80,8 +80,12 @@ class _Tracer(torch.autograd.Function):
         args = (ray_o, ray_d, st.bg, triangles_points, sigma, num_points_per_triangle,
                 cumsum_of_points_per_triangle, color, others, ctx.number_of_points, shs, st.sh_degree, opacities,
                 grad_color, grad_others, scaling, st.debug)
-        res = _call_with_snapshot(ctx.tracer.trace_backward, args, st.debug, "snapshot_bw.dump", "backward")
+        use_cols = shs.numel() == 0 and colors_precomp.numel() > 0  # precomputed colours in place of SH
+        fn = (lambda *a: ctx.tracer.trace_backward(*a, colors_precomp=colors_precomp)) if use_cols \
+            else ctx.tracer.trace_backward
+        res = _call_with_snapshot(fn, args, st.debug, "snapshot_bw.dump", "backward")
         grad_triangles, grad_sigma, grad_opacities, grad_sh = res.data
+        grad_cols = res.dL_dcolors.reshape(colors_precomp.shape) if use_cols else None
         return (
             None,  # tracer
             None,  # ray_o
@@ -91,8 +95,8 @@ class _Tracer(torch.autograd.Function):
             None,  # num_points_per_triangle
             None,  # cumsum_of_points_per_triangle
             None,  # number_of_points
-            grad_sh,
-            None,  # colors_precomp
+            grad_sh if not use_cols else None,
+            grad_cols,  # colors_precomp (the reference returns None: it never reads them)
             grad_opacities,
             None,  # scaling
             None,  # density_factor

@@ -68,6 +68,7 @@ class TtBwdArgs(ctypes.Structure):
         ("debug", ctypes.c_int),
         ("dL_dtriangle", _vp), ("dL_dsigma", _vp), ("dL_dopacity", _vp), ("dL_dsh", _vp),
         ("gpu_time_ms", _f),
+        ("colors_precomp", _vp), ("dL_dcolors", _vp),
     ]
 
 
@@ -110,7 +111,8 @@ EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
     "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
-    "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree",
+    "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree", "tt_bvh_save",
+    "tt_bvh_load",
 )
 
 
@@ -136,6 +138,8 @@ def _load():
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
     lib.tt_forward_secondary.argtypes = [_vp, ctypes.POINTER(TtFwdArgs), ctypes.POINTER(TtSecondary), _vp]
     lib.tt_backward_secondary.argtypes = [_vp, ctypes.POINTER(TtBwdArgs), ctypes.POINTER(TtSecondary), _vp]
+    lib.tt_bvh_save.argtypes = [_vp, _vp, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong), _vp]
+    lib.tt_bvh_load.argtypes = [_vp, _vp, ctypes.c_ulonglong, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]
     lib.tt_secondary_tree.argtypes = [_vp, _vp, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_int), _vp]
     lib.tt_mlp_update.argtypes = [_vp, ctypes.POINTER(TtMlp), _vp]
     lib.tt_mlp_train_step.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtMlpStep), _vp, _vp, ctypes.c_int,

@@ -91,7 +91,9 @@ typedef struct tt_fwd_args {
   const float* shs;
   int sh_degree; /* 0..3 */
   int M;         /* coefficients per triangle, >= (sh_degree+1)^2 */
-  const float* colors_precomp; /* accepted and ignored, as in the reference */
+  const float* colors_precomp; /* [P][3] RGB per triangle, used in place of SH when shs is NULL
+                                  (the reference accepts it and never reads it, and reads a null
+                                  SH pointer in that case); ignored when shs is given */
   const float* opacities;      /* already activated */
   const float* sigma;
   float* scaling;        /* in/out */
@@ -135,6 +137,8 @@ typedef struct tt_bwd_args {
   float* dL_dopacity;  /* [P] */
   float* dL_dsh;       /* [P,M,3] */
   float* gpu_time_ms;  /* host pointer, may be NULL */
+  const float* colors_precomp; /* [P][3]: the forward's precomputed colours (shs NULL), or NULL */
+  float* dL_dcolors;           /* [P][3] gradient of colors_precomp (zeroed, then accumulated) */
 } tt_bwd_args;
 
 /* One camera image of a batched call: rays [H][W][3]; the forward writes
@@ -233,6 +237,19 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream);
 
 /* Zeroes the counters (asynchronously on `stream`). */
 int tt_reset_stats(tt_tracer* h, void* stream);
+
+/* Serialised acceleration structure (no reference counterpart: OptiX's GAS
+ * is rebuilt by every process). tt_bvh_save writes the handle's BVH
+ * topology (Morton order, binary and 8-wide hierarchies; not the triangle
+ * records or boxes) into the host buffer dst and its size into *bytes; with
+ * dst == NULL it only reports the size. It synchronises `stream`.
+ * tt_bvh_load restores such a blob into a handle and refits it to the given
+ * vertices (the same triangles, moved or not): the result equals a build
+ * followed by refits. A blob for another triangle count, or a damaged one,
+ * gives TT_ERR_INVALID. */
+int tt_bvh_save(tt_tracer* h, void* dst, unsigned long long capacity, unsigned long long* bytes, void* stream);
+int tt_bvh_load(tt_tracer* h, const void* src, unsigned long long bytes, const float* vertices, int num_vertices,
+                const int* cumsum, int P, void* stream);
 
 /* Test hook, no reference counterpart: the first `max_hits` triangle hits of
  * each of R rays in [0, 1000], ordered by (t, primitive index), found by the

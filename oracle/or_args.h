@@ -43,5 +43,7 @@ struct or_args {
   const float* env;
   int env_h, env_w, max_depth;
   int exact_adjoint;  // 1: full chain rule + forward depth (FP64 with exact geometry)
+  const float* precomp;  // [P][3] precomputed colours in place of SH, or NULL
+  void* dprecomp;        // their gradient (precision of the call), backward only
 };
 }

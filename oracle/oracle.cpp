@@ -40,6 +40,7 @@ static Inputs to_inputs(const or_args* a) {
   in.extra = a->extra;
   in.extra_len = a->extra_len;
   in.interval = a->interval;
+  in.colors = a->precomp;
   return in;
 }
 
@@ -105,7 +106,7 @@ static int backward_impl(void* scene, const or_args* a, R* dtri, R* dsigma, R* d
   const Inputs in = to_inputs(a);
   const Opts opt = to_opts(a, sizeof(R) == 8);
   BwdIn<R> bi{static_cast<const R*>(a->colors), static_cast<const R*>(a->others), a->dL_dpixels, a->dL_dothers};
-  BwdOut<R> bo{dtri, dsigma, dopac, dsh};
+  BwdOut<R> bo{dtri, dsigma, dopac, dsh, static_cast<R*>(a->dprecomp)};
   parallel_rows(a, [&](int pix) { backward_ray(sc, in, pix, opt, bi, bo); });
   return 0;
 }

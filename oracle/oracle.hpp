@@ -347,6 +347,7 @@ struct Inputs {
   const float* extra = nullptr;
   int extra_len = 0;
   const float* interval = nullptr;  // optional [2][H][W] proposed [t_near, t_far] per ray
+  const float* colors = nullptr;    // optional [P][3] precomputed colours in place of SH
 };
 
 inline void ray_interval(const Inputs& in, int pix, float& t_near, float& t_far) {
@@ -447,6 +448,10 @@ inline Window<R> window_fn(const Inputs& in, int prim, V3<R> hit_p) {
 // common.h:16-55: real SH basis on the normalised direction, +0.5, clamp >= 0.
 template <class R>
 inline V3<R> sh_color(const Inputs& in, int idx, V3<R> dir, bool clamped[3]) {
+  if (in.colors) {  // precomputed colours (no reference counterpart: it never reads them)
+    if (clamped) clamped[0] = clamped[1] = clamped[2] = false;
+    return from_f<R>(in.colors + 3 * (size_t)idx);
+  }
   dir = dir / length(dir);
   const float* base = in.shs + 3 * (size_t)idx * in.M;
   auto sh = [&](int k) { return from_f<R>(base + 3 * k); };
@@ -763,6 +768,7 @@ struct BwdOut {
   R* dsigma;  // [P]
   R* dopac;   // [P]
   R* dsh;     // [P, M, 3]
+  R* dcolors = nullptr;  // [P, 3] with precomputed colours
 };
 
 template <class R>
@@ -1010,7 +1016,10 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
         } else {
           window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, dL_dnormal, bo.dtri, opt.mt);
         }
-        sh_color_bwd(in, (int)prim, d, clamped, dL_dcolor, bo.dsh, opt.mt);
+        if (in.colors)
+          add3(bo.dcolors, (int)prim, mk<R>(dL_dcolor[0], dL_dcolor[1], dL_dcolor[2]), opt.mt);
+        else
+          sh_color_bwd(in, (int)prim, d, clamped, dL_dcolor, bo.dsh, opt.mt);
         T = test_T;
         return false;
       },

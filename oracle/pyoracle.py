@@ -41,6 +41,7 @@ class OrArgs(ctypes.Structure):
         ("interval", _fp),
         ("material", _ip), ("ior", _fp), ("env", _fp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
         ("max_depth", ctypes.c_int), ("exact_adjoint", ctypes.c_int),
+        ("precomp", _fp), ("dprecomp", ctypes.c_void_p),
     ]
 
 
@@ -72,6 +73,7 @@ class BwdResult:
     dsigma: np.ndarray
     dopac: np.ndarray
     dsh: np.ndarray
+    dcolors: np.ndarray | None = None
 
 
 class _Runner:
@@ -147,9 +149,12 @@ class _Runner:
 
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
                 canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None,
-                interval=None, secondary=None, exact_adjoint=False):
+                interval=None, secondary=None, exact_adjoint=False, precomp=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, extra, variant, tmin_inclusive, canonical, exact, nthreads, rows)
         a.exact_adjoint = int(exact_adjoint)
+        if precomp is not None:
+            keep["precomp"] = _c(precomp, np.float32)
+            a.precomp = _ptr(keep["precomp"])
         self._interval(a, keep, interval)
         sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64
@@ -180,9 +185,15 @@ class _Runner:
 
     def backward(self, scene, ray_o, ray_d, colors, others, dL_dpixels, dL_dothers, bg=None, precision=32,
                  tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None,
-                 secondary=None, exact_adjoint=False):
+                 secondary=None, exact_adjoint=False, precomp=None):
         a, keep = self._args(scene, ray_o, ray_d, bg, None, 0, tmin_inclusive, canonical, exact, nthreads, rows)
         a.exact_adjoint = int(exact_adjoint)
+        dcolors = None
+        if precomp is not None:
+            keep["precomp"] = _c(precomp, np.float32)
+            a.precomp = _ptr(keep["precomp"])
+            dcolors = np.zeros((scene.P, 3), np.float32 if precision == 32 else np.float64)
+            a.dprecomp = dcolors.ctypes.data
         self._interval(a, keep, interval)
         sec = self._secondary(a, keep, secondary)
         dt = np.float32 if precision == 32 else np.float64
@@ -209,7 +220,9 @@ class _Runner:
         rc = fn(self._scene(scene)[1], ctypes.byref(a), _ptr(dtri, t), _ptr(dsigma, t), _ptr(dopac, t), _ptr(dsh, t))
         if rc != 0:
             raise RuntimeError(f"{self.prefix} backward failed ({rc})")
-        return BwdResult(dtri, dsigma, dopac, dsh)
+        res = BwdResult(dtri, dsigma, dopac, dsh)
+        res.dcolors = dcolors
+        return res
 
     def close(self):
         for _, h, _, _ in self._scenes.values():

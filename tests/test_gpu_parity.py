@@ -291,3 +291,76 @@ def test_exact_adjoint_vs_fp64_oracle(oracle, traversal):
     pout = gpu_forward(plain, sc, ro, rd, settings())
     pg = gpu_backward(plain, sc, ro, rd, settings(), pout["color"], pout["others"], g, go)
     assert rel_norm(pg["dtri"], grads["dtri"]) > 0.1
+
+
+def test_colors_precomp_vs_fp64_oracle(oracle):
+    """shs empty + colors_precomp [P, 3]: the colours replace SH (the
+    reference accepts the tensor and never reads it), with their gradient."""
+    sc, (ro, rd) = dense_scene(seed=3, P=3000), dense_view(H=40, W=56)
+    H, W = ro.shape[:2]
+    cols = np.random.default_rng(8).uniform(0.0, 1.0, (sc.P, 3)).astype(np.float32)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    empty = torch.empty(0, device=DEV)
+    res = tr.trace_forward(T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P,
+                           empty, 3, T(cols), T(sc.opacities), torch.zeros(sc.P, device=DEV),
+                           torch.zeros(sc.P, device=DEV), torch.zeros(3, device=DEV), torch.zeros(5, device=DEV), 0,
+                           False).data
+    color, others = res[0], res[1]
+    ref = oracle.forward(sc, ro, rd, precision=64, exact=True, canonical=True, record=256, nthreads=8, precomp=cols)
+    ok = (ref.margin > MARGIN).reshape(H, W)
+    a, b = color.cpu().numpy()[:, ok], ref.color[:, ok]
+    assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + ATOL)
+    g, go = scenes.upstream_grads(H, W, seed=13, others_std=1.0)
+    g, go = g * ok[None], go * ok[None]
+    bres = tr.trace_backward(T(ro), T(rd), torch.zeros(3, device=DEV), T(sc.verts.reshape(-1)), T(sc.sigma),
+                             T(sc.num_points), T(sc.cumsum), color, others, sc.P, empty, 3, T(sc.opacities), T(g), T(go),
+                             torch.zeros(sc.P, device=DEV), False, colors_precomp=T(cols))
+    torch.cuda.synchronize()
+    tr.device_status()
+    rb = oracle.backward(sc, ro, rd, ref.color, ref.others, g, go, precision=64, exact=True, canonical=True,
+                         nthreads=8, precomp=cols)
+    assert rel_norm(bres.dL_dcolors.cpu().numpy(), rb.dcolors) < GRAD_RTOL
+    for key, x in zip(("dtri", "dsigma", "dopac"), bres.data[:3]):
+        assert rel_norm(x.cpu().numpy(), getattr(rb, key)) < GRAD_RTOL, key
+    # through the drop-in module: shs=None, colors_precomp given
+    cp = T(cols).requires_grad_(True)
+    tracer = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
+    out = tracer(T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P,
+                 T(sc.opacities), torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), None, cp, settings())
+    (out[0] * T(g)).sum().backward()
+    torch.cuda.synchronize()
+    assert cp.grad is not None and rel_norm(cp.grad.cpu().numpy(), rb.dcolors) < GRAD_RTOL
+
+
+def test_bvh_save_and_load(tmp_path):
+    """A saved BVH topology, loaded into a fresh handle (refitted to the same
+    or to moved vertices), traces exactly like the original structure."""
+    sc = dense_scene(seed=2, P=2500)
+    ro, rd = dense_view(H=32, W=40)
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.build_tri_accel(T(sc.verts), T(sc.cumsum), sc.P, True)
+    path = tmp_path / "scene.bvh"
+    blob = tr.save_bvh(str(path))
+    assert path.stat().st_size == len(blob) > 0
+    ref = [x.cpu().numpy() for x in tr.hit_stream(T(ro), T(rd), max_hits=48)]
+    tr2 = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr2.load_bvh(str(path), T(sc.verts), T(sc.cumsum), sc.P)
+    got = [x.cpu().numpy() for x in tr2.hit_stream(T(ro), T(rd), max_hits=48)]
+    for a, b in zip(got, ref):
+        np.testing.assert_array_equal(a, b)
+    out1 = gpu_forward(tr, sc, ro, rd, settings(rebuild=2))
+    out2 = gpu_forward(tr2, sc, ro, rd, settings(rebuild=2))
+    np.testing.assert_array_equal(out1["color"], out2["color"])
+    # loading onto moved vertices equals refitting the original
+    moved = sc.__class__(**{**sc.__dict__})
+    moved.verts = (sc.verts + np.random.default_rng(1).normal(0, 0.005, sc.verts.shape)).astype(np.float32)
+    tr.build_tri_accel(T(moved.verts), T(moved.cumsum), moved.P, False)  # refit
+    tr3 = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr3.load_bvh(blob, T(moved.verts), T(moved.cumsum), moved.P)
+    a = [x.cpu().numpy() for x in tr.hit_stream(T(ro), T(rd), max_hits=48)]
+    b = [x.cpu().numpy() for x in tr3.hit_stream(T(ro), T(rd), max_hits=48)]
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    tr3.device_status()
+    with pytest.raises(RuntimeError, match="not a BVH blob"):
+        _C.OptixTracer("", "forward.ptx", "backward.ptx").load_bvh(blob, T(sc.verts[:100]), T(sc.cumsum[:100]), 100)
