@@ -867,8 +867,9 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned ra
 }
 
 // forward.cu:109-152 per hit and :204-214 per ray. EXACT (no reference
-// counterpart) also accumulates the depth channel, sum of w t, which the
-// reference leaves at 0.
+// counterpart) also fills the channels the reference leaves at 0: depth
+// sum w t, middepth (t of the hit after which T <= 0.5) and distortion
+// sum_{i<j} w_i w_j (t_i - t_j)^2 (running sums of w and w t^2).
 template <bool EXACT>
 struct FwdShader {
   const TraceParams& p;
@@ -876,7 +877,8 @@ struct FwdShader {
   int pix;
   float3 o, d;
   float C0, C1, C2, N0, N1, N2, T;
-  float D;  // EXACT only
+  float D, Wsum, Wt2, mid, dist2;  // EXACT only
+  bool mid_set;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
   unsigned first_eval = 0;  // value of n_eval at the ray's first hit (record only)
 
@@ -888,7 +890,8 @@ struct FwdShader {
     o = ro;
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
-    D = 0.f;
+    D = Wsum = Wt2 = mid = dist2 = 0.f;
+    mid_set = false;
     T = 1.0f;
     ++n_rays;
     if (v->record) {
@@ -931,7 +934,17 @@ struct FwdShader {
     N0 += g.n.x * w;
     N1 += g.n.y * w;
     N2 += g.n.z * w;
-    if (EXACT) D += w * g.t;
+    if (EXACT) {
+      const float ht = g.t;
+      dist2 += w * (ht * ht * Wsum - 2.0f * ht * D + Wt2);
+      Wsum += w;
+      D += w * ht;
+      Wt2 += w * ht * ht;
+      if (!mid_set && test_T <= 0.5f) {
+        mid = ht;
+        mid_set = true;
+      }
+    }
     float3 c;
     if (p.cols) {  // precomputed colours in place of SH
       c = make_float3(__ldg(p.cols + 3 * prim), __ldg(p.cols + 3 * prim + 1), __ldg(p.cols + 3 * prim + 2));
@@ -958,8 +971,8 @@ struct FwdShader {
     v->out_others[(kNormalCh + 0) * HW + pix] = N0;
     v->out_others[(kNormalCh + 1) * HW + pix] = N1;
     v->out_others[(kNormalCh + 2) * HW + pix] = N2;
-    v->out_others[kMidDepthCh * HW + pix] = 0.0f;
-    v->out_others[kDistortionCh * HW + pix] = 0.0f;
+    v->out_others[kMidDepthCh * HW + pix] = EXACT ? mid : 0.0f;
+    v->out_others[kDistortionCh * HW + pix] = EXACT ? dist2 : 0.0f;
   }
 };
 
@@ -1314,6 +1327,9 @@ struct BwdShader {
   float Cf0, Cf1, Cf2, Df, Nf0, Nf1, Nf2;
   float g0, g1, g2, gD, gN0, gN1, gN2;
   float C0, C1, C2, N0, N1, N2, D, T;
+  // EXACT: middepth / distortion (finals per chunk, running sum S, mid flag)
+  float Wf, distf, gMid, gDist, S;
+  bool mid_seen;
 
   __device__ explicit BwdShader(const TraceParams& params) : p(params) {}
 
@@ -1324,6 +1340,8 @@ struct BwdShader {
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = D = 0.f;
     T = 1.0f;
+    S = 0.f;
+    mid_seen = false;
     return true;
   }
 
@@ -1345,6 +1363,12 @@ struct BwdShader {
     gN0 = __ldg(v->dL_doth + (kNormalCh + 0) * HW + pix);
     gN1 = __ldg(v->dL_doth + (kNormalCh + 1) * HW + pix);
     gN2 = __ldg(v->dL_doth + (kNormalCh + 2) * HW + pix);
+    if (EXACT) {
+      Wf = __ldg(v->others + kAlphaCh * HW + pix);
+      distf = __ldg(v->others + kDistortionCh * HW + pix);
+      gMid = __ldg(v->dL_doth + kMidDepthCh * HW + pix);
+      gDist = __ldg(v->dL_doth + kDistortionCh * HW + pix);
+    }
   }
 
   __device__ __forceinline__ bool visit(uint32_t prim, float) {
@@ -1381,6 +1405,20 @@ struct BwdShader {
     dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
     dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
                  gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
+    float dL_dt = gD * w;
+    if (EXACT) {
+      // distortion: dD/dalpha_k = T_k E_k - (2 D_f - S_k) / (1 - alpha_k),
+      // E_k = t^2 W_f - 2 t B_f + C_f, C_f = (D_f + B_f^2) / W_f; dD/dt_k = 2 w (t W_f - B_f)
+      const float Cf = Wf > 0.f ? (distf + Df * Df) / Wf : 0.f;
+      const float E = g.t * g.t * Wf - 2.0f * g.t * Df + Cf;
+      S += w * E;
+      dL_dalpha += gDist * (T * E - (2.0f * distf - S) * inv1a);
+      dL_dt += gDist * 2.0f * w * (g.t * Wf - Df);
+      if (!mid_seen && test_T <= 0.5f) {
+        mid_seen = true;
+        dL_dt += gMid;
+      }
+    }
     const bool live = !EXACT || opacity * g.Cx < kAlphaMax;
     const float dL_dC = live ? opacity * dL_dalpha : 0.0f;
     if (live) red_add(p.d_opac + prim, dL_dalpha * g.Cx);
@@ -1388,7 +1426,7 @@ struct BwdShader {
     const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
     float3 gv[3];
     if (EXACT)
-      window_bwd_exact(g, d, dL_dphi, dL_dC * sig * g.Cx, make_float3(gN0 * w, gN1 * w, gN2 * w), gD * w, gv);
+      window_bwd_exact(g, d, dL_dphi, dL_dC * sig * g.Cx, make_float3(gN0 * w, gN1 * w, gN2 * w), dL_dt, gv);
     else
       window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
     float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);

@@ -71,8 +71,11 @@ typedef struct tt_config {
   int exact_adjoint;  /* 0 (default): the reference's gradients (backward.cu), whose vertex
                          gradient leaves out how the incenter distance, the hit point and t
                          move; 1: the full chain rule, no gradient through a clamped alpha, and
-                         the forward accumulates depth (out_others channel 0 = sum w t). No
-                         reference counterpart; plain program only */
+                         the forward fills the channels the reference leaves at 0: depth
+                         (sum w t), middepth (t of the hit after which T <= 0.5) and
+                         distortion (sum over hit pairs i < j of w_i w_j (t_i - t_j)^2), all
+                         differentiated by the adjoint. No reference counterpart; plain
+                         program only */
   int reserved[2];    /* zero */
 } tt_config;
 

@@ -558,6 +558,10 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
   R C[3] = {0, 0, 0}, N[3] = {0, 0, 0};
   R T = 1;
   R D = 0;  // the reference never accumulates depth; the exact adjoint's forward does
+  // exact adjoint's forward only: middepth (t of the hit after which T <= 0.5)
+  // and distortion sum_{i<j} w_i w_j (t_i - t_j)^2 with running sums of w, w t^2
+  R Wsum = 0, C2 = 0, mid = 0, dist2 = 0;
+  bool mid_set = false;
   march(
       sc, rp, opt,
       [&](uint32_t prim, float t) -> bool {
@@ -576,7 +580,17 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
         N[0] += w.n.x * bw;
         N[1] += w.n.y * bw;
         N[2] += w.n.z * bw;
-        if (opt.exact_adjoint) D += bw * hit_dist(in, (int)prim, o, d, t, opt);
+        if (opt.exact_adjoint) {
+          const R ht = hit_dist(in, (int)prim, o, d, t, opt);
+          dist2 += bw * (ht * ht * Wsum - R(2) * ht * D + C2);
+          Wsum += bw;
+          D += bw * ht;
+          C2 += bw * ht * ht;
+          if (!mid_set && test_T <= R(0.5)) {
+            mid = ht;
+            mid_set = true;
+          }
+        }
         const V3<R> col = sh_color(in, (int)prim, d, nullptr);
         C[0] += col.x * bw;
         C[1] += col.y * bw;
@@ -592,8 +606,8 @@ inline void forward_ray(const Scene& sc, const Inputs& in, int pix, const Opts& 
   out.others[pix + kDepth * HW] = D;
   out.others[pix + kAlphaOff * HW] = R(1) - T;
   for (int ch = 0; ch < 3; ++ch) out.others[pix + (kNormal + ch) * HW] = N[ch];
-  out.others[pix + kMidDepth * HW] = R(0);
-  out.others[pix + kDistortion * HW] = R(0);
+  out.others[pix + kMidDepth * HW] = mid;
+  out.others[pix + kDistortion * HW] = dist2;
 }
 
 // ---------------------------------------------------------------- variants
@@ -964,6 +978,15 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
                                    (R)bi.dL_dothers[(kNormal + 2) * HW + pix]);
   float t_near, t_far;
   ray_interval(in, pix, t_near, t_far);
+  // exact adjoint: middepth / distortion from their final values; the
+  // distortion's alpha gradient is T_k E_k - (2 dist_f - S_k) / (1 - alpha_k)
+  // with E_k = t_k^2 W_f - 2 t_k B_f + C_f (C_f = (dist_f + B_f^2) / W_f) and
+  // S_k = sum_{i<=k} w_i E_i; its t gradient is 2 w_k (t_k W_f - B_f)
+  const R g_mid = (R)bi.dL_dothers[kMidDepth * HW + pix], g_dist = (R)bi.dL_dothers[kDistortion * HW + pix];
+  const R W_f = bi.others[pix + kAlphaOff * HW], dist_f = bi.others[pix + kDistortion * HW];
+  const R C_f = W_f > R(0) ? (dist_f + final_depth * final_depth) / W_f : R(0);
+  R S = 0;
+  bool mid_seen = false;
   R C[3] = {0, 0, 0}, N[3] = {0, 0, 0};
   R D = 0, T = 1;
   march(
@@ -999,6 +1022,17 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
         dL_dalpha += dL_ddepth * (T * hit_t - (final_depth - D) * inv_1_alpha);
         const V3<R> Nf = mk<R>(N[0], N[1], N[2]);
         dL_dalpha += sum3(vmul(dL_dnormal2D, T * w.n - (final_normal - Nf) * inv_1_alpha));
+        R dL_dt_extra = dL_ddepth * bw;
+        if (opt.exact_adjoint) {
+          const R E = hit_t * hit_t * W_f - R(2) * hit_t * final_depth + C_f;
+          S += bw * E;
+          dL_dalpha += g_dist * (T * E - (R(2) * dist_f - S) * inv_1_alpha);
+          dL_dt_extra += g_dist * R(2) * bw * (hit_t * W_f - final_depth);
+          if (!mid_seen && test_T <= R(0.5)) {
+            mid_seen = true;
+            dL_dt_extra += g_mid;
+          }
+        }
         // the exact adjoint honours the alpha clamp (no gradient through a
         // clamped alpha); the reference differentiates through it
         const bool live = !opt.exact_adjoint || opacity * w.Cx < R(kAlphaMax);
@@ -1011,8 +1045,7 @@ inline void backward_ray(const Scene& sc, const Inputs& in, int pix, const Opts&
         const V3<R> dL_dnormal = dL_dnormal2D * bw;
         if (opt.exact_adjoint) {
           const R dL_ddist = -dL_dC * (R)in.sigma[prim] * w.Cx / w.dist;
-          window_bwd_exact(in, (int)prim, d, hp, w, dL_dphi_x, dL_ddist, dL_dnormal, dL_ddepth * bw, bo.dtri,
-                           opt.mt);
+          window_bwd_exact(in, (int)prim, d, hp, w, dL_dphi_x, dL_ddist, dL_dnormal, dL_dt_extra, bo.dtri, opt.mt);
         } else {
           window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, dL_dnormal, bo.dtri, opt.mt);
         }

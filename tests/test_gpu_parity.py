@@ -264,8 +264,8 @@ def test_sphere_variants_vs_fp64_oracle(oracle, prog, variant):
 
 @pytest.mark.parametrize("traversal", ["packets", "lanes"])
 def test_exact_adjoint_vs_fp64_oracle(oracle, traversal):
-    """exact_adjoint=True: the forward accumulates depth and the adjoint is the
-    full chain rule (checked against finite differences on the CPU oracle in
+    """exact_adjoint=True: the forward accumulates depth, middepth and
+    distortion and the adjoint is the full chain rule (checked against finite differences on the CPU oracle in
     test_oracle_fd.py); the GPU's FP32 evaluation against the FP64 oracle."""
     sc, (ro, rd) = dense_scene(seed=1, P=3000), dense_view(H=48, W=64)
     H, W = ro.shape[:2]
@@ -274,9 +274,11 @@ def test_exact_adjoint_vs_fp64_oracle(oracle, traversal):
     ref = oracle.forward(sc, ro, rd, record=256, **kw)
     ok = (ref.margin > MARGIN).reshape(H, W)
     g, go = scenes.upstream_grads(H, W, seed=12, others_std=1.0)
+    go[5:7] = np.random.default_rng(12).normal(0, 1.0, (2, H, W))  # middepth, distortion
     g, go = g * ok[None], go * ok[None]
     out = gpu_forward(tr, sc, ro, rd, settings())
     assert np.abs(out["others"][0]).max() > 1.0  # depth is accumulated
+    assert out["others"][5].max() > 1.0 and out["others"][6].max() > 0  # middepth, distortion
     a, b = out["others"][:, ok], ref.others[:, ok]
     assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + ATOL)
     grads = gpu_backward(tr, sc, ro, rd, settings(), out["color"], out["others"], g, go)

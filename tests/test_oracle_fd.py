@@ -3,8 +3,8 @@ on a 1k-triangle scene at 64x64 (the GPU adjoint is held to the same oracle in
 the GPU parity tests, so these checks carry over).
 
 The loss is L = sum(g * colour) + sum(g_n * normal) with fixed upstream
-gradients (plus sum(g_d * depth) for the exact adjoint, whose forward
-accumulates depth). Opacity, sigma and SH gradients follow the chain rule exactly
+gradients (plus the depth, middepth and distortion channels for the exact adjoint,
+whose forward accumulates them). Opacity, sigma and SH gradients follow the chain rule exactly
 (away from the alpha / transmittance thresholds). The reference's vertex
 gradient (backward.cu:104-189) is partial - it leaves out how the incenter,
 the hit point and t move with the vertices - so it is NOT expected to match
@@ -100,14 +100,16 @@ def test_exact_adjoint_matches_finite_differences(oracle):
     cam = scenes.look_at_camera([0.4, 0.3, 3.0], H, W, fov_deg=10.0)
     ro, rd = scenes.camera_rays(cam)
     g, go = scenes.upstream_grads(H, W, seed=4, others_std=1.0)
+    go[5:7] = np.random.default_rng(6).normal(0, 1.0, (2, H, W))  # middepth and distortion too
     kw = dict(precision=64, exact=True, canonical=True, nthreads=8, exact_adjoint=True)
     f = oracle.forward(sc, ro, rd, **kw)
     assert np.abs(f.others[0]).max() > 0  # depth is accumulated
+    assert f.others[5].max() > 0 and f.others[6].max() > 0  # middepth and distortion too
     b = oracle.backward(sc, ro, rd, f.color, f.others, g, go, **kw)
 
     def loss():
         r = oracle.forward(sc, ro, rd, **kw)
-        return float((r.color * g).sum() + (r.others[0] * go[0]).sum() + (r.others[2:5] * go[2:5]).sum())
+        return float((r.color * g).sum() + (r.others[0] * go[0]).sum() + (r.others[2:7] * go[2:7]).sum())
 
     # vertices use h = 1e-5: in this dense cloud a 1e-4 move of a vertex
     # already reorders overlapping hits for some rays (a jump in the loss)
