@@ -208,12 +208,15 @@ def reference_arm(args, rank):
     }), flush=True)
 
 
-def algorithmic_bytes(rays, evals, blends):
+def algorithmic_bytes(rays, evals, blends, cache_k=0):
     """Per launch, from the per-ray figures: forward 24 + 40 + 48 h_e + 204 h_b;
     adjoint 24 + 40 + 28 + 48 h_e + (192 + 2*236) h_b (h_e/h_b = evaluated /
-    blended hits, counted by the forward kernel)."""
-    fwd = rays * (24 + 40) + 48 * evals + 204 * blends
-    bwd = rays * (24 + 40 + 28) + 48 * evals + (192 + 2 * 236) * blends
+    blended hits, counted by the forward kernel); with a hit cache of k-hit
+    queries, (k + 1) * 8 bytes per ray more: written by the forward, read by
+    the adjoint."""
+    c = (cache_k + 1) * 8 if cache_k else 0
+    fwd = rays * (24 + 40 + c) + 48 * evals + 204 * blends
+    bwd = rays * (24 + 40 + 28 + c) + 48 * evals + (192 + 2 * 236) * blends
     return fwd, bwd
 
 
@@ -465,6 +468,8 @@ def main():
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
+    ap.add_argument("--no-hit-cache", action="store_true",
+                    help="adjoint re-traverses every query instead of replaying the forward's first one")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
                     help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
@@ -509,23 +514,29 @@ def main():
 
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
     tr.build_tri_accel(verts, cums, P, True)
+    use_cache = not args.no_hit_cache
+
     def step():
+        # the hit cache is the step's activation: allocated (caching allocator) and filled every step
+        cache = tr.new_hit_cache(R) if use_cache else None
         out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg, extra,
-                               1, False).data
-        tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling, False)
+                               1, False, hit_cache=cache).data
+        tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling, False,
+                          hit_cache=cache)
 
     # kernel-level timing: forward and adjoint each bracketed by events
-    def timed_kernels(n):
+    def timed_kernels(n, cached=use_cache):
         fwd_ms, bwd_ms = [], []
         for _ in range(n):
             e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             tr.build_tri_accel(verts, cums, P, False)
+            cache = tr.new_hit_cache(R) if cached else None
             e[0].record()
             out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg,
-                                   extra, 2, False).data
+                                   extra, 2, False, hit_cache=cache).data
             e[1].record()
             tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling,
-                              False)
+                              False, hit_cache=cache)
             e[2].record()
             torch.cuda.synchronize()
             fwd_ms.append(e[0].elapsed_time(e[1]))
@@ -574,10 +585,12 @@ def main():
 
     # ---------------- roofline of the dominant kernel (adjoint)
     fwd_ms, bwd_ms = timed_kernels(3)
+    fwd_plain_ms, bwd_retrace_ms = timed_kernels(2, cached=False) if use_cache else (fwd_ms, bwd_ms)
     rays_step = st["rays"] / args.steps
     evals = st["evaluated_hits"] / args.steps
     blends = st["blended_hits"] / args.steps
-    fwd_b, bwd_b = algorithmic_bytes(rays_step, evals, blends)
+    k_cache = int(tuned["k"]) if tuned else 16
+    fwd_b, bwd_b = algorithmic_bytes(rays_step, evals, blends, cache_k=k_cache if use_cache else 0)
     peak, peak_kind = peaks()
     dominant = "adjoint" if bwd_ms >= fwd_ms else "forward"
     dom_bytes, dom_ms = (bwd_b, bwd_ms) if dominant == "adjoint" else (fwd_b, fwd_ms)
@@ -591,8 +604,9 @@ def main():
                 traffic = float(parts[1])
 
     # ---------------- end to end through the public API (host buffers)
-    tracer_mod = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
+    tracer_mod = diff_tritracer.Tracer("forward.ptx", "backward.ptx", hit_cache=use_cache)
     tracer_mod.tracer = tr
+    tr.use_hit_cache = use_cache
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     ro_h, rd_h, g_h = pin(ro_np), pin(rd_np), pin(g_np)
     color_h = torch.empty((3, HH, WW), dtype=torch.float32).pin_memory()
@@ -655,6 +669,9 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "triangles": P, "views": views, "H": H, "W": W, "rays_per_step": R,
                    "step": "BVH refit + forward trace + adjoint trace",
+                   "hit_cache": ("the forward stores each ray's first k-closest query (the step's activation, "
+                                 "(k+1)*8 B/ray); the adjoint replays it and traverses only for later queries"
+                                 if use_cache else "off: the adjoint re-traverses every query"),
                    "l2": "inputs larger than L2 (scene + BVH + rays ~0.5 GB per step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
@@ -669,6 +686,7 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
                      "forward_ms": fwd_ms, "adjoint_ms": bwd_ms,
+                     "forward_without_cache_ms": fwd_plain_ms, "adjoint_retrace_ms": bwd_retrace_ms,
                      "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
         "cpu_baseline": cpu,
         "proposal": prop,

@@ -28,12 +28,15 @@ struct tt_tracer {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
+  unsigned long long bvh_gen = 0;         // BVH builds, refits and loads so far (hit cache validity)
+  int k() const { return cfg_id == tt::kCfgPackets32 ? 32 : 16; }
   unsigned long long launches() const { return trace_launches + bvh.launches(); }
 };
 
 namespace {
 
 constexpr int kSecCountOffset = 96;
+static_assert(16 + tt::kNumStats * 8 <= kSecCountOffset, "stats overlap the secondary-ray counters");
 
 int fail(tt_tracer* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -72,6 +75,7 @@ int accel_step(tt_tracer* h, const float* verts, int num_vertices, const int* cu
     TT_REQUIRE(h, num_vertices >= 3, "need at least 3 vertices");
   }
   TT_REQUIRE(h, P < (1 << 27), "at most 2^27 triangles");
+  ++h->bvh_gen;
   cudaError_t e = (mode == TT_BUILD) ? h->bvh.build(verts, cumsum, P, s) : h->bvh.refit(verts, cumsum, P, s);
   if (e != cudaSuccess) return cuda_fail(h, e, mode == TT_BUILD ? "bvh build" : "bvh refit");
   return TT_OK;
@@ -146,6 +150,11 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth) {
   return TT_OK;
 }
 
+size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays) {
+  if (!h || rays < 0) return 0;
+  return tt::hit_cache_bytes(h->k(), rays);
+}
+
 int tt_destroy(tt_tracer* h) {
   if (!h) return TT_ERR_INVALID;
   h->bvh.release();
@@ -202,6 +211,8 @@ static int add_view(tt_tracer* h, tt::TraceParams& p, const tt_view& v) {
   d.W = v.W;
   d.ntx = (v.W + 7) / 8;
   d.tile_begin = p.ntiles;
+  d.ray_begin = p.cache_rays;
+  p.cache_rays += (long long)v.H * v.W;
   const long long tiles = (long long)p.ntiles + (long long)d.ntx * ((v.H + 3) / 4);
   TT_REQUIRE(h, tiles < (1ll << 26), "too many tiles in one call");
   p.ntiles = (int)tiles;
@@ -236,6 +247,15 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   }
   rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
   if (rc != TT_OK) return rc;
+  if (a->hit_cache) {
+    TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "the hit cache is for the plain program only");
+    TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
+    TT_REQUIRE(h, a->hit_cache_bytes >= tt::hit_cache_bytes(h->k(), p.cache_rays),
+               "hit_cache is smaller than tt_hit_cache_bytes() for these rays");
+    p.hit_cache = a->hit_cache;
+    p.cache_mode = tt::kCacheWrite;
+    p.cache_gen = h->bvh_gen;
+  }
   p.bvh = h->bvh.view();
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
@@ -334,6 +354,14 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
   p.d_sigma = a->dL_dsigma;
   p.d_opac = a->dL_dopacity;
   p.d_sh = a->dL_dsh;
+  // a cache written for another k or ray count (or too small for this k)
+  // fails the kernels' header check or is not passed at all: they re-trace
+  if (a->hit_cache && a->hit_cache_bytes >= tt::hit_cache_bytes(h->k(), p.cache_rays)) {
+    TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
+    p.hit_cache = const_cast<void*>(a->hit_cache);
+    p.cache_mode = tt::kCacheRead;
+    p.cache_gen = h->bvh_gen;
+  }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
   TT_CUDA(h, tt::launch_backward(p, h->bwd_grid, s));
@@ -402,6 +430,7 @@ int tt_get_stats(tt_tracer* h, tt_stats* out, void* stream) {
   out->packet_node_visits = v[6];
   out->interval_continuations = v[7];
   out->interval_retraces = v[8];
+  out->hit_cache_replays = v[tt::kStatReplays];
   return TT_OK;
 }
 
@@ -780,6 +809,7 @@ int tt_bvh_load(tt_tracer* h, const void* src, unsigned long long bytes, const f
   if (!h) return TT_ERR_INVALID;
   TT_REQUIRE(h, src && vertices && cumsum && P > 0 && num_vertices >= 3, "need a blob, vertices and cumsum");
   cudaError_t e = cudaSuccess;
+  ++h->bvh_gen;
   if (h->bvh.load(src, (size_t)bytes, vertices, cumsum, P, as_stream(stream), &e) != 0)
     return fail(h, TT_ERR_INVALID, "not a BVH blob for this triangle count");
   if (e != cudaSuccess) return cuda_fail(h, e, "bvh load");

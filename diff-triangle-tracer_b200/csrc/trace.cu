@@ -64,6 +64,7 @@ __device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsi
 struct Counters {
   unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
   unsigned cont = 0, restart = 0;  // proposed intervals left by continuation / re-trace
+  unsigned replays = 0;            // first queries taken from the hit cache (adjoint)
 };
 
 // Three-input FP32 min / max (one instruction on sm_100); min and max are
@@ -266,6 +267,11 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
   const float t_lo = want ? key_t(key_min) : 0.f;
   float tmax = want ? t_hi : -1.0f;  // a lane without a query never passes a test
   const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
+  // the rays of a packet nearly always share the watertight axis permutation:
+  // then the triangle tests use it as a compile-time constant
+  const int pk = perm_pack(r);
+  const int pk0 = __shfl_sync(full, pk, __ffs(act) - 1);
+  const int wperm = __all_sync(full, !want || pk == pk0) ? pk0 : -1;
   if (lane == 0) {
     ws.ref[0] = 0u;
     ws.mask[0] = act;
@@ -289,18 +295,20 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     if (ref_is_leaf(ref)) {
       const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
       if (on) cnt.tris += ntri;
-      for (uint32_t j = 0; j < ntri; ++j) {
-        const float4* tr = bvh.tris + 3 * (size_t)(first + j);
-        const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
-        float t;
-        if (!on || !isect_tri(r, a, b, c, t)) continue;
-        if (!(t >= t_lo) || !(t <= tmax)) continue;
-        const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-        if (key >= key_min && key < kb_last) {
-          kb_insert_smem<K>(kb, kstride, key, kb_last);
-          if (kb_last != kEmptyKey) tmax = key_t(kb_last);
+      with_perm(wperm, r, [&](const auto& pm) {
+        for (uint32_t j = 0; j < ntri; ++j) {
+          const float4* tr = bvh.tris + 3 * (size_t)(first + j);
+          const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+          float t;
+          if (!on || !isect_tri_p(r, pm, a, b, c, t)) continue;
+          if (!(t >= t_lo) || !(t <= tmax)) continue;
+          const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
+          if (key >= key_min && key < kb_last) {
+            kb_insert_smem<K>(kb, kstride, key, kb_last);
+            if (kb_last != kEmptyKey) tmax = key_t(kb_last);
+          }
         }
-      }
+      });
       continue;
     }
     if (on) ++cnt.nodes;
@@ -684,6 +692,50 @@ __device__ __forceinline__ int find_view(const TraceParams& p, int tile) {
   return lo;
 }
 
+// Hit cache (HitCacheHeader): the forward stores each ray's first query, the
+// adjoint replays it. Rows are written and read once, so they bypass L2
+// residency (streaming stores / loads) and leave it to the BVH.
+__device__ __forceinline__ unsigned long long* cache_rows(const TraceParams& p) {
+  return reinterpret_cast<unsigned long long*>(static_cast<char*>(p.hit_cache) + sizeof(HitCacheHeader));
+}
+
+template <int K>
+__device__ __forceinline__ bool cache_replays(const TraceParams& p) {
+  if (p.cache_mode != kCacheRead) return false;
+  const HitCacheHeader* h = static_cast<const HitCacheHeader*>(p.hit_cache);
+  return h->magic == kHitCacheMagic && h->k == (uint32_t)K && h->rays == p.cache_rays && h->gen == p.cache_gen;
+}
+
+template <int K>
+__device__ __forceinline__ void cache_store(const TraceParams& p, long long g, const Smem& sm, float t_drop) {
+  unsigned long long* rows = cache_rows(p) + g;
+#pragma unroll 4
+  for (int i = 0; i < K; ++i) __stcs(rows + (size_t)i * p.cache_rays, sm.keys[i * sm.stride]);
+  __stcs(rows + (size_t)K * p.cache_rays, (unsigned long long)__float_as_uint(t_drop));
+}
+
+// Fills the lane's query buffer; returns the stored t_drop.
+template <int K>
+__device__ __forceinline__ float cache_load(const TraceParams& p, long long g, const Smem& sm) {
+  const unsigned long long* rows = cache_rows(p) + g;
+#pragma unroll 4
+  for (int i = 0; i < K; ++i) sm.keys[i * sm.stride] = __ldcs(rows + (size_t)i * p.cache_rays);
+  return __uint_as_float((uint32_t)__ldcs(rows + (size_t)K * p.cache_rays));
+}
+
+template <int K>
+__device__ __forceinline__ void cache_header(const TraceParams& p) {
+  if (p.cache_mode == kCacheWrite && blockIdx.x == 0 && threadIdx.x == 0) {
+    HitCacheHeader h;
+    h.magic = kHitCacheMagic;
+    h.k = K;
+    h.rays = p.cache_rays;
+    h.gen = p.cache_gen;
+    h.pad = 0;
+    *static_cast<HitCacheHeader*>(p.hit_cache) = h;
+  }
+}
+
 // Persistent warp driver. Each round: lanes without a ray take the next rays
 // of the tile-ordered image (8x4 pixels per 32 slots) from the global counter,
 // then every lane holding a ray runs its k-closest query, then every such lane
@@ -699,6 +751,8 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
   bool have = false, exhausted = false;
   Cursor cur = first_cursor(p.tmin_inclusive);
   float3 o = make_float3(0.f, 0.f, 0.f), d = o;
+  long long g = 0;  // hit cache index of the lane's ray
+  const bool replay = cache_replays<K>(p);
   for (;;) {
     const unsigned need = __ballot_sync(full, !have && !exhausted);
     if (need) {
@@ -719,6 +773,7 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
             const int pix = py * v.W + px;
             o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
             d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
+            g = v.ray_begin + pix;
             cur = first_cursor(p.tmin_inclusive);
             if (v.interval) clip_cursor(cur, v.interval, v.H * v.W, pix);
             if (sh.begin(&v, pix, o, d))
@@ -735,11 +790,17 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
     }
     float t_drop = INFINITY;
     if (have) {
-      const RayW r = make_ray(o, d);
-      unsigned long long kb[kChunk];
-      query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
+      if (replay && cur.chunks == 0) {  // first query of the ray, as the forward found it
+        t_drop = cache_load<K>(p, g, sm);
+        ++cnt.replays;
+      } else {
+        const RayW r = make_ray(o, d);
+        unsigned long long kb[kChunk];
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
-      for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        if (p.cache_mode == kCacheWrite && cur.chunks == 0) cache_store<K>(p, g, sm, t_drop);
+      }
     }
     __syncwarp();
     if (have) {
@@ -777,6 +838,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
                                               Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
+  const bool replay = cache_replays<K>(p);
   for (;;) {
     int tile = 0;
     if (lane == 0) tile = atomicAdd(p.work, 1);
@@ -788,17 +850,27 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
     bool active = px < v.W && py < v.H;
     float3 o = make_float3(0.f, 0.f, 1.f), d = make_float3(0.f, 0.f, 1.f);
     Cursor cur = first_cursor(p.tmin_inclusive);
+    long long g = 0;  // hit cache index of the lane's ray
     if (active) {
       const int pix = py * v.W + px;
+      g = v.ray_begin + pix;
       o = make_float3(v.ray_o[3 * pix], v.ray_o[3 * pix + 1], v.ray_o[3 * pix + 2]);
       d = make_float3(v.ray_d[3 * pix], v.ray_d[3 * pix + 1], v.ray_d[3 * pix + 2]);
       if (v.interval) clip_cursor(cur, v.interval, v.H * v.W, pix);
       sh.begin(&v, pix, o, d);  // the plain shaders always trace their one ray
     }
     const RayW r = make_ray(o, d);
-    while (__any_sync(full, active)) {
-      float t_drop;
-      packet_query<K>(p.bvh, r, active, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+    for (bool first = true; __any_sync(full, active); first = false) {
+      float t_drop = INFINITY;
+      if (first && replay) {  // every ray's first query, as the forward found it
+        if (active) {
+          t_drop = cache_load<K>(p, g, sm);
+          ++cnt.replays;
+        }
+      } else {
+        packet_query<K>(p.bvh, r, active, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+        if (first && active && p.cache_mode == kCacheWrite) cache_store<K>(p, g, sm, t_drop);
+      }
       if (active) {
         bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);
         if (!done && ++cur.chunks >= kMaxChunks) {
@@ -875,7 +947,8 @@ __device__ __forceinline__ void run(const TraceParams& p, Shader& sh, Counters& 
 // ---------------------------------------------------------------- forward
 __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned rays, unsigned evals, unsigned blends,
                                           const Counters& c) {
-  const unsigned v[kNumStats] = {rays, evals, blends, c.nodes, c.tris, c.queries, c.warp_nodes, c.cont, c.restart};
+  const unsigned v[kNumStats] = {rays,         evals,   blends,    c.nodes,   c.tris,
+                                 c.queries,    c.warp_nodes, c.cont, c.restart, c.replays};
 #pragma unroll
   for (int i = 0; i < kNumStats; ++i) {
     const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[i]);
@@ -995,6 +1068,7 @@ struct FwdShader {
 
 template <int CFG, bool EXACT>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
+  cache_header<TraversalCfg<CFG>::K>(p);
   Counters cnt;
   FwdShader<EXACT> sh(p);
   run<CFG>(p, sh, cnt);
@@ -1497,6 +1571,8 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __
   Counters cnt;
   BwdShader<EXACT> sh(p);
   run<CFG>(p, sh, cnt);
+  const unsigned s = __reduce_add_sync(0xFFFFFFFFu, cnt.replays);
+  if ((threadIdx.x & 31) == 0 && s != 0u) atomicAdd(p.stats + kStatReplays, (unsigned long long)s);
 }
 
 // ---------------------------------------------------------------- secondary rays

@@ -22,7 +22,27 @@ struct ViewDesc {
   const float* interval;  // optional [2][H][W]: per-ray [t_near, t_far] clip of the traversal
   float* record;          // optional [3][H][W] (forward): t of the first / last hit visited, terminated
   int H, W, ntx, tile_begin;
+  long long ray_begin;    // hit cache index of the view's pixel 0 (views laid out one after another)
 };
+
+// Hit cache: every ray's first k-closest query as the forward found it, so
+// the adjoint replays it instead of traversing again (the query's result
+// depends only on the ray, the BVH and the key range, all unchanged). A
+// 32-byte header, then k + 1 rows of `rays` 64-bit words: rows 0..k-1 the
+// sorted keys, row k the trusted bound t_drop (float bits). The adjoint uses
+// it only if the header's k, ray count and BVH generation are its own.
+struct HitCacheHeader {
+  uint32_t magic;
+  uint32_t k;
+  long long rays;
+  unsigned long long gen;  // BVH builds + refits of the handle when the forward ran
+  unsigned long long pad;
+};
+constexpr uint32_t kHitCacheMagic = 0x43485454u;  // "TTHC"
+constexpr int kCacheOff = 0, kCacheWrite = 1, kCacheRead = 2;
+__host__ __device__ inline size_t hit_cache_bytes(int k, long long rays) {
+  return sizeof(HitCacheHeader) + (size_t)(k + 1) * 8 * (size_t)rays;
+}
 
 // Secondary-ray passes: one record per ray of each pixel's ray tree
 // (64 bytes). Level 0 holds the primary rays (record i = pixel i of view 0;
@@ -89,6 +109,11 @@ struct TraceParams {
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)
   SecParams sec;              // secondary-ray passes only
+  // hit cache (plain forward / adjoint only)
+  void* hit_cache;
+  int cache_mode;             // kCache*
+  long long cache_rays;       // rays of all views of the launch
+  unsigned long long cache_gen;
 };
 
 struct HitStreamParams {
@@ -103,10 +128,11 @@ struct HitStreamParams {
   int* status;
 };
 
-// forward counters: rays, evaluated hits, blended hits, node visits, triangle
-// tests, queries, warp-packet node visits, interval continuations, interval
-// re-traces
-constexpr int kNumStats = 9;
+// counters: rays, evaluated hits, blended hits, node visits, triangle tests,
+// queries, warp-packet node visits, interval continuations, interval
+// re-traces (forward), hit cache replays (adjoint)
+constexpr int kNumStats = 10;
+constexpr int kStatReplays = 9;
 
 constexpr int kTraceThreads = 128;
 constexpr int kStackDepth = 32;

@@ -107,17 +107,40 @@ __device__ __forceinline__ RayW make_ray(float3 o, float3 d) {
   return r;
 }
 
+// Axis permutation of the watertight test: the ray's own (kx, ky, kz), picked
+// at run time ...
+struct PermRt {
+  int kx, ky, kz;
+  __device__ __forceinline__ float x(float a, float b, float c) const { return sel3(a, b, c, kx); }
+  __device__ __forceinline__ float y(float a, float b, float c) const { return sel3(a, b, c, ky); }
+  __device__ __forceinline__ float z(float a, float b, float c) const { return sel3(a, b, c, kz); }
+};
+// ... or fixed at compile time, for a warp whose rays all share it (the
+// selects disappear; the arithmetic is the same).
+template <int KX, int KY, int KZ>
+struct PermCt {
+  template <int K>
+  __device__ __forceinline__ static float pick(float a, float b, float c) {
+    return K == 0 ? a : (K == 1 ? b : c);
+  }
+  __device__ __forceinline__ float x(float a, float b, float c) const { return pick<KX>(a, b, c); }
+  __device__ __forceinline__ float y(float a, float b, float c) const { return pick<KY>(a, b, c); }
+  __device__ __forceinline__ float z(float a, float b, float c) const { return pick<KZ>(a, b, c); }
+};
+
 // Watertight, non-culling ray/triangle test in FP32 with the paper's FP64
 // fall-back for zero edge functions. Every operation uses an explicit
 // round-to-nearest intrinsic so nothing is contracted: t is bit-identical to
-// the CPU oracle's evaluation of the same steps.
-__device__ __forceinline__ bool isect_tri(const RayW& r, float4 a, float4 b, float4 c, float& t) {
+// the CPU oracle's evaluation of the same steps. `pm` must be the ray's own
+// permutation (r.kx, r.ky, r.kz).
+template <class Perm>
+__device__ __forceinline__ bool isect_tri_p(const RayW& r, const Perm& pm, float4 a, float4 b, float4 c, float& t) {
   const float Ax0 = __fsub_rn(a.x, r.ox), Ay0 = __fsub_rn(a.y, r.oy), Az0 = __fsub_rn(a.z, r.oz);
   const float Bx0 = __fsub_rn(b.x, r.ox), By0 = __fsub_rn(b.y, r.oy), Bz0 = __fsub_rn(b.z, r.oz);
   const float Cx0 = __fsub_rn(c.x, r.ox), Cy0 = __fsub_rn(c.y, r.oy), Cz0 = __fsub_rn(c.z, r.oz);
-  const float Akx = sel3(Ax0, Ay0, Az0, r.kx), Aky = sel3(Ax0, Ay0, Az0, r.ky), Akz = sel3(Ax0, Ay0, Az0, r.kz);
-  const float Bkx = sel3(Bx0, By0, Bz0, r.kx), Bky = sel3(Bx0, By0, Bz0, r.ky), Bkz = sel3(Bx0, By0, Bz0, r.kz);
-  const float Ckx = sel3(Cx0, Cy0, Cz0, r.kx), Cky = sel3(Cx0, Cy0, Cz0, r.ky), Ckz = sel3(Cx0, Cy0, Cz0, r.kz);
+  const float Akx = pm.x(Ax0, Ay0, Az0), Aky = pm.y(Ax0, Ay0, Az0), Akz = pm.z(Ax0, Ay0, Az0);
+  const float Bkx = pm.x(Bx0, By0, Bz0), Bky = pm.y(Bx0, By0, Bz0), Bkz = pm.z(Bx0, By0, Bz0);
+  const float Ckx = pm.x(Cx0, Cy0, Cz0), Cky = pm.y(Cx0, Cy0, Cz0), Ckz = pm.z(Cx0, Cy0, Cz0);
   const float Ax = __fsub_rn(Akx, __fmul_rn(r.Sx, Akz));
   const float Ay = __fsub_rn(Aky, __fmul_rn(r.Sy, Akz));
   const float Bx = __fsub_rn(Bkx, __fmul_rn(r.Sx, Bkz));
@@ -144,6 +167,33 @@ __device__ __forceinline__ bool isect_tri(const RayW& r, float4 a, float4 b, flo
   // bits, where -0 would sort after every other hit
   t = __fadd_rn(__fdiv_rn(T, det), 0.0f);
   return true;
+}
+
+__device__ __forceinline__ bool isect_tri(const RayW& r, float4 a, float4 b, float4 c, float& t) {
+  return isect_tri_p(r, PermRt{r.kx, r.ky, r.kz}, a, b, c, t);
+}
+
+// Packed permutation: kx | ky << 2 | kz << 4. The six values the watertight
+// set-up produces (kz = dominant axis; kx, ky the other two, swapped when the
+// direction along kz is negative).
+__device__ __forceinline__ int perm_pack(const RayW& r) { return r.kx | (r.ky << 2) | (r.kz << 4); }
+constexpr int kPerm12_0 = 1 | (2 << 2) | (0 << 4), kPerm21_0 = 2 | (1 << 2) | (0 << 4);
+constexpr int kPerm20_1 = 2 | (0 << 2) | (1 << 4), kPerm02_1 = 0 | (2 << 2) | (1 << 4);
+constexpr int kPerm01_2 = 0 | (1 << 2) | (2 << 4), kPerm10_2 = 1 | (0 << 2) | (2 << 4);
+
+// Calls fn(perm) with a compile-time permutation when `pack` (warp-uniform)
+// is one of the six, else with the ray's run-time one.
+template <class Fn>
+__device__ __forceinline__ void with_perm(int pack, const RayW& r, Fn&& fn) {
+  switch (pack) {
+    case kPerm12_0: fn(PermCt<1, 2, 0>{}); break;
+    case kPerm21_0: fn(PermCt<2, 1, 0>{}); break;
+    case kPerm20_1: fn(PermCt<2, 0, 1>{}); break;
+    case kPerm02_1: fn(PermCt<0, 2, 1>{}); break;
+    case kPerm01_2: fn(PermCt<0, 1, 2>{}); break;
+    case kPerm10_2: fn(PermCt<1, 0, 2>{}); break;
+    default: fn(PermRt{r.kx, r.ky, r.kz}); break;
+  }
 }
 
 // ---------------------------------------------------------------- vectors

@@ -45,6 +45,16 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
 
 
+def _set_cache(a, hit_cache, device):
+    """Puts an optional hit-cache buffer (uint8 device tensor) into an argument block."""
+    if hit_cache is None:
+        a.hit_cache, a.hit_cache_bytes = ctypes.c_void_p(0), 0
+        return
+    if not isinstance(hit_cache, torch.Tensor) or hit_cache.device != device or not hit_cache.is_contiguous():
+        raise RuntimeError("hit_cache must be a contiguous tensor on the tracer's device (new_hit_cache)")
+    a.hit_cache, a.hit_cache_bytes = _ptr(hit_cache), hit_cache.numel() * hit_cache.element_size()
+
+
 def _f32(t, name, device):
     if not isinstance(t, torch.Tensor):
         raise RuntimeError(f"{name} must be a tensor")
@@ -81,6 +91,7 @@ class OptixTracer:
             raise RuntimeError("OptixTracer needs a CUDA device")
         self.variant = _VARIANTS[forward]
         self.device = torch.device("cuda", torch.cuda.current_device())
+        self.use_hit_cache = False  # set by diff_tritracer.Tracer (its autograd path passes a hit cache)
         cfg = _lib.TtConfig()
         cfg.variant = self.variant
         cfg.tmin_inclusive = 1 if tmin_inclusive else 0
@@ -142,11 +153,22 @@ class OptixTracer:
                                        int(number_of_points), _stream()))
         self._keep = (verts, cumsum)
 
+    def new_hit_cache(self, rays, k=None):
+        """A device buffer for the hit cache of `rays` rays: sized for the
+        current traversal configuration (tt_hit_cache_bytes), or for queries of
+        `k` hits (k = 32 fits every configuration). No reference counterpart."""
+        n = lib.tt_hit_cache_bytes(self._h, int(rays))
+        if k is not None:
+            n = max(n, 32 + (int(k) + 1) * 8 * int(rays))
+        return torch.empty((n,), dtype=torch.uint8, device=self.device)
+
     def trace_forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
                       cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, colors_precomp, opacities,
-                      scaling, density_factor, bg_color, extra, rebuild_gas_opt, debug):
+                      scaling, density_factor, bg_color, extra, rebuild_gas_opt, debug, hit_cache=None):
         """tracer.cpp:16-142: returns FwdTraceResult((color [3,H,W], others [7,H,W],
-        gpu_time [1], scaling, density_factor, max_blending [P]))."""
+        gpu_time [1], scaling, density_factor, max_blending [P])). With
+        `hit_cache` (a new_hit_cache(H * W) buffer) the forward also stores every
+        ray's first query there for trace_backward."""
         dev = self.device
         P = int(number_of_points)
         ro = _f32(ray_o, "ray_o", dev)
@@ -189,6 +211,7 @@ class OptixTracer:
         a.rebuild_gas, a.debug = int(rebuild_gas_opt), 1 if debug else 0
         a.out_color, a.out_others, a.max_blending = _ptr(out_color), _ptr(out_others), _ptr(max_blending)
         a.gpu_time_ms = ctypes.pointer(ms)
+        _set_cache(a, hit_cache, dev)
         if self._proposal is not None:
             v = _lib.TtView()
             v.H, v.W, v.ray_o, v.ray_d = H, W, a.ray_o, a.ray_d
@@ -207,16 +230,18 @@ class OptixTracer:
         if debug:
             gpu_time.fill_(ms.value)
         # the arrays the kernels read must outlive the asynchronous launch
-        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de, iv, cp)
+        self._keep = (ro, rd, verts, sig, npts, cums, sh, opac, bg, ex, sc, de, iv, cp, hit_cache)
         return FwdTraceResult((out_color, out_others, gpu_time, scaling, density_factor, max_blending))
 
     def trace_backward(self, ray_o, ray_d, background, triangles_points, sigma, num_points_per_triangle,
                        cumsum_of_points_per_triangle, colors, others, number_of_points, shs, sh_degree, opacities,
-                       dL_dpixels, dL_dothers, scaling, debug, colors_precomp=None):
+                       dL_dpixels, dL_dothers, scaling, debug, colors_precomp=None, hit_cache=None):
         """tracer.cpp:144-228: returns BwdTraceResult((dL_dtriangle [V,3],
         dL_dsigma like sigma, dL_dopacity like opacities, dL_dsh [P,M,3])).
         With empty shs and colors_precomp [P, 3] (the forward's colours) the
-        result also carries .dL_dcolors [P, 3]."""
+        result also carries .dL_dcolors [P, 3]. `hit_cache`: the buffer the
+        forward of these rays filled; the adjoint replays it where still valid
+        (same results either way)."""
         dev = self.device
         P = int(number_of_points)
         ro = _f32(ray_o, "ray_o", dev)
@@ -257,6 +282,7 @@ class OptixTracer:
         a.dL_dtriangle, a.dL_dsigma = _ptr(dL_dtriangle), _ptr(dL_dsigma)
         a.dL_dopacity, a.dL_dsh = _ptr(dL_dopacity), _ptr(dL_dsh)
         a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        _set_cache(a, hit_cache, dev)
         if self._proposal is not None:
             v = _lib.TtView()
             v.H, v.W, v.ray_o, v.ray_d = H, W, a.ray_o, a.ray_d
@@ -267,7 +293,7 @@ class OptixTracer:
         else:
             iv = None
             check(self._h, lib.tt_backward(self._h, ctypes.byref(a), _stream()))
-        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg, iv, cp)
+        self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg, iv, cp, hit_cache)
         res = BwdTraceResult((dL_dtriangle, dL_dsigma, dL_dopacity, dL_dsh))
         res.dL_dcolors = dcols
         return res
@@ -414,11 +440,12 @@ class OptixTracer:
     def trace_forward_views(self, rays, triangles_points, sigma, num_points_per_triangle,
                             cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, opacities, scaling,
                             density_factor, bg_color, rebuild_gas_opt, outputs=None, max_blending=None,
-                            intervals=None, records=None):
+                            intervals=None, records=None, hit_cache=None):
         """Forward over up to 32 views of any resolutions in one launch.
         rays: list of (ray_o, ray_d), each [H, W, 3]. Returns ([(color, others)], max_blending).
         intervals: optional per-view [2, H, W] proposed [t_near, t_far] clips (None entries allowed);
-        records: optional per-view [3, H, W] outputs of (t_first, t_last, terminated) per ray."""
+        records: optional per-view [3, H, W] outputs of (t_first, t_last, terminated) per ray;
+        hit_cache: optional new_hit_cache(sum of H * W) buffer for trace_backward_views."""
         dev = self.device
         P = int(number_of_points)
         if max_blending is None:
@@ -443,13 +470,14 @@ class OptixTracer:
             outs.append((col, oth))
             keep = keep + (ro, rd)
             keep = keep + self._interval_record(vs[i], H, W, intervals, records, i)
+        _set_cache(a, hit_cache, dev)
         check(self._h, lib.tt_forward_views(self._h, ctypes.byref(a), vs, len(rays), _stream()))
-        self._keep = keep
+        self._keep = keep + (hit_cache,)
         return outs, max_blending
 
     def trace_backward_views(self, rays, forward_outputs, upstream, triangles_points, sigma,
                              num_points_per_triangle, cumsum_of_points_per_triangle, number_of_points, shs,
-                             sh_degree, opacities, bg_color, grads=None, intervals=None):
+                             sh_degree, opacities, bg_color, grads=None, intervals=None, hit_cache=None):
         """Adjoint over the views of trace_forward_views. upstream: list of
         (dL_dpixels [3,H,W], dL_dothers [7,H,W]). Returns (dL_dtriangle, dL_dsigma,
         dL_dopacity, dL_dsh) summed over the views."""
@@ -477,8 +505,9 @@ class OptixTracer:
         a.opacities = _ptr(opac)
         a.dL_dtriangle, a.dL_dsigma, a.dL_dopacity, a.dL_dsh = [_ptr(g) for g in grads]
         a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
+        _set_cache(a, hit_cache, dev)
         vs = (_lib.TtView * len(rays))()
-        keep = (verts, sig, npts, cums, sh, opac, bg)
+        keep = (verts, sig, npts, cums, sh, opac, bg, hit_cache)
         for i, ((ro, rd), (col, oth), (g, go)) in enumerate(zip(rays, forward_outputs, upstream)):
             ro, rd = _f32(ro, "ray_o", dev), _f32(rd, "ray_d", dev)
             col, oth = _f32(col, "colors", dev), _f32(oth, "others", dev)

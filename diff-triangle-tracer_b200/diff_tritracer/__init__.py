@@ -58,8 +58,14 @@ class _Tracer(torch.autograd.Function):
         args = (ray_o, ray_d, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,
                 number_of_points, shs, st.sh_degree, colors_precomp, opacities, scaling, density_factor, st.bg,
                 st.extra_params, st.rebuild_gas, st.debug)
-        res = _call_with_snapshot(tracer.trace_forward, args, st.debug, "snapshot_fw.dump", "forward")
+        # every ray's first hit query, kept for the adjoint like an activation
+        cache = None
+        if tracer.use_hit_cache and tracer.variant == _C._lib.TT_VARIANT_PLAIN and ray_o.dim() >= 2:
+            cache = tracer.new_hit_cache(int(ray_o.shape[0]) * int(ray_o.shape[1]))
+        fwd = tracer.trace_forward if cache is None else (lambda *a: tracer.trace_forward(*a, hit_cache=cache))
+        res = _call_with_snapshot(fwd, args, st.debug, "snapshot_fw.dump", "forward")
         color, others, gpu_time, scaling, density_factor, max_blending = res.data
+        ctx.hit_cache = cache
         ctx.tracer_settings = st
         ctx.tracer = tracer
         ctx.number_of_points = number_of_points
@@ -81,9 +87,14 @@ class _Tracer(torch.autograd.Function):
                 cumsum_of_points_per_triangle, color, others, ctx.number_of_points, shs, st.sh_degree, opacities,
                 grad_color, grad_others, scaling, st.debug)
         use_cols = shs.numel() == 0 and colors_precomp.numel() > 0  # precomputed colours in place of SH
-        fn = (lambda *a: ctx.tracer.trace_backward(*a, colors_precomp=colors_precomp)) if use_cols \
-            else ctx.tracer.trace_backward
+        cache = ctx.hit_cache
+
+        def fn(*a):
+            return ctx.tracer.trace_backward(*a, colors_precomp=colors_precomp if use_cols else None,
+                                             hit_cache=cache)
+
         res = _call_with_snapshot(fn, args, st.debug, "snapshot_bw.dump", "backward")
+        ctx.hit_cache = None
         grad_triangles, grad_sigma, grad_opacities, grad_sh = res.data
         grad_cols = res.dL_dcolors.reshape(colors_precomp.shape) if use_cols else None
         return (
@@ -110,10 +121,15 @@ class Tracer(nn.Module):
     "envlight.ptx" / "backward.ptx"); nothing is read from disk."""
 
     def __init__(self, forwad_ptx="forward.ptx", backward_ptx="backward.ptx", tmin_inclusive: bool = True,
-                 exact_adjoint: bool = False) -> None:
+                 exact_adjoint: bool = False, hit_cache: bool = True) -> None:
+        """hit_cache (no reference counterpart): the forward keeps every ray's
+        first k-closest query in a device buffer held by the autograd graph
+        ((k + 1) * 8 bytes a ray) and the backward replays it instead of
+        traversing the BVH again; the gradients are the same either way."""
         super().__init__()
         self.tracer = _C.OptixTracer("", forwad_ptx, backward_ptx, tmin_inclusive=tmin_inclusive,
                                      exact_adjoint=exact_adjoint)
+        self.tracer.use_hit_cache = bool(hit_cache)
 
     def forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,
                 number_of_points, opacities, scaling, density_factor, shs, colors_precomp,

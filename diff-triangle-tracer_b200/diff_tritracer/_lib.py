@@ -53,6 +53,7 @@ class TtFwdArgs(ctypes.Structure):
         ("rebuild_gas", ctypes.c_int), ("debug", ctypes.c_int),
         ("out_color", _vp), ("out_others", _vp), ("max_blending", _vp),
         ("gpu_time_ms", _f),
+        ("hit_cache", _vp), ("hit_cache_bytes", ctypes.c_size_t),
     ]
 
 
@@ -69,6 +70,7 @@ class TtBwdArgs(ctypes.Structure):
         ("dL_dtriangle", _vp), ("dL_dsigma", _vp), ("dL_dopacity", _vp), ("dL_dsh", _vp),
         ("gpu_time_ms", _f),
         ("colors_precomp", _vp), ("dL_dcolors", _vp),
+        ("hit_cache", _vp), ("hit_cache_bytes", ctypes.c_size_t),
     ]
 
 
@@ -83,7 +85,8 @@ class TtStats(ctypes.Structure):
                 ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
                 ("node_visits", ctypes.c_ulonglong), ("triangle_tests", ctypes.c_ulonglong),
                 ("queries", ctypes.c_ulonglong), ("packet_node_visits", ctypes.c_ulonglong),
-                ("interval_continuations", ctypes.c_ulonglong), ("interval_retraces", ctypes.c_ulonglong)]
+                ("interval_continuations", ctypes.c_ulonglong), ("interval_retraces", ctypes.c_ulonglong),
+                ("hit_cache_replays", ctypes.c_ulonglong)]
 
 
 TT_MLP_PARAMS = 16640
@@ -112,7 +115,7 @@ EXPORTS = (
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
     "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
     "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree", "tt_bvh_save",
-    "tt_bvh_load",
+    "tt_bvh_load", "tt_hit_cache_bytes",
 )
 
 
@@ -147,8 +150,10 @@ def _load():
     lib.tt_mlp_predict.argtypes = [_vp, ctypes.POINTER(TtMlp), _vp, ctypes.c_int, _vp, _vp]
     lib.tt_mlp_intervals.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtView), ctypes.c_int,
                                      ctypes.POINTER(_vp), ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp]
+    lib.tt_hit_cache_bytes.argtypes = [_vp, ctypes.c_longlong]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype if name == "tt_last_error" else ctypes.c_int
+    lib.tt_hit_cache_bytes.restype = ctypes.c_size_t
     return lib
 
 

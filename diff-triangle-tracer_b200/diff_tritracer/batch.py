@@ -4,7 +4,9 @@
 through ONE persistent forward launch and ONE adjoint launch per step
 (tt_forward_views / tt_backward_views). With `graph=True` the step - BVH refit
 to the current vertices, forward, adjoint - is recorded once into a CUDA graph
-and replayed, so a training step costs one graph launch on the host. Rays and
+and replayed, so a training step costs one graph launch on the host. With
+`hit_cache=True` the forward keeps every ray's first query in a static buffer
+and the adjoint replays it instead of traversing again. Rays and
 upstream gradients are copied into the batch's static buffers before replay;
 the scene tensors must keep their storage between steps (optimisers update
 them in place).
@@ -19,7 +21,7 @@ from ._C import OptixTracer
 
 class ViewBatch:
     def __init__(self, tracer: OptixTracer, shapes, scene: dict, sh_degree: int, bg: torch.Tensor,
-                 graph: bool = True):
+                 graph: bool = True, hit_cache: bool = True):
         """shapes: [(H, W)] per view. scene: dict with triangles_points, sigma,
         num_points_per_triangle, cumsum_of_points_per_triangle, number_of_points,
         shs, opacities, scaling, density_factor (device tensors)."""
@@ -40,6 +42,8 @@ class ViewBatch:
         M = scene["shs"].shape[1]
         self.grads = (torch.zeros((V, 3), **f32), torch.zeros_like(scene["sigma"]),
                       torch.zeros_like(scene["opacities"]), torch.zeros((P, M, 3), **f32))
+        # sized for 32-hit queries, so it serves every traversal configuration
+        self.hit_cache = tracer.new_hit_cache(sum(H * W for H, W in shapes), k=32) if hit_cache else None
         self.graph = None
         # the first pass builds the BVH outside any capture
         self._forward(0)
@@ -56,14 +60,15 @@ class ViewBatch:
         self.tracer.trace_forward_views(self.rays, s["triangles_points"], s["sigma"], s["num_points_per_triangle"],
                                         s["cumsum_of_points_per_triangle"], s["number_of_points"], s["shs"],
                                         self.sh_degree, s["opacities"], s["scaling"], s["density_factor"], self.bg,
-                                        rebuild_gas, outputs=self.outputs, max_blending=self.max_blending)
+                                        rebuild_gas, outputs=self.outputs, max_blending=self.max_blending,
+                                        hit_cache=self.hit_cache)
 
     def _backward(self):
         s = self.scene
         self.tracer.trace_backward_views(self.rays, self.outputs, self.upstream, s["triangles_points"], s["sigma"],
                                          s["num_points_per_triangle"], s["cumsum_of_points_per_triangle"],
                                          s["number_of_points"], s["shs"], self.sh_degree, s["opacities"], self.bg,
-                                         grads=self.grads)
+                                         grads=self.grads, hit_cache=self.hit_cache)
 
     def set_rays(self, rays):
         for (ro, rd), (so, sd) in zip(rays, self.rays):

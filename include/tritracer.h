@@ -22,6 +22,7 @@
 #ifndef TRITRACER_H
 #define TRITRACER_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -110,6 +111,14 @@ typedef struct tt_fwd_args {
   float* out_others;     /* [7,H,W], fully written */
   float* max_blending;   /* [P], zeroed then written */
   float* gpu_time_ms;    /* host pointer, may be NULL */
+  /* Optional hit cache (plain program; NULL = none; no reference counterpart):
+   * device memory of at least tt_hit_cache_bytes(h, rays) bytes, 16-byte
+   * aligned, rays = H * W (the sum over the views of a batched call). The
+   * forward stores every ray's first k-closest query in it; a tt_backward
+   * given the same cache replays those queries instead of traversing the BVH
+   * again. tt_forward_noalloc ignores it. */
+  void* hit_cache;
+  size_t hit_cache_bytes;
 } tt_fwd_args;
 
 /* Arguments of the adjoint: OptixTracer::trace_bwd (tritracer/tracer.h:97-114,
@@ -142,6 +151,13 @@ typedef struct tt_bwd_args {
   float* gpu_time_ms;  /* host pointer, may be NULL */
   const float* colors_precomp; /* [P][3]: the forward's precomputed colours (shs NULL), or NULL */
   float* dL_dcolors;           /* [P][3] gradient of colors_precomp (zeroed, then accumulated) */
+  /* Optional: the hit cache the forward of these rays filled (NULL = re-trace).
+   * It is only replayed if it was written with the handle's current k and ray
+   * count, and no build, refit or load of the BVH happened since; otherwise
+   * the adjoint traverses as without it. The results are the same either way:
+   * a replayed query is the one the adjoint would compute. */
+  const void* hit_cache;
+  size_t hit_cache_bytes;
 } tt_bwd_args;
 
 /* One camera image of a batched call: rays [H][W][3]; the forward writes
@@ -207,6 +223,11 @@ int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, 
  * used by the autotuner. No reference counterpart. */
 int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
 
+/* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the
+ * handle's current traversal configuration: 32 + (k + 1) * 8 * rays. No
+ * reference counterpart. */
+size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays);
+
 /* Message of the last failed call on this handle (never NULL). */
 const char* tt_last_error(const tt_tracer* h);
 
@@ -233,6 +254,7 @@ typedef struct tt_stats {
   unsigned long long packet_node_visits; /* node visits counted once per warp packet */
   unsigned long long interval_continuations; /* rays that went on beyond their proposed t_far */
   unsigned long long interval_retraces;      /* rays traced again: no hit in their interval */
+  unsigned long long hit_cache_replays;      /* adjoint queries replayed from a hit cache */
 } tt_stats;
 
 /* Synchronises `stream`, then fills *out. */

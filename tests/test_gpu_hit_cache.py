@@ -1,0 +1,153 @@
+"""Hit cache (tt_fwd_args.hit_cache / tt_bwd_args.hit_cache): the forward
+stores every ray's first k-closest query, the adjoint replays it instead of
+traversing the BVH again.
+
+* the replayed adjoint equals the re-traced one (gradients up to the order of
+  float atomics) for every traversal configuration, and every ray's first
+  query is replayed (hit_cache_replays == rays);
+* a refit between forward and adjoint, or a different k, makes the adjoint
+  ignore the cache (no replay) and still give the same gradients;
+* batched views, proposed intervals and the exact adjoint replay too;
+* the autograd module gives the same gradients with and without the cache;
+* the forward rejects a cache smaller than tt_hit_cache_bytes.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import diff_tritracer  # noqa: E402
+from diff_tritracer import _C, scenes  # noqa: E402
+from gpu_helpers import DEV, T, rel_norm, settings  # noqa: E402
+from scenes_for_tests import dense_scene, dense_view  # noqa: E402
+
+H, W = 48, 64
+GRAD_RTOL = 1e-6  # same hits in the same order: only the atomic summation order differs
+
+
+@pytest.fixture(scope="module")
+def setup():
+    sc = dense_scene(seed=2, P=3000)
+    ro, rd = dense_view(H=H, W=W)
+    g, go = scenes.upstream_grads(H, W, seed=3, others_std=1.0)
+    s = dict(verts=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), npts=T(sc.num_points), cums=T(sc.cumsum),
+             shs=T(sc.shs), opac=T(sc.opacities))
+    return sc, s, T(ro), T(rd), T(g), T(go)
+
+
+def forward(tr, sc, s, ro, rd, cache=None, rebuild=0):
+    st = settings(rebuild=rebuild)
+    res = tr.trace_forward(ro, rd, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3,
+                           torch.empty(0, device=DEV), s["opac"], torch.zeros(sc.P, device=DEV),
+                           torch.zeros(sc.P, device=DEV), st.bg, st.extra_params, st.rebuild_gas, False,
+                           hit_cache=cache)
+    return res.data[0], res.data[1]
+
+
+def backward(tr, sc, s, ro, rd, col, oth, g, go, cache=None):
+    tr.reset_stats()
+    res = tr.trace_backward(ro, rd, torch.zeros(3, device=DEV), s["verts"], s["sigma"], s["npts"], s["cums"], col,
+                            oth, sc.P, s["shs"], 3, s["opac"], g, go, torch.zeros(sc.P, device=DEV), False,
+                            hit_cache=cache)
+    replays = tr.stats()["hit_cache_replays"]
+    tr.device_status()
+    return [x.cpu().numpy() for x in res.data], replays
+
+
+def assert_grads_equal(a, b):
+    for x, y, name in zip(a, b, ("dtri", "dsigma", "dopac", "dsh")):
+        assert rel_norm(x, y) < GRAD_RTOL, name
+
+
+@pytest.mark.parametrize("mode,k", [("packets", 32), ("packets", 16), ("lanes", 16)])
+def test_replay_equals_retrace(setup, mode, k):
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal=mode)
+    tr.set_traversal(mode, k=k)
+    cache = tr.new_hit_cache(H * W)
+    assert cache.numel() == 32 + (k + 1) * 8 * H * W
+    col, oth = forward(tr, sc, s, ro, rd, cache)
+    # the cache does not change the forward
+    col0, oth0 = forward(tr, sc, s, ro, rd, None, rebuild=2)
+    assert torch.equal(col, col0) and torch.equal(oth, oth0)
+    forward(tr, sc, s, ro, rd, cache, rebuild=2)  # keep: the BVH generation is unchanged
+    replayed, n = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+    assert n == H * W
+    traced, n0 = backward(tr, sc, s, ro, rd, col, oth, g, go, None)
+    assert n0 == 0
+    assert_grads_equal(replayed, traced)
+
+
+def test_stale_cache_is_ignored(setup):
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal="packets")
+    tr.set_traversal("packets", k=32)
+    cache = tr.new_hit_cache(H * W)
+    col, oth = forward(tr, sc, s, ro, rd, cache)
+    traced, _ = backward(tr, sc, s, ro, rd, col, oth, g, go, None)
+    # a refit after the forward: the cache may no longer match the BVH
+    tr.build_tri_accel(s["verts"], s["cums"], sc.P, False)
+    got, n = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+    assert n == 0
+    assert_grads_equal(got, traced)
+    # another k: the cache holds 32-hit queries, the adjoint now takes 16
+    col, oth = forward(tr, sc, s, ro, rd, cache, rebuild=2)
+    tr.set_traversal("packets", k=16)
+    got, n = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+    assert n == 0
+    assert_grads_equal(got, traced)
+
+
+def test_views_intervals_and_exact_adjoint(setup):
+    sc, s, ro, rd, g, go = setup
+    views = [(ro, rd), tuple(T(a) for a in dense_view(H=7, W=130, origin=(-0.2, 0.5, 2.8)))]
+    ups = [(g, go), tuple(T(a) for a in scenes.upstream_grads(7, 130, seed=4, others_std=1.0))]
+    rays = sum(v[0].shape[0] * v[0].shape[1] for v in views)
+    # a far clip in the middle of the cloud: unterminated rays continue beyond it
+    ivs = [torch.stack([torch.zeros(v[0].shape[:2], device=DEV), torch.full(v[0].shape[:2], 2.9, device=DEV)])
+           for v in views]
+    for exact in (False, True):
+        tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", exact_adjoint=exact)
+        tr.build_tri_accel(s["verts"], s["cums"], sc.P, True)
+        for iv in (None, ivs):
+            cache = tr.new_hit_cache(rays)
+            outs, _ = tr.trace_forward_views(views, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3,
+                                             s["opac"], torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV),
+                                             torch.zeros(3, device=DEV), 2, intervals=iv, hit_cache=cache)
+            res = {}
+            for c in (cache, None):
+                tr.reset_stats()
+                gr = tr.trace_backward_views(views, outs, ups, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P,
+                                             s["shs"], 3, s["opac"], torch.zeros(3, device=DEV), intervals=iv,
+                                             hit_cache=c)
+                res[c is None] = ([x.cpu().numpy() for x in gr], tr.stats()["hit_cache_replays"])
+                tr.device_status()
+            assert res[False][1] == rays and res[True][1] == 0, (exact, iv is None)
+            assert_grads_equal(res[False][0], res[True][0])
+
+
+def test_autograd_module_with_and_without_cache(setup):
+    sc, s, ro, rd, g, go = setup
+    grads = {}
+    for use in (True, False):
+        tracer = diff_tritracer.Tracer(hit_cache=use)
+        verts = s["verts"].clone().requires_grad_(True)
+        sig, opac, shs = (s[k].clone().requires_grad_(True) for k in ("sigma", "opac", "shs"))
+        color, _, _, _, others, _ = tracer(ro, rd, verts, sig, s["npts"], s["cums"], sc.P, opac,
+                                           torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), shs, None,
+                                           settings(rebuild=0))
+        ((color * g).sum() + (others * go).sum()).backward()
+        grads[use] = [x.grad.cpu().numpy() for x in (verts, sig, opac, shs)]
+    assert_grads_equal(grads[True], grads[False])
+
+
+def test_small_cache_rejected(setup):
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    small = torch.empty(tr.new_hit_cache(H * W).numel() - 8, dtype=torch.uint8, device=DEV)
+    with pytest.raises(RuntimeError, match="hit_cache"):
+        forward(tr, sc, s, ro, rd, small)
