@@ -81,6 +81,15 @@ int accel_step(tt_tracer* h, const float* verts, int num_vertices, const int* cu
   return TT_OK;
 }
 
+// Pool entries a hit cache of `bytes` holds after its main part (-1: too
+// small for the main part).
+long long cache_pool_cap(int k, long long rays, size_t bytes) {
+  const size_t main = tt::hit_cache_main_bytes(k, rays);
+  if (bytes < main) return -1;
+  const unsigned long long cap = (bytes - main) / ((size_t)(k + 2) * 8);
+  return (long long)(cap < 0xFFFFFFF0ull ? cap : 0xFFFFFFF0ull);
+}
+
 int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P, const float* cols = nullptr) {
   if (cols && !shs) return TT_OK;  // precomputed colours in place of SH
   TT_REQUIRE(h, deg >= 0 && deg <= 3, "sh_degree must be in [0, 3]");
@@ -250,11 +259,13 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   if (a->hit_cache) {
     TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "the hit cache is for the plain program only");
     TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
-    TT_REQUIRE(h, a->hit_cache_bytes >= tt::hit_cache_bytes(h->k(), p.cache_rays),
-               "hit_cache is smaller than tt_hit_cache_bytes() for these rays");
+    const long long cap = cache_pool_cap(h->k(), p.cache_rays, a->hit_cache_bytes);
+    TT_REQUIRE(h, cap >= 0, "hit_cache is too small for these rays (tt_hit_cache_bytes)");
     p.hit_cache = a->hit_cache;
     p.cache_mode = tt::kCacheWrite;
     p.cache_gen = h->bvh_gen;
+    p.cache_pool_cap = (uint32_t)cap;
+    TT_CUDA(h, cudaMemsetAsync(a->hit_cache, 0, sizeof(tt::HitCacheHeader), s));
   }
   p.bvh = h->bvh.view();
   p.verts = a->vertices;
@@ -354,13 +365,15 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
   p.d_sigma = a->dL_dsigma;
   p.d_opac = a->dL_dopacity;
   p.d_sh = a->dL_dsh;
-  // a cache written for another k or ray count (or too small for this k)
-  // fails the kernels' header check or is not passed at all: they re-trace
-  if (a->hit_cache && a->hit_cache_bytes >= tt::hit_cache_bytes(h->k(), p.cache_rays)) {
+  // a cache written for another k, ray count or pool size (or too small for
+  // this k) fails the kernels' header check or is not passed at all: they re-trace
+  const long long cap = a->hit_cache ? cache_pool_cap(h->k(), p.cache_rays, a->hit_cache_bytes) : -1;
+  if (cap >= 0) {
     TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
     p.hit_cache = const_cast<void*>(a->hit_cache);
     p.cache_mode = tt::kCacheRead;
     p.cache_gen = h->bvh_gen;
+    p.cache_pool_cap = (uint32_t)cap;
   }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));

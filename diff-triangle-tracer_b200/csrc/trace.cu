@@ -64,7 +64,7 @@ __device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsi
 struct Counters {
   unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
   unsigned cont = 0, restart = 0;  // proposed intervals left by continuation / re-trace
-  unsigned replays = 0;            // first queries taken from the hit cache (adjoint)
+  unsigned replays = 0;            // queries taken from the hit cache (adjoint)
 };
 
 // Three-input FP32 min / max (one instruction on sm_100); min and max are
@@ -692,47 +692,96 @@ __device__ __forceinline__ int find_view(const TraceParams& p, int tile) {
   return lo;
 }
 
-// Hit cache (HitCacheHeader): the forward stores each ray's first query, the
-// adjoint replays it. Rows are written and read once, so they bypass L2
+// Hit cache (HitCacheHeader): the forward stores every query of a ray, the
+// adjoint replays them. Rows are written and read once, so they bypass L2
 // residency (streaming stores / loads) and leave it to the BVH.
-__device__ __forceinline__ unsigned long long* cache_rows(const TraceParams& p) {
+__device__ __forceinline__ HitCacheHeader* cache_header_ptr(const TraceParams& p) {
+  return static_cast<HitCacheHeader*>(p.hit_cache);
+}
+__device__ __forceinline__ unsigned long long* cache_main(const TraceParams& p) {
   return reinterpret_cast<unsigned long long*>(static_cast<char*>(p.hit_cache) + sizeof(HitCacheHeader));
+}
+template <int K>
+__device__ __forceinline__ unsigned long long* cache_pool(const TraceParams& p) {
+  return cache_main(p) + (size_t)(K + 1) * p.cache_rays;
 }
 
 template <int K>
 __device__ __forceinline__ bool cache_replays(const TraceParams& p) {
   if (p.cache_mode != kCacheRead) return false;
-  const HitCacheHeader* h = static_cast<const HitCacheHeader*>(p.hit_cache);
-  return h->magic == kHitCacheMagic && h->k == (uint32_t)K && h->rays == p.cache_rays && h->gen == p.cache_gen;
+  const HitCacheHeader* h = cache_header_ptr(p);
+  return h->magic == kHitCacheMagic && h->k == (uint32_t)K && h->rays == p.cache_rays && h->gen == p.cache_gen &&
+         h->pool_cap == p.cache_pool_cap;
 }
 
+// Forward, first query of ray g. Returns where the entry of its next query
+// gets linked (the high half of row k).
 template <int K>
-__device__ __forceinline__ void cache_store(const TraceParams& p, long long g, const Smem& sm, float t_drop) {
-  unsigned long long* rows = cache_rows(p) + g;
+__device__ __forceinline__ uint32_t* cache_put_first(const TraceParams& p, long long g, const Smem& sm, float t_drop) {
+  unsigned long long* rows = cache_main(p) + g;
+  const size_t R = (size_t)p.cache_rays;
 #pragma unroll 4
-  for (int i = 0; i < K; ++i) __stcs(rows + (size_t)i * p.cache_rays, sm.keys[i * sm.stride]);
-  __stcs(rows + (size_t)K * p.cache_rays, (unsigned long long)__float_as_uint(t_drop));
+  for (int i = 0; i < K; ++i) __stcs(rows + i * R, sm.keys[i * sm.stride]);
+  unsigned long long* w = rows + K * R;
+  __stcs(w, ((unsigned long long)kNoEntry << 32) | __float_as_uint(t_drop));
+  return reinterpret_cast<uint32_t*>(w) + 1;
 }
 
-// Fills the lane's query buffer; returns the stored t_drop.
+// Forward, a later query into pool entry e (< pool_cap), linked from `link`.
 template <int K>
-__device__ __forceinline__ float cache_load(const TraceParams& p, long long g, const Smem& sm) {
-  const unsigned long long* rows = cache_rows(p) + g;
+__device__ __forceinline__ uint32_t* cache_put_more(const TraceParams& p, uint32_t e, unsigned long long key_min,
+                                                    const Smem& sm, float t_drop, uint32_t* link) {
+  unsigned long long* rows = cache_pool<K>(p) + e;
+  const size_t C = p.cache_pool_cap;
 #pragma unroll 4
-  for (int i = 0; i < K; ++i) sm.keys[i * sm.stride] = __ldcs(rows + (size_t)i * p.cache_rays);
-  return __uint_as_float((uint32_t)__ldcs(rows + (size_t)K * p.cache_rays));
+  for (int i = 0; i < K; ++i) __stcs(rows + i * C, sm.keys[i * sm.stride]);
+  unsigned long long* w = rows + K * C;
+  __stcs(w, ((unsigned long long)kNoEntry << 32) | __float_as_uint(t_drop));
+  __stcs(rows + (K + 1) * C, key_min);
+  *link = e;
+  return reinterpret_cast<uint32_t*>(w) + 1;
+}
+
+// Forward: pool entries for the lanes in `want` (one atomic per warp).
+__device__ __forceinline__ uint32_t cache_alloc(const TraceParams& p, bool want) {
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
+  if (m == 0u) return kNoEntry;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  uint32_t base = 0u;
+  if (lane == leader) base = atomicAdd(&cache_header_ptr(p)->pool_used, (uint32_t)__popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  return want ? base + (uint32_t)__popc(m & ((1u << lane) - 1u)) : kNoEntry;
+}
+
+// Adjoint: fills the lane's query buffer from the first query of ray g or
+// from pool entry e; returns t_drop and the entry of the next query.
+template <int K>
+__device__ __forceinline__ float cache_get(const TraceParams& p, bool first, long long g, uint32_t e, const Smem& sm,
+                                           uint32_t& next) {
+  const unsigned long long* rows = first ? cache_main(p) + g : cache_pool<K>(p) + e;
+  const size_t S = first ? (size_t)p.cache_rays : (size_t)p.cache_pool_cap;
+#pragma unroll 4
+  for (int i = 0; i < K; ++i) sm.keys[i * sm.stride] = __ldcs(rows + i * S);
+  const unsigned long long w = __ldcs(rows + K * S);
+  next = (uint32_t)(w >> 32);
+  return __uint_as_float((uint32_t)w);
+}
+
+// Adjoint: does pool entry e hold the query that starts at key_min?
+template <int K>
+__device__ __forceinline__ bool cache_has(const TraceParams& p, uint32_t e, unsigned long long key_min) {
+  return e < p.cache_pool_cap && __ldcs(cache_pool<K>(p) + (size_t)(K + 1) * p.cache_pool_cap + e) == key_min;
 }
 
 template <int K>
 __device__ __forceinline__ void cache_header(const TraceParams& p) {
   if (p.cache_mode == kCacheWrite && blockIdx.x == 0 && threadIdx.x == 0) {
-    HitCacheHeader h;
-    h.magic = kHitCacheMagic;
-    h.k = K;
-    h.rays = p.cache_rays;
-    h.gen = p.cache_gen;
-    h.pad = 0;
-    *static_cast<HitCacheHeader*>(p.hit_cache) = h;
+    HitCacheHeader* h = cache_header_ptr(p);  // pool_used was zeroed by the host
+    h->magic = kHitCacheMagic;
+    h->k = K;
+    h->rays = p.cache_rays;
+    h->gen = p.cache_gen;
+    h->pool_cap = p.cache_pool_cap;
   }
 }
 
@@ -751,7 +800,9 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
   bool have = false, exhausted = false;
   Cursor cur = first_cursor(p.tmin_inclusive);
   float3 o = make_float3(0.f, 0.f, 0.f), d = o;
-  long long g = 0;  // hit cache index of the lane's ray
+  long long g = 0;              // hit cache index of the lane's ray
+  uint32_t* link = nullptr;     // forward: where the entry of the ray's next query gets linked
+  uint32_t next = kNoEntry;     // adjoint: entry of the ray's next query
   const bool replay = cache_replays<K>(p);
   for (;;) {
     const unsigned need = __ballot_sync(full, !have && !exhausted);
@@ -790,16 +841,25 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
     }
     float t_drop = INFINITY;
     if (have) {
-      if (replay && cur.chunks == 0) {  // first query of the ray, as the forward found it
-        t_drop = cache_load<K>(p, g, sm);
+      const bool first = cur.chunks == 0;  // the ray's queries are numbered by its chunks
+      if (replay && (first || cache_has<K>(p, next, cur.key_min))) {  // as the forward found it
+        t_drop = cache_get<K>(p, first, g, next, sm, next);
         ++cnt.replays;
       } else {
+        next = kNoEntry;
         const RayW r = make_ray(o, d);
         unsigned long long kb[kChunk];
         query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
         for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
-        if (p.cache_mode == kCacheWrite && cur.chunks == 0) cache_store<K>(p, g, sm, t_drop);
+        if (p.cache_mode == kCacheWrite) {
+          if (first) {
+            link = cache_put_first<K>(p, g, sm, t_drop);
+          } else if (link) {
+            const uint32_t e = atomicAdd(&cache_header_ptr(p)->pool_used, 1u);
+            link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
+          }
+        }
       }
     }
     __syncwarp();
@@ -860,16 +920,29 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       sh.begin(&v, pix, o, d);  // the plain shaders always trace their one ray
     }
     const RayW r = make_ray(o, d);
+    uint32_t* link = nullptr;  // forward: where the entry of the ray's next query gets linked
+    uint32_t next = kNoEntry;  // adjoint: entry of the ray's next query
     for (bool first = true; __any_sync(full, active); first = false) {
       float t_drop = INFINITY;
-      if (first && replay) {  // every ray's first query, as the forward found it
-        if (active) {
-          t_drop = cache_load<K>(p, g, sm);
-          ++cnt.replays;
-        }
+      // lanes whose query the forward stored replay it; the others traverse
+      const bool rep = replay && active && (first || cache_has<K>(p, next, cur.key_min));
+      const bool trav = active && !rep;
+      if (__any_sync(full, trav))
+        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+      if (rep) {
+        t_drop = cache_get<K>(p, first, g, next, sm, next);
+        ++cnt.replays;
       } else {
-        packet_query<K>(p.bvh, r, active, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
-        if (first && active && p.cache_mode == kCacheWrite) cache_store<K>(p, g, sm, t_drop);
+        next = kNoEntry;
+      }
+      if (p.cache_mode == kCacheWrite) {
+        if (first) {
+          if (trav) link = cache_put_first<K>(p, g, sm, t_drop);
+        } else {
+          const bool more = trav && link != nullptr;
+          const uint32_t e = cache_alloc(p, more);
+          if (more) link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
+        }
       }
       if (active) {
         bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);

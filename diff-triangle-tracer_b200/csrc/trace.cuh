@@ -25,24 +25,35 @@ struct ViewDesc {
   long long ray_begin;    // hit cache index of the view's pixel 0 (views laid out one after another)
 };
 
-// Hit cache: every ray's first k-closest query as the forward found it, so
-// the adjoint replays it instead of traversing again (the query's result
+// Hit cache: the k-closest queries of every ray as the forward found them,
+// so the adjoint replays them instead of traversing again (a query's result
 // depends only on the ray, the BVH and the key range, all unchanged). A
-// 32-byte header, then k + 1 rows of `rays` 64-bit words: rows 0..k-1 the
-// sorted keys, row k the trusted bound t_drop (float bits). The adjoint uses
-// it only if the header's k, ray count and BVH generation are its own.
+// 32-byte header; then the main part, k + 1 rows of `rays` 64-bit words with
+// each ray's first query: rows 0..k-1 the sorted keys, row k the trusted
+// bound t_drop (float bits, low half) and the pool entry of the ray's next
+// query (high half, kNoEntry if none); then the pool, k + 2 rows of
+// `pool_cap` words: later queries laid out the same way plus row k + 1, the
+// query's lower key. The adjoint uses the cache only if the header's k, ray
+// count, pool size and BVH generation are its own, and a pool entry only if
+// its lower key is the one its own march asks for.
 struct HitCacheHeader {
   uint32_t magic;
   uint32_t k;
   long long rays;
   unsigned long long gen;  // BVH builds + refits of the handle when the forward ran
-  unsigned long long pad;
+  uint32_t pool_cap;       // pool entries
+  uint32_t pool_used;      // entries handed out (may pass pool_cap: the rest were not stored)
 };
 constexpr uint32_t kHitCacheMagic = 0x43485454u;  // "TTHC"
-constexpr int kCacheOff = 0, kCacheWrite = 1, kCacheRead = 2;
-__host__ __device__ inline size_t hit_cache_bytes(int k, long long rays) {
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
+__host__ __device__ inline size_t hit_cache_main_bytes(int k, long long rays) {
   return sizeof(HitCacheHeader) + (size_t)(k + 1) * 8 * (size_t)rays;
 }
+// default pool: later queries of a quarter of the rays
+__host__ __device__ inline size_t hit_cache_bytes(int k, long long rays) {
+  return hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)((rays + 3) / 4);
+}
+constexpr int kCacheOff = 0, kCacheWrite = 1, kCacheRead = 2;
 
 // Secondary-ray passes: one record per ray of each pixel's ray tree
 // (64 bytes). Level 0 holds the primary rays (record i = pixel i of view 0;
@@ -114,6 +125,7 @@ struct TraceParams {
   int cache_mode;             // kCache*
   long long cache_rays;       // rays of all views of the launch
   unsigned long long cache_gen;
+  uint32_t cache_pool_cap;    // pool entries the buffer holds
 };
 
 struct HitStreamParams {

@@ -159,7 +159,7 @@ class OptixTracer:
         `k` hits (k = 32 fits every configuration). No reference counterpart."""
         n = lib.tt_hit_cache_bytes(self._h, int(rays))
         if k is not None:
-            n = max(n, 32 + (int(k) + 1) * 8 * int(rays))
+            n = max(n, 32 + (int(k) + 1) * 8 * int(rays) + (int(k) + 2) * 8 * ((int(rays) + 3) // 4))
         return torch.empty((n,), dtype=torch.uint8, device=self.device)
 
     def trace_forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,

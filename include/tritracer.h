@@ -112,11 +112,14 @@ typedef struct tt_fwd_args {
   float* max_blending;   /* [P], zeroed then written */
   float* gpu_time_ms;    /* host pointer, may be NULL */
   /* Optional hit cache (plain program; NULL = none; no reference counterpart):
-   * device memory of at least tt_hit_cache_bytes(h, rays) bytes, 16-byte
-   * aligned, rays = H * W (the sum over the views of a batched call). The
-   * forward stores every ray's first k-closest query in it; a tt_backward
-   * given the same cache replays those queries instead of traversing the BVH
-   * again. tt_forward_noalloc ignores it. */
+   * 16-byte aligned device memory, rays = H * W (the sum over the views of a
+   * batched call). The forward stores every ray's k-closest queries in it:
+   * the first ones in a main part of 32 + (k + 1) * 8 * rays bytes (the
+   * minimum size), later ones in a pool filling the rest, (k + 2) * 8 bytes a
+   * query, while it lasts. tt_hit_cache_bytes(h, rays) sizes the pool for a
+   * quarter of the rays. A tt_backward given the same cache replays the
+   * stored queries instead of traversing the BVH again. tt_forward_noalloc
+   * ignores it. */
   void* hit_cache;
   size_t hit_cache_bytes;
 } tt_fwd_args;
@@ -151,9 +154,10 @@ typedef struct tt_bwd_args {
   float* gpu_time_ms;  /* host pointer, may be NULL */
   const float* colors_precomp; /* [P][3]: the forward's precomputed colours (shs NULL), or NULL */
   float* dL_dcolors;           /* [P][3] gradient of colors_precomp (zeroed, then accumulated) */
-  /* Optional: the hit cache the forward of these rays filled (NULL = re-trace).
-   * It is only replayed if it was written with the handle's current k and ray
-   * count, and no build, refit or load of the BVH happened since; otherwise
+  /* Optional: the hit cache the forward of these rays filled (NULL = re-trace),
+   * with the size it had there. It is only replayed if it was written with the
+   * handle's current k and ray count, and no build, refit or load of the BVH
+   * happened since; otherwise, and for queries the forward could not store,
    * the adjoint traverses as without it. The results are the same either way:
    * a replayed query is the one the adjoint would compute. */
   const void* hit_cache;
@@ -224,8 +228,9 @@ int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, 
 int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
 
 /* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the
- * handle's current traversal configuration: 32 + (k + 1) * 8 * rays. No
- * reference counterpart. */
+ * handle's current traversal configuration, with a pool for later queries of
+ * a quarter of the rays: 32 + (k + 1) * 8 * rays + (k + 2) * 8 * ceil(rays / 4).
+ * No reference counterpart. */
 size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays);
 
 /* Message of the last failed call on this handle (never NULL). */
