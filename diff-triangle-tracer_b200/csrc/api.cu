@@ -23,6 +23,8 @@ struct tt_tracer {
   tt::DevBuf scratch;  // int[0] tile counter, int[1] status word, u64 stats[kNumStats] from byte 16,
                        // int[3] secondary-ray queue counters from byte kSecCountOffset
   tt::DevBuf sec_rec;  // secondary-ray queue: R * (2^(depth+1) - 1) records
+  tt::DevBuf sec_cache;        // hit cache of that ray tree (tt_forward_secondary writes, the adjoint replays)
+  size_t sec_cache_bytes = 0;  // its size for the last tree
   int sec_R = 0, sec_depth = -1;  // the ray tree the last tt_forward_secondary left
   int sec_trace_grid = 0, sec_bwd_grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -169,6 +171,7 @@ int tt_destroy(tt_tracer* h) {
   h->bvh.release();
   h->scratch.release();
   h->sec_rec.release();
+  h->sec_cache.release();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   delete h;
@@ -679,6 +682,18 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
   rc = accel_step(h, a->vertices, a->num_vertices, a->cumsum, a->P, a->rebuild_gas, s);
   if (rc != TT_OK) return rc;
   TT_CUDA(h, h->sec_rec.reserve((size_t)nrec * sizeof(tt::SecRecord)));
+  // hit cache of the ray tree: each pixel's primary ray in the main part,
+  // spawned rays and later queries in a pool of two entries per pixel
+  const size_t cache_bytes =
+      tt::hit_cache_main_bytes(tt::kChunk, R) + (size_t)(tt::kChunk + 2) * 8 * (size_t)(2 * R);
+  h->sec_cache_bytes = 0;
+  TT_CUDA(h, h->sec_cache.reserve(cache_bytes));
+  h->sec_cache_bytes = cache_bytes;
+  p.hit_cache = h->sec_cache.p;
+  p.cache_mode = tt::kCacheWrite;
+  p.cache_gen = h->bvh_gen;
+  p.cache_pool_cap = (uint32_t)cache_pool_cap(tt::kChunk, R, cache_bytes);
+  TT_CUDA(h, cudaMemsetAsync(h->sec_cache.p, 0, sizeof(tt::HitCacheHeader), s));
   p.bvh = h->bvh.view();
   p.verts = a->vertices;
   p.cumsum = a->cumsum;
@@ -790,6 +805,12 @@ int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary
   p.d_sh = a->dL_dsh;
   int* count = reinterpret_cast<int*>(h->scratch.as<char>() + kSecCountOffset);
   sec_layout(p.sec, sec, h->sec_rec.as<tt::SecRecord>(), h->sec_R, count);
+  if (h->sec_cache_bytes > 0) {  // replayed where its header matches (same BVH generation)
+    p.hit_cache = h->sec_cache.p;
+    p.cache_mode = tt::kCacheRead;
+    p.cache_gen = h->bvh_gen;
+    p.cache_pool_cap = (uint32_t)cache_pool_cap(tt::kChunk, p.cache_rays, h->sec_cache_bytes);
+  }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
   TT_CUDA(h, tt::launch_sec_backward(p, h->sec_bwd_grid, s));

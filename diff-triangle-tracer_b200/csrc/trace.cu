@@ -1675,6 +1675,9 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
   bool have = false, exhausted = false;
   Cursor cur = first_cursor(p.tmin_inclusive);
   float3 o = make_float3(0.f, 0.f, 0.f), d = o;
+  uint32_t* link = nullptr;  // forward: where the entry of the ray's next query gets linked
+  uint32_t next = kNoEntry;  // adjoint: entry of the ray's next query
+  const bool replay = cache_replays<K>(p);
   for (;;) {
     const unsigned need = __ballot_sync(full, !have && !exhausted);
     if (need) {
@@ -1699,11 +1702,35 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
     }
     float t_drop = INFINITY;
     if (have) {
-      const RayW r = make_ray(o, d);
-      unsigned long long kb[kChunk];
-      query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
+      // Hit cache: a level-0 ray (record = pixel) keeps its first query in
+      // the main part; a deeper ray starts its chain in the pool, linked from
+      // its queue record
+      const bool first = cur.chunks == 0;
+      const bool main_part = first && sh.ridx < p.cache_rays;
+      uint32_t* rec_link = &p.sec.rec[sh.ridx].cache_link;
+      if (replay && first && !main_part) next = __ldcg(rec_link);
+      if (replay && (main_part || cache_has<K>(p, next, cur.key_min))) {
+        t_drop = cache_get<K>(p, main_part, sh.ridx, next, sm, next);
+        ++cnt.replays;
+      } else {
+        next = kNoEntry;
+        const RayW r = make_ray(o, d);
+        unsigned long long kb[kChunk];
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
 #pragma unroll
-      for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        if (p.cache_mode == kCacheWrite) {
+          if (main_part) {
+            link = cache_put_first<K>(p, sh.ridx, sm, t_drop);
+          } else {
+            if (first) link = rec_link;
+            if (link) {
+              const uint32_t e = atomicAdd(&cache_header_ptr(p)->pool_used, 1u);
+              link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
+            }
+          }
+        }
+      }
     }
     __syncwarp();
     if (have) {
@@ -1870,6 +1897,7 @@ struct SecShader {
     c->d[2] = cd.z;
     c->pixel = pix;
     c->tau = ctau;
+    c->cache_link = kNoEntry;
     return slot;
   }
 
@@ -1938,6 +1966,7 @@ __device__ __forceinline__ int sec_level_size(const TraceParams& p, int level) {
 }
 
 __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_trace(const __grid_constant__ TraceParams p) {
+  if (p.sec.level == 0) cache_header<kChunk>(p);  // the deeper levels append to the same cache
   Counters cnt;
   SecShader sh(p);
   drive_items<32>(p, thread_smem<32>(), sh, cnt, sec_level_size(p, p.sec.level));
@@ -2144,6 +2173,8 @@ __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_backward(const __grid_
   int total = 0;
   for (int l = 0; l <= p.sec.max_depth; ++l) total += sec_level_size(p, l);
   drive_items<32>(p, thread_smem<32>(), sh, cnt, total);
+  const unsigned s = __reduce_add_sync(0xFFFFFFFFu, cnt.replays);
+  if ((threadIdx.x & 31) == 0 && s != 0u) atomicAdd(p.stats + kStatReplays, (unsigned long long)s);
 }
 
 // ---------------------------------------------------------------- hit stream

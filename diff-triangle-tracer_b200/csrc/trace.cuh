@@ -68,7 +68,7 @@ struct SecRecord {
   float F;     // Fresnel share of the reflected child
   float w;     // blending weight of the spawning hit
   int child_r, child_t;  // records of the children in the next level, or -1
-  int pad;
+  uint32_t cache_link;   // hit cache: pool entry of the ray's first query (levels >= 1), or kNoEntry
 };
 
 constexpr int kMaxSecDepth = 2;

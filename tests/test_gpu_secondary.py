@@ -122,3 +122,39 @@ def test_autograd_module_and_state(setup):
                                     T(sc.cumsum), color.detach(), others, sc.P, T(sc.shs), 3, T(sc.opacities),
                                     torch.zeros_like(color), torch.zeros_like(others), T(sec["material"]),
                                     T(sec["ior"]), T(sec["env"]), 2)
+
+
+def test_adjoint_replays_the_ray_tree_queries(setup):
+    """The forward stores the queries of every ray of the tree (primary rays
+    in the hit cache's main part, spawned rays in its pool); the adjoint
+    replays them, and gives the gradients of an adjoint that re-traverses
+    (forced by a refit between the passes, which invalidates the cache)."""
+    sc, ro, rd, sec = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    g, go = scenes.upstream_grads(H, W, seed=12, others_std=1.0)
+    tr.reset_stats()
+    fwd = gpu_secondary(tr, sc, ro, rd, sec)
+    st = tr.stats()
+    rays, queries = st["rays"], st["queries"]
+    assert rays > H * W * 1.5 and queries > rays
+
+    def adjoint():
+        tr.reset_stats()
+        gr = tr.trace_backward_secondary(
+            T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), T(fwd["color"]),
+            T(fwd["others"]), sc.P, T(sc.shs), 3, T(sc.opacities), T(g), T(go), T(sec["material"]), T(sec["ior"]),
+            T(sec["env"]), 2)
+        torch.cuda.synchronize()
+        tr.device_status()
+        return [x.cpu().numpy() for x in gr], tr.stats()["hit_cache_replays"]
+
+    replayed, n = adjoint()
+    print(f"pixels {H * W}, rays {rays}, queries {queries}, replayed {n}")
+    assert H * W < n <= queries  # primary queries and spawned rays' queries
+    if queries - H * W <= 2 * H * W:  # the pool (two entries per pixel) held every one
+        assert n == queries
+    tr.build_tri_accel(T(sc.verts.reshape(-1)), T(sc.cumsum), sc.P, False)  # same vertices, new generation
+    traced, n0 = adjoint()
+    assert n0 == 0
+    for x, y, name in zip(replayed, traced, ("dtri", "dsigma", "dopac", "dsh")):
+        assert rel_norm(x, y) < 1e-6, name
