@@ -105,14 +105,17 @@ class OptixTracer:
         if rc != _lib.TT_OK:
             raise _lib.TracerError(rc, f"OptixTracer construction failed (tt_create returned {rc})")
         self._h = h
+        self._destroy = lib.tt_destroy
         self._keep = ()
         self._proposal = None
         self._proposal_args = (None, None, None)
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            lib.tt_destroy(h)
+        # the bound function, not the module global: at interpreter exit the
+        # module's globals may already be cleared when this runs
+        h, destroy = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and destroy is not None:
+            destroy(h)
             self._h = None
 
     # ------------------------------------------------------------------
