@@ -251,7 +251,7 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
 
     def fwd_bwd(intervals, records=None):
         z1, z2 = torch.zeros(sc.P, device=dev), torch.zeros(sc.P, device=dev)
-        cache = tr.new_hit_cache(R)  # both arms replay the first query in the adjoint
+        cache = tr.new_hit_cache(R)  # both arms replay the forward's queries in the adjoint
         outs, _ = tr.trace_forward_views(held, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"], 3,
                                          S["opac"], z1, z2, bg, 2, intervals=intervals, records=records,
                                          hit_cache=cache)

@@ -171,7 +171,7 @@ class OptixTracer:
         """tracer.cpp:16-142: returns FwdTraceResult((color [3,H,W], others [7,H,W],
         gpu_time [1], scaling, density_factor, max_blending [P])). With
         `hit_cache` (a new_hit_cache(H * W) buffer) the forward also stores every
-        ray's first query there for trace_backward."""
+        ray's k-closest queries there for trace_backward."""
         dev = self.device
         P = int(number_of_points)
         ro = _f32(ray_o, "ray_o", dev)

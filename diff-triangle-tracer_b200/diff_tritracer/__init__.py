@@ -122,10 +122,11 @@ class Tracer(nn.Module):
 
     def __init__(self, forwad_ptx="forward.ptx", backward_ptx="backward.ptx", tmin_inclusive: bool = True,
                  exact_adjoint: bool = False, hit_cache: bool = True) -> None:
-        """hit_cache (no reference counterpart): the forward keeps every ray's
-        first k-closest query in a device buffer held by the autograd graph
-        ((k + 1) * 8 bytes a ray) and the backward replays it instead of
-        traversing the BVH again; the gradients are the same either way."""
+        """hit_cache (no reference counterpart): the forward keeps its
+        k-closest queries in a device buffer held by the autograd graph ((k + 1)
+        * 8 bytes a ray for the first ones, plus a pool of a quarter of that for
+        later ones) and the backward replays them instead of traversing the BVH
+        again; the gradients are the same either way."""
         super().__init__()
         self.tracer = _C.OptixTracer("", forwad_ptx, backward_ptx, tmin_inclusive=tmin_inclusive,
                                      exact_adjoint=exact_adjoint)

@@ -5,8 +5,8 @@ through ONE persistent forward launch and ONE adjoint launch per step
 (tt_forward_views / tt_backward_views). With `graph=True` the step - BVH refit
 to the current vertices, forward, adjoint - is recorded once into a CUDA graph
 and replayed, so a training step costs one graph launch on the host. With
-`hit_cache=True` the forward keeps every ray's first query in a static buffer
-and the adjoint replays it instead of traversing again. Rays and
+`hit_cache=True` the forward keeps its k-closest queries in a static buffer
+and the adjoint replays them instead of traversing again. Rays and
 upstream gradients are copied into the batch's static buffers before replay;
 the scene tensors must keep their storage between steps (optimisers update
 them in place).
