@@ -292,25 +292,6 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     __syncwarp();
     if (m == 0) continue;
     const bool on = (m >> lane) & 1u;
-    if (ref_is_leaf(ref)) {
-      const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
-      if (on) cnt.tris += ntri;
-      with_perm(wperm, r, [&](const auto& pm) {
-        for (uint32_t j = 0; j < ntri; ++j) {
-          const float4* tr = bvh.tris + 3 * (size_t)(first + j);
-          const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
-          float t;
-          if (!on || !isect_tri_p(r, pm, a, b, c, t)) continue;
-          if (!(t >= t_lo) || !(t <= tmax)) continue;
-          const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-          if (key >= key_min && key < kb_last) {
-            kb_insert_smem<K>(kb, kstride, key, kb_last);
-            if (kb_last != kEmptyKey) tmax = key_t(kb_last);
-          }
-        }
-      });
-      continue;
-    }
     if (on) ++cnt.nodes;
     if (lane == 0) ++cnt.warp_nodes;
     const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
@@ -332,22 +313,46 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
         mine = __uint_as_float(cmin);
       }
     }
-    const unsigned hm = __ballot_sync(full, mymask != 0u);  // bit c: some lane enters child c
-    if (hm == 0u) continue;
-    const int nh = __popc(hm);
+    // Leaf children are tested right away by the lanes that entered them (a
+    // push and a pop saved per leaf); only interior children go on the stack.
+    const bool my_leaf = mymask != 0u && ref_is_leaf(my_ref);
+    for (unsigned lb = __ballot_sync(full, my_leaf); lb != 0u; lb &= lb - 1u) {
+      const int lc = __ffs(lb) - 1;
+      const uint32_t lref = __shfl_sync(full, my_ref, lc);
+      const bool lon = (__shfl_sync(full, mymask, lc) >> lane) & 1u;
+      const uint32_t first = leaf_first(lref), ntri = leaf_count(lref);
+      if (lon) cnt.tris += ntri;
+      with_perm(wperm, r, [&](const auto& pm) {
+        for (uint32_t j = 0; j < ntri; ++j) {
+          const float4* tr = bvh.tris + 3 * (size_t)(first + j);
+          const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+          float t;
+          if (!lon || !isect_tri_p(r, pm, a, b, c, t)) continue;
+          if (!(t >= t_lo) || !(t <= tmax)) continue;
+          const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
+          if (key >= key_min && key < kb_last) {
+            kb_insert_smem<K>(kb, kstride, key, kb_last);
+            if (kb_last != kEmptyKey) tmax = key_t(kb_last);
+          }
+        }
+      });
+    }
+    const unsigned pmask = my_leaf ? 0u : mymask;  // lane c: lanes entering interior child c
+    const int nh = __popc(__ballot_sync(full, pmask != 0u));
+    if (nh == 0) continue;
     // rank among the entered children by entry distance: distances are >= 0,
     // so their bit patterns order like the values; the low 3 bits make room
     // for the slot (near-ties go by slot, which only affects the visit order)
-    const unsigned key = mymask != 0u ? ((__float_as_uint(mine) & ~7u) | (unsigned)lane) : 0xFFFFFFFFu;
+    const unsigned key = pmask != 0u ? ((__float_as_uint(mine) & ~7u) | (unsigned)lane) : 0xFFFFFFFFu;
     int rank = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) rank += __shfl_sync(full, key, c) < key ? 1 : 0;
     const int avail = kWarpStack - sp;
     const int npush = nh < avail ? nh : avail;
-    if (mymask != 0u && rank < npush) {
+    if (pmask != 0u && rank < npush) {
       const int pos = sp + npush - 1 - rank;  // nearest on top
       ws.ref[pos] = my_ref;
-      ws.mask[pos] = mymask;
+      ws.mask[pos] = pmask;
       ws.tmin[pos] = mine;
     }
     if (nh > avail) {
@@ -355,7 +360,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
       // keys nearer than the dropped entry distance
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        const unsigned m = __shfl_sync(full, mymask, c);
+        const unsigned m = __shfl_sync(full, pmask, c);
         const float e = __shfl_sync(full, mine, c);
         const int rk = __shfl_sync(full, rank, c);
         if (m != 0u && rk >= npush && ((m >> lane) & 1u)) t_drop = fminf(t_drop, e);
