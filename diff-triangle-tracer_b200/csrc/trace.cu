@@ -222,9 +222,11 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
 // lanes whose ray hit its box and the smallest entry distance among them.
 // Every active lane tests its own ray (its own [t_lo, tmax] interval and
 // k-buffer) against the 8 children; ballots give each child's lane mask and
-// __reduce_min_sync its nearest entry distance; hit children are ranked
-// lane-parallel (lane c ranks child c) and pushed far-to-near. Control flow
-// is warp-uniform, so SIMT efficiency equals the fraction of lanes whose ray
+// __reduce_min_sync its nearest entry distance; the triangles of hit leaf
+// children are tested at once by the lanes that entered them, and hit
+// interior children are ranked lane-parallel (lane c ranks child c) and
+// pushed far-to-near, so the stack holds interior nodes only. Control flow is
+// warp-uniform, so SIMT efficiency equals the fraction of lanes whose ray
 // still needs the node, and every node/triangle record is read once per warp.
 constexpr int kWarpStack = 192;
 

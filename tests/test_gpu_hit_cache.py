@@ -170,3 +170,18 @@ def test_small_cache_rejected(setup):
     small = torch.empty(32 + 17 * 8 * H * W - 8, dtype=torch.uint8, device=DEV)
     with pytest.raises(RuntimeError, match="hit_cache"):
         forward(tr, sc, s, ro, rd, small)
+
+
+def test_misaligned_cache_and_variant_program_rejected(setup):
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    buf = tr.new_hit_cache(H * W + 8)
+    with pytest.raises(RuntimeError, match="16-byte aligned"):
+        forward(tr, sc, s, ro, rd, buf[8:])  # the storage is aligned, this view is not
+    var = _C.OptixTracer("", "reflect.ptx", "backward.ptx")
+    st = settings(rebuild=0, extra=[0.3, 0.0, 0.0, 0.0, 0.0])
+    with pytest.raises(RuntimeError, match="plain program"):
+        var.trace_forward(ro, rd, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3,
+                          torch.empty(0, device=DEV), s["opac"], torch.zeros(sc.P, device=DEV),
+                          torch.zeros(sc.P, device=DEV), st.bg, st.extra_params, st.rebuild_gas, False,
+                          hit_cache=var.new_hit_cache(H * W))
