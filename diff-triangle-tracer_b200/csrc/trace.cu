@@ -228,7 +228,9 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
 // pushed far-to-near, so the stack holds interior nodes only. Control flow is
 // warp-uniform, so SIMT efficiency equals the fraction of lanes whose ray
 // still needs the node, and every node/triangle record is read once per warp.
-constexpr int kWarpStack = 192;
+// Interior nodes only (leaf children are tested at their parent's visit):
+// a BVH8 of depth d needs at most ~7d entries.
+constexpr int kWarpStack = 96;
 
 struct WarpStack {
   uint32_t* ref;
