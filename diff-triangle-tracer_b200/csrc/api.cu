@@ -26,7 +26,7 @@ struct tt_tracer {
   tt::DevBuf sec_cache;        // hit cache of that ray tree (tt_forward_secondary writes, the adjoint replays)
   size_t sec_cache_bytes = 0;  // its size for the last tree
   int sec_R = 0, sec_depth = -1;  // the ray tree the last tt_forward_secondary left
-  int sec_trace_grid = 0, sec_bwd_grid = 0;
+  int sec_trace_grid = 0, sec_bwd_grid = 0, sec_primary_grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
@@ -128,6 +128,7 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
   }
   h->sec_trace_grid = h->num_sms * tt::sec_blocks_per_sm(0);
+  h->sec_primary_grid = h->num_sms * tt::sec_blocks_per_sm(2);
   h->sec_bwd_grid = h->num_sms * tt::sec_blocks_per_sm(1);
   if (tt_set_traversal(h, h->cfg.traversal, h->cfg.k, h->cfg.stack_depth) != TT_OK) {
     delete h;
@@ -716,7 +717,8 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
   for (int level = 0; level <= sec->max_depth; ++level) {
     p.sec.level = level;
     TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
-    TT_CUDA(h, tt::launch_sec_trace(p, h->sec_trace_grid, s));
+    TT_CUDA(h, level == 0 ? tt::launch_sec_primary(p, h->sec_primary_grid, s)
+                          : tt::launch_sec_trace(p, h->sec_trace_grid, s));
     ++h->trace_launches;
   }
   for (int level = sec->max_depth; level >= 0; --level) {

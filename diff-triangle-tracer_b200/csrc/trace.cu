@@ -1888,6 +1888,13 @@ struct SecShader {
     ++n_rays;
   }
 
+  // The packet driver's entry (level 0): the primary ray of `pixel`.
+  __device__ __forceinline__ bool begin(const ViewDesc*, int pixel, float3, float3) {
+    float3 ro, rd;
+    begin_item(pixel, ro, rd);
+    return true;
+  }
+
   __device__ __forceinline__ void prepare() {}
 
   __device__ __forceinline__ int push_child(float3 co, float3 cd, float ctau) {
@@ -1974,8 +1981,21 @@ __device__ __forceinline__ int sec_level_size(const TraceParams& p, int level) {
   return level == 0 ? p.views[0].H * p.views[0].W : min(__ldcg(p.sec.count + level), p.sec.cap[level]);
 }
 
+// Level 0: the primary rays are camera-coherent, so they are traced as warp
+// packets of 8x4 pixels (with the hit cache's 16 hits per query), in a kernel
+// of their own (the lane driver's registers would spill in the same kernel).
+__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_sec_primary(const __grid_constant__ TraceParams p) {
+  cache_header<kChunk>(p);  // the deeper levels append to the same cache
+  Counters cnt;
+  SecShader sh(p);
+  unsigned char* rest;
+  const Smem sm = packet_smem<kChunk>(rest);
+  drive_packets<kChunk>(p, sm, warp_stack(rest), sh, cnt);
+  add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
+}
+
+// Levels >= 1: spawned rays, incoherent: one ray per lane.
 __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_trace(const __grid_constant__ TraceParams p) {
-  if (p.sec.level == 0) cache_header<kChunk>(p);  // the deeper levels append to the same cache
   Counters cnt;
   SecShader sh(p);
   drive_items<32>(p, thread_smem<32>(), sh, cnt, sec_level_size(p, p.sec.level));
@@ -2295,15 +2315,20 @@ cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
 
 int sec_blocks_per_sm(int which) {
   int n = 0;
-  const void* fn = which == 0 ? (const void*)k_sec_trace : (const void*)k_sec_backward;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem_bytes_for<kCfgLanes32>()) !=
-      cudaSuccess)
-    n = 1;
+  const void* fn = which == 0 ? (const void*)k_sec_trace
+                              : (which == 1 ? (const void*)k_sec_backward : (const void*)k_sec_primary);
+  const size_t smem = which == 2 ? smem_bytes_for<kCfgPackets16>() : smem_bytes_for<kCfgLanes32>();
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem) != cudaSuccess) n = 1;
   return n > 0 ? n : 1;
 }
 
 cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s) {
   k_sec_trace<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sec_primary(const TraceParams& p, int grid, cudaStream_t s) {
+  k_sec_primary<<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p);
   return cudaGetLastError();
 }
 

@@ -163,8 +163,9 @@ cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);
 // Secondary-ray passes (views[0] only): trace level p.sec.level, resolve it,
 // or run the adjoint of every ray of every level.
-int sec_blocks_per_sm(int which /*0 trace, 1 adjoint*/);
+int sec_blocks_per_sm(int which /*0 trace (levels >= 1), 1 adjoint, 2 primary level*/);
 cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s);
+cudaError_t launch_sec_primary(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s);
 cudaError_t launch_sec_backward(const TraceParams& p, int grid, cudaStream_t s);
 
