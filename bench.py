@@ -175,6 +175,20 @@ def cpu_baseline(name, sc, ro, rd, g, go, budget_s=12.0):
                       f"CPU BVH build {build_s:.1f} s untimed"}, runner, kind, nthreads, rows
 
 
+def slowest_rank_ms(ms, world, dev):
+    """Device time of the timed region on the slowest rank. Every rank calls
+    this with its own CUDA-event time, at the same point: it is the only
+    collective of the replicas, which share no data."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(ms)], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
@@ -434,10 +448,8 @@ def run_views(args, world, rank, local, dev):
     clocks = sampler.stop()
     ms = t0.elapsed_time(t1)
     st = tr.stats()
+    ms = slowest_rank_ms(ms, world, dev)
     if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
         dist.destroy_process_group()
     if rank != 0:
         return
@@ -471,7 +483,7 @@ def main():
     ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
     ap.add_argument("--no-hit-cache", action="store_true",
-                    help="adjoint re-traverses every query instead of replaying the forward's first one")
+                    help="adjoint re-traverses every query instead of replaying the forward's")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
                     help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
@@ -578,10 +590,7 @@ def main():
     elapsed_ms = t0.elapsed_time(t1)
     st = tr.stats()
     tr.device_status()
-    if world > 1:
-        tt = torch.tensor([elapsed_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tt.item())
+    elapsed_ms = slowest_rank_ms(elapsed_ms, world, dev)
     ms_per_step = elapsed_ms / args.steps
     value = world * R * args.steps / (elapsed_ms / 1e3) / 1e6
 
@@ -670,10 +679,7 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = slowest_rank_ms(e2e_ms, world, dev)
     e2e_value = world * R * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     h2d = ro_h.numel() * 4 + rd_h.numel() * 4 + g_h.numel() * 4
     d2h = color_h.numel() * 4
