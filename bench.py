@@ -91,6 +91,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = 0
 
     def start(self):
         try:
@@ -99,6 +100,12 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: have it sampling before the
+            # timed region begins, so that short regions still get samples
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.first = len(self.lines)
         except Exception:
             self.proc = None
 
@@ -109,6 +116,10 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return None
+        # a region shorter than the sampling period: the next sample, taken as it ends
+        t0 = time.time()
+        while len(self.lines) <= self.first and time.time() - t0 < 0.5 and self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -117,7 +128,7 @@ class ClockSampler:
         time.sleep(0.05)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 7:
                 continue
