@@ -31,7 +31,9 @@ constexpr int kMaxSteps = 1 << 24;    // bound on stack pops per query
 // Resident blocks per SM the register budget must allow: 4 x 128 threads
 // leave 128 registers a thread. Measured on 1M triangles, 4 x 800^2 rays,
 // packets of 32: forward 19.0 / adjoint 21.6 ms at 4 blocks, 20.5 / 23.2 at
-// 5 (96 registers, ~300 bytes of spills a thread), 21.8 / 24.9 at 6.
+// 5 (96 registers, ~300 bytes of spills a thread), 21.8 / 24.9 at 6; later,
+// with the forward at 18.2 ms at 4 blocks, 19.9 at 3 (168 registers, no
+// spills, 12 warps per SM).
 #ifndef TT_MIN_BLOCKS
 #define TT_MIN_BLOCKS 4
 #endif
