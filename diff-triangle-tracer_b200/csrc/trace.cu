@@ -9,8 +9,9 @@
 //    the image is done, so rays of very different depth complexity balance;
 //  * one ray per thread; the traversal stack (node reference + entry distance)
 //    lives in shared memory, strided by the block size (no bank conflicts);
-//  * k-buffer: 16 (t, primitive) pairs packed as 64-bit keys in registers,
-//    inserted by a branch-free compare-exchange chain;
+//  * k-buffer: the k nearest (t, primitive) pairs packed as 64-bit keys, kept
+//    sorted in shared memory (one column per lane) by insertion, the largest
+//    mirrored in a register;
 //  * the chunked march of the reference is reproduced exactly on top of the
 //    key stream: after every 16th visited hit the next query starts AT the
 //    last hit's t (closed interval, optixTrace) or strictly after it;
@@ -53,15 +54,23 @@ struct Stack {
   }
 };
 
-__device__ __forceinline__ void kb_insert(unsigned long long (&kb)[kChunk], unsigned long long key) {
-#pragma unroll
-  for (int i = 0; i < kChunk; ++i) {
-    const unsigned long long cur = kb[i];
-    const bool lt = key < cur;
-    kb[i] = lt ? key : cur;
-    key = lt ? cur : key;
+// Sorted insert into the lane's k-buffer in shared memory (hits are rare
+// next to box tests, so the buffer need not occupy 32 registers); kb_last
+// mirrors the largest key.
+template <int K>
+__device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key,
+                                               unsigned long long& kb_last) {
+  int i = K - 1;
+  while (i > 0) {
+    const unsigned long long prev = kb[(i - 1) * stride];
+    if (prev <= key) break;
+    kb[i * stride] = prev;
+    --i;
   }
+  kb[i * stride] = key;
+  kb_last = kb[(K - 1) * stride];
 }
+
 
 struct Counters {
   unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
@@ -128,11 +137,12 @@ __device__ __forceinline__ void slab8(const float4* __restrict__ nd, int nx, int
 // pass. Hit children are pushed in slot order with the nearest one on top.
 template <int SD>
 __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min, float t_hi,
-                                      unsigned long long (&kb)[kChunk], Stack st, float& t_drop, int* status,
+                                      unsigned long long* kb, int kstride, Stack st, float& t_drop, int* status,
                                       Counters& cnt) {
   ++cnt.queries;
 #pragma unroll
-  for (int i = 0; i < kChunk; ++i) kb[i] = kEmptyKey;
+  for (int i = 0; i < kChunk; ++i) kb[i * kstride] = kEmptyKey;
+  unsigned long long kb_last = kEmptyKey;
   t_drop = INFINITY;
   if (!bvh.has_root) return;
   const float t_lo = key_t(key_min);
@@ -171,9 +181,9 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
         if (!isect_tri(r, a, b, c, t)) continue;
         if (!(t >= t_lo) || !(t <= tmax)) continue;
         const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-        if (key >= key_min && key < kb[kChunk - 1]) {
-          kb_insert(kb, key);
-          if (kb[kChunk - 1] != kEmptyKey) tmax = key_t(kb[kChunk - 1]);
+        if (key >= key_min && key < kb_last) {
+          kb_insert_smem<kChunk>(kb, kstride, key, kb_last);
+          if (kb_last != kEmptyKey) tmax = key_t(kb_last);
         }
       }
       continue;
@@ -239,23 +249,6 @@ struct WarpStack {
   unsigned* mask;
   float* tmin;
 };
-
-// Sorted insert into the lane's k-buffer in shared memory (hits are rare
-// next to box tests, so the buffer need not occupy 32 registers); kb_last
-// mirrors the largest key.
-template <int K>
-__device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key,
-                                               unsigned long long& kb_last) {
-  int i = K - 1;
-  while (i > 0) {
-    const unsigned long long prev = kb[(i - 1) * stride];
-    if (prev <= key) break;
-    kb[i * stride] = prev;
-    --i;
-  }
-  kb[i * stride] = key;
-  kb_last = kb[(K - 1) * stride];
-}
 
 template <int K>
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
@@ -803,7 +796,7 @@ __device__ __forceinline__ void cache_header(const TraceParams& p) {
 // whose ray finished are refilled instead of idling.
 template <int SD, class Shader>
 __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shader& sh, Counters& cnt) {
-  constexpr int K = kChunk;  // per-lane k-buffers live in registers
+  constexpr int K = kChunk;  // hits per per-lane query
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -859,10 +852,7 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
-        unsigned long long kb[kChunk];
-        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
-#pragma unroll
-        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
         if (p.cache_mode == kCacheWrite) {
           if (first) {
             link = cache_put_first<K>(p, g, sm, t_drop);
@@ -1726,10 +1716,7 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
-        unsigned long long kb[kChunk];
-        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, kb, sm.st, t_drop, p.status, cnt);
-#pragma unroll
-        for (int i = 0; i < kChunk; ++i) sm.keys[i * sm.stride] = kb[i];
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
         if (p.cache_mode == kCacheWrite) {
           if (main_part) {
             link = cache_put_first<K>(p, sh.ridx, sm, t_drop);
@@ -2210,24 +2197,23 @@ __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_backward(const __grid_
 
 // ---------------------------------------------------------------- hit stream
 __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p) {
-  const Stack st = thread_smem<kStackDepth>().st;
+  const Smem sm = thread_smem<kStackDepth>();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.R) return;
   const float3 o = make_float3(p.ray_o[3 * i], p.ray_o[3 * i + 1], p.ray_o[3 * i + 2]);
   const float3 d = make_float3(p.ray_d[3 * i], p.ray_d[3 * i + 1], p.ray_d[3 * i + 2]);
   const RayW r = make_ray(o, d);
   unsigned long long key_min = 0ull;
-  unsigned long long kb[kChunk];
   int count = 0;
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
     Counters cnt;
-    query<kStackDepth>(p.bvh, r, key_min, kFar, kb, st, t_drop, p.status, cnt);
+    query<kStackDepth>(p.bvh, r, key_min, kFar, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
     int consumed = 0;
     unsigned long long last = 0;
 #pragma unroll
     for (int j = 0; j < kChunk; ++j) {
-      const unsigned long long key = kb[j];
+      const unsigned long long key = sm.keys[j * sm.stride];
       if (key == kEmptyKey || key_t(key) >= t_drop) break;
       if (count < p.max_hits) {
         p.ids[(size_t)i * p.max_hits + count] = key_prim(key);
