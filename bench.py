@@ -541,9 +541,9 @@ def main():
     tr.build_tri_accel(verts, cums, P, True)
     use_cache = not args.no_hit_cache
 
-    def step():
+    def step(cached=use_cache):
         # the hit cache is the step's activation: allocated (caching allocator) and filled every step
-        cache = tr.new_hit_cache(R) if use_cache else None
+        cache = tr.new_hit_cache(R) if cached else None
         out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg, extra,
                                1, False, hit_cache=cache).data
         tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling, False,
@@ -604,6 +604,23 @@ def main():
     elapsed_ms = slowest_rank_ms(elapsed_ms, world, dev)
     ms_per_step = elapsed_ms / args.steps
     value = world * R * args.steps / (elapsed_ms / 1e3) / 1e6
+
+    # the same timed protocol with the adjoint re-traversing every query
+    value_retrace = None
+    if use_cache:
+        for _ in range(2):
+            step(False)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0.record()
+        for _ in range(args.steps):
+            step(False)
+        t1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        value_retrace = world * R * args.steps / (slowest_rank_ms(t0.elapsed_time(t1), world, dev) / 1e3) / 1e6
 
     # ---------------- roofline of the dominant kernel (adjoint)
     fwd_ms, bwd_ms = timed_kernels(3)
@@ -718,8 +735,10 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "triangles": P, "views": views, "H": H, "W": W, "rays_per_step": R,
                    "step": "BVH refit + forward trace + adjoint trace",
-                   "hit_cache": ("the forward stores each ray's first k-closest query (the step's activation, "
-                                 "(k+1)*8 B/ray); the adjoint replays it and traverses only for later queries"
+                   "hit_cache": ({"on": "the forward stores its k-closest queries (the step's activation: "
+                                        "(k+1)*8 B/ray for first queries + a pool for later ones); the adjoint "
+                                        "replays them instead of re-traversing",
+                                  "value_with_retracing_adjoint": value_retrace}
                                  if use_cache else "off: the adjoint re-traverses every query"),
                    "l2": "inputs larger than L2 (scene + BVH + rays ~0.5 GB per step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
