@@ -156,7 +156,8 @@ def cpu_run(runner, sc, ro, rd, g, go, rows, nthreads):
 def cpu_baseline(name, sc, ro, rd, g, go, budget_s=12.0):
     """Times the reference's own per-ray code built for the host (oracle/_ref)
     if it was built, else the oracle's FP32 port, on all host cores, over a
-    bounded band of rows of the first view."""
+    bounded band of rows of the stacked views (centred on the first view's
+    middle row)."""
     from oracle import pyoracle
 
     if pyoracle.reference_available():
@@ -445,14 +446,16 @@ def run_views(args, world, rank, local, dev):
     eager = ViewBatch(tr, shapes, scene, 3, bg, graph=False)
     eager.set_rays([(T(a), T(b)) for a, b in rays_np])
     eager.set_upstream([(T(a), T(b)) for a, b in ups_np])
-    tuned = None if args.no_autotune else autotune(tr, eager.step, key=name, iters=2)
+    tuned = None if args.no_autotune else autotune(tr, eager.step, key=name, iters=2, prepare=eager.fit_hit_cache)
     # kernels per step, counted on an eager step (graph replays are not seen by the host counter)
+    eager.fit_hit_cache()
     tr.reset_stats()
     eager.step()
     per_step = tr.stats()["kernel_launches"]
     vb = ViewBatch(tr, shapes, scene, 3, bg, graph=True)
     vb.set_rays([(T(a), T(b)) for a, b in rays_np])
     vb.set_upstream([(T(a), T(b)) for a, b in ups_np])
+    cache_use = vb.fit_hit_cache()
     for _ in range(max(3, args.warmup)):
         vb.step()
     torch.cuda.synchronize()
@@ -489,6 +492,9 @@ def run_views(args, world, rank, local, dev):
                    "step": "one CUDA-graph replay: refit + forward + adjoint over all views",
                    "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
                    "autotune_ms": tuned.get("all") if tuned else None,
+                   "hit_cache": {"pool_queries": cache_use["pool_cap"], "later_queries": cache_use["pool_used"],
+                                 "replays_per_ray": st["hit_cache_replays"] / max(st["rays"], 1),
+                                 "queries_per_ray": st["queries"] / max(st["rays"], 1)},
                    "hits_per_ray": {"evaluated": st["evaluated_hits"] / max(st["rays"], 1),
                                     "blended": st["blended_hits"] / max(st["rays"], 1)}},
         "gpu_launches": int(per_step * args.steps), "clocks": clocks,

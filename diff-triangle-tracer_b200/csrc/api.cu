@@ -167,6 +167,27 @@ size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays) {
   return tt::hit_cache_bytes(h->k(), rays);
 }
 
+size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long pool_queries) {
+  if (!h || rays < 0 || pool_queries < 0) return 0;
+  const int k = h->k();
+  return tt::hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)pool_queries;
+}
+
+int tt_hit_cache_usage(tt_tracer* h, const void* hit_cache, void* stream, int* k, long long* pool_cap,
+                       long long* pool_used) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, hit_cache != nullptr, "hit_cache is null");
+  tt::HitCacheHeader hd;
+  const cudaStream_t s = as_stream(stream);
+  TT_CUDA(h, cudaMemcpyAsync(&hd, hit_cache, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(h, cudaStreamSynchronize(s));
+  TT_REQUIRE(h, hd.magic == tt::kHitCacheMagic, "hit_cache was not written by a forward");
+  if (k) *k = (int)hd.k;
+  if (pool_cap) *pool_cap = hd.pool_cap;
+  if (pool_used) *pool_used = hd.pool_used;
+  return TT_OK;
+}
+
 int tt_destroy(tt_tracer* h) {
   if (!h) return TT_ERR_INVALID;
   h->bvh.release();

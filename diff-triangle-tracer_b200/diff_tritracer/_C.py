@@ -156,14 +156,29 @@ class OptixTracer:
                                        int(number_of_points), _stream()))
         self._keep = (verts, cumsum)
 
-    def new_hit_cache(self, rays, k=None):
+    def new_hit_cache(self, rays, k=None, pool=None):
         """A device buffer for the hit cache of `rays` rays: sized for the
-        current traversal configuration (tt_hit_cache_bytes), or for queries of
-        `k` hits (k = 32 fits every configuration). No reference counterpart."""
-        n = lib.tt_hit_cache_bytes(self._h, int(rays))
+        current traversal configuration (tt_hit_cache_bytes_pool), or for
+        queries of `k` hits (k = 32 fits every configuration), with room for
+        `pool` later queries (default: a quarter of the rays). No reference
+        counterpart."""
+        rays = int(rays)
+        pool = (rays + 3) // 4 if pool is None else int(pool)
+        n = lib.tt_hit_cache_bytes_pool(self._h, rays, pool)
         if k is not None:
-            n = max(n, 32 + (int(k) + 1) * 8 * int(rays) + (int(k) + 2) * 8 * ((int(rays) + 3) // 4))
+            n = max(n, 32 + (int(k) + 1) * 8 * rays + (int(k) + 2) * 8 * pool)
         return torch.empty((n,), dtype=torch.uint8, device=self.device)
+
+    def hit_cache_usage(self, hit_cache):
+        """The header of a hit cache a forward has filled (synchronises the
+        current stream): {"k", "pool_cap", "pool_used"}. pool_used > pool_cap
+        means some later queries were not stored and the adjoint traverses
+        again for them; the count is then a lower bound on what the pool
+        needs (a ray stops asking after its first refusal)."""
+        k, cap, used = ctypes.c_int(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+        check(self._h, lib.tt_hit_cache_usage(self._h, ctypes.c_void_p(hit_cache.data_ptr()), _stream(),
+                                              ctypes.byref(k), ctypes.byref(cap), ctypes.byref(used)))
+        return {"k": k.value, "pool_cap": cap.value, "pool_used": used.value}
 
     def trace_forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
                       cumsum_of_points_per_triangle, number_of_points, shs, sh_degree, colors_precomp, opacities,

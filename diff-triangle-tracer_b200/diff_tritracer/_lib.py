@@ -115,7 +115,7 @@ EXPORTS = (
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
     "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
     "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree", "tt_bvh_save",
-    "tt_bvh_load", "tt_hit_cache_bytes",
+    "tt_bvh_load", "tt_hit_cache_bytes", "tt_hit_cache_bytes_pool", "tt_hit_cache_usage",
 )
 
 
@@ -151,9 +151,13 @@ def _load():
     lib.tt_mlp_intervals.argtypes = [_vp, ctypes.POINTER(TtMlp), ctypes.POINTER(TtView), ctypes.c_int,
                                      ctypes.POINTER(_vp), ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp]
     lib.tt_hit_cache_bytes.argtypes = [_vp, ctypes.c_longlong]
+    lib.tt_hit_cache_bytes_pool.argtypes = [_vp, ctypes.c_longlong, ctypes.c_longlong]
+    lib.tt_hit_cache_usage.argtypes = [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype if name == "tt_last_error" else ctypes.c_int
     lib.tt_hit_cache_bytes.restype = ctypes.c_size_t
+    lib.tt_hit_cache_bytes_pool.restype = ctypes.c_size_t
     return lib
 
 

@@ -35,8 +35,11 @@ def _load(path):
         return {}
 
 
-def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int = 3, force: bool = False):
-    """Returns the chosen configuration (dict) and applies it to `tracer`."""
+def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int = 3, force: bool = False,
+             prepare=None):
+    """Returns the chosen configuration (dict) and applies it to `tracer`.
+    `prepare` (e.g. ViewBatch.fit_hit_cache) runs after each candidate is
+    applied and before it is timed."""
     full_key = f"{torch.cuda.get_device_name(tracer.device)}|{key}"
     cache = _load(cache_path)
     if not force and full_key in cache:
@@ -46,6 +49,8 @@ def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int
     timings = []
     for cand in CANDIDATES:
         tracer.set_traversal(cand["traversal"], cand["k"], cand["stack_depth"])
+        if prepare is not None:
+            prepare()
         step()  # warm-up
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)

@@ -6,7 +6,9 @@ through ONE persistent forward launch and ONE adjoint launch per step
 to the current vertices, forward, adjoint - is recorded once into a CUDA graph
 and replayed, so a training step costs one graph launch on the host. With
 `hit_cache=True` the forward keeps its k-closest queries in a static buffer
-and the adjoint replays them instead of traversing again. Rays and
+and the adjoint replays them instead of traversing again; the first step
+(and every `fit_hit_cache()` call) grows that buffer's pool until one
+forward's later queries all fit, so deep scenes replay every query. Rays and
 upstream gradients are copied into the batch's static buffers before replay;
 the scene tensors must keep their storage between steps (optimisers update
 them in place).
@@ -42,18 +44,48 @@ class ViewBatch:
         M = scene["shs"].shape[1]
         self.grads = (torch.zeros((V, 3), **f32), torch.zeros_like(scene["sigma"]),
                       torch.zeros_like(scene["opacities"]), torch.zeros((P, M, 3), **f32))
+        self.num_rays = sum(H * W for H, W in shapes)
         # sized for 32-hit queries, so it serves every traversal configuration
-        self.hit_cache = tracer.new_hit_cache(sum(H * W for H, W in shapes), k=32) if hit_cache else None
+        self.hit_cache = tracer.new_hit_cache(self.num_rays, k=32) if hit_cache else None
+        self._fitted = not hit_cache
         self.graph = None
         # the first pass builds the BVH outside any capture
         self._forward(0)
         self._backward()
         torch.cuda.synchronize()
-        if graph:
-            self.graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.graph):
+        self._use_graph = graph
+        self._capture()
+
+    def _capture(self):
+        self.graph = None
+        if self._use_graph:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
                 self._forward(1)
                 self._backward()
+            self.graph = graph
+
+    def fit_hit_cache(self, rounds: int = 4):
+        """Runs forwards over the current rays and grows the hit cache's pool
+        until all of one forward's later queries fit (a ray stops asking after
+        its first refusal, so an overflow may take a few rounds to size). The
+        graph is recorded again if the buffer changed. Synchronises; returns
+        the last forward's pool usage (see OptixTracer.hit_cache_usage)."""
+        self._fitted = True
+        if self.hit_cache is None:
+            return None
+        grown = False
+        for _ in range(rounds):
+            self._forward(1)
+            use = self.tracer.hit_cache_usage(self.hit_cache)
+            if use["pool_used"] <= use["pool_cap"]:
+                break
+            self.hit_cache = None  # release the old buffer first
+            self.hit_cache = self.tracer.new_hit_cache(self.num_rays, k=32, pool=int(use["pool_used"] * 1.25) + 1024)
+            grown = True
+        if grown:
+            self._capture()
+        return use
 
     def _forward(self, rebuild_gas):
         s = self.scene
@@ -82,7 +114,10 @@ class ViewBatch:
 
     def step(self):
         """Refit + forward + adjoint over all views; results in .outputs,
-        .max_blending and .grads."""
+        .max_blending and .grads. The first step fits the hit cache to the
+        rays (fit_hit_cache) and synchronises."""
+        if not self._fitted:
+            self.fit_hit_cache()
         if self.graph is not None:
             self.graph.replay()
         else:

@@ -233,6 +233,23 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  * No reference counterpart. */
 size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays);
 
+/* Bytes of a hit cache for `rays` rays whose pool holds `pool_queries` later
+ * queries under the handle's current traversal configuration:
+ * 32 + (k + 1) * 8 * rays + (k + 2) * 8 * pool_queries. No reference
+ * counterpart. */
+size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long pool_queries);
+
+/* Reads the header of a hit cache that a forward has filled, after
+ * synchronising `stream`. It gives the hits per query `k` the cache was laid
+ * out for, the pool's capacity, and the later queries the forward asked the
+ * pool for. The last count can pass the capacity: those queries were not
+ * stored and the adjoint traverses again for them. A ray stops asking after
+ * its first refusal, so after an overflow the count is a lower bound.
+ * Returns TT_ERR_INVALID if no forward wrote the cache. No reference
+ * counterpart. */
+int tt_hit_cache_usage(tt_tracer* h, const void* hit_cache, void* stream, int* k, long long* pool_cap,
+                       long long* pool_used);
+
 /* Message of the last failed call on this handle (never NULL). */
 const char* tt_last_error(const tt_tracer* h);
 

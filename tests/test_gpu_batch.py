@@ -157,3 +157,41 @@ def test_graph_replays_with_hit_cache_match_retraced_eager():
         for a, b in zip(gg, ge):
             assert rel_norm(a, b) < 1e-5
     assert not np.array_equal(results[True][0][0][0], results[True][1][0][0])
+
+
+def test_batch_fits_its_hit_cache_pool():
+    """A batch whose cache has no pool: fit_hit_cache grows it until one
+    forward's later queries all fit and records the graph again; every query
+    is then replayed and the results equal an uncached eager batch."""
+    sc = dense_scene(seed=8, P=3000)
+    vs = views()
+    ups = [scenes.upstream_grads(H, W, seed=30 + i, others_std=1.0) for i, (H, W) in enumerate(SHAPES)]
+    bg = torch.zeros(3, device=DEV)
+    results = {}
+    for cached in (True, False):
+        s = scene_tensors(sc)
+        tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+        tr.set_traversal("packets", k=16)
+        vb = ViewBatch(tr, SHAPES, s, 3, bg, graph=cached, hit_cache=cached)
+        vb.set_rays([(T(ro), T(rd)) for ro, rd in vs])
+        vb.set_upstream([(T(g), T(go)) for g, go in ups])
+        if cached:
+            vb.hit_cache = tr.new_hit_cache(vb.num_rays, pool=0)  # 16-hit queries, main part only
+            vb._capture()
+            vb._forward(1)
+            before = tr.hit_cache_usage(vb.hit_cache)
+            assert before["pool_cap"] == 0 and before["pool_used"] > 0
+            use = vb.fit_hit_cache()
+            assert 0 < use["pool_used"] <= use["pool_cap"]
+        tr.reset_stats()
+        vb.step()
+        torch.cuda.synchronize()
+        tr.device_status()
+        st = tr.stats()
+        if cached:
+            assert st["hit_cache_replays"] == st["queries"]
+        results[cached] = ([c.cpu().numpy() for c, _ in vb.outputs], [g.cpu().numpy() for g in vb.grads])
+    for a, b in zip(results[True][0], results[False][0]):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(results[True][1], results[False][1]):
+        assert rel_norm(a, b) < 1e-5

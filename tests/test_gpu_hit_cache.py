@@ -11,7 +11,8 @@ traversing the BVH again.
   ignore the cache (no replay) and still give the same gradients;
 * batched views, proposed intervals and the exact adjoint replay too;
 * the autograd module gives the same gradients with and without the cache;
-* the forward rejects a cache smaller than tt_hit_cache_bytes.
+* the forward rejects a cache smaller than tt_hit_cache_bytes;
+* tt_hit_cache_usage reports the pool's capacity and demand.
 """
 import numpy as np
 import pytest
@@ -185,3 +186,26 @@ def test_misaligned_cache_and_variant_program_rejected(setup):
                           torch.empty(0, device=DEV), s["opac"], torch.zeros(sc.P, device=DEV),
                           torch.zeros(sc.P, device=DEV), st.bg, st.extra_params, st.rebuild_gas, False,
                           hit_cache=var.new_hit_cache(H * W))
+
+
+def test_usage_reports_pool_capacity_and_demand(setup):
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal="packets")
+    tr.set_traversal("packets", k=16)
+    R = H * W
+    with pytest.raises(RuntimeError, match="not written by a forward"):
+        tr.hit_cache_usage(torch.zeros(tr.new_hit_cache(R).numel(), dtype=torch.uint8, device=DEV))
+    # a pool for every later query: the demand is exact (queries after each ray's first)
+    big = tr.new_hit_cache(R, pool=8 * R)
+    assert big.numel() == 32 + 17 * 8 * R + 18 * 8 * 8 * R
+    forward(tr, sc, s, ro, rd, big)
+    queries = tr.stats()["queries"]
+    use = tr.hit_cache_usage(big)
+    assert use == {"k": 16, "pool_cap": 8 * R, "pool_used": queries - R}
+    # no pool: every ray that needs a later query asks once and is refused
+    none = tr.new_hit_cache(R, pool=0)
+    forward(tr, sc, s, ro, rd, none, rebuild=2)
+    use = tr.hit_cache_usage(none)
+    assert use["pool_cap"] == 0 and 0 < use["pool_used"] <= queries - R
+    _, n = backward(tr, sc, s, ro, rd, *forward(tr, sc, s, ro, rd, none, rebuild=2), g, go, none)
+    assert n == R
