@@ -11,7 +11,11 @@ are checked through properties that do not depend on size:
   oracle's adjoint of the sampled rays (gradients within 1e-4 relative);
 * the traversal configurations give the same images bit for bit, a forward
   repeated gives the same bits, and the replayed adjoint equals the
-  re-traversing one up to the order of float atomics (1e-6).
+  re-traversing one up to the order of float atomics (1e-6);
+* the batched workload (3M triangles, 16 views of uneven size, 10.2M rays,
+  one CUDA-graph replay of refit + forward + adjoint with the fitted hit
+  cache): a sample of its pixels and the adjoint of that sample equal the
+  oracle's.
 """
 import numpy as np
 import pytest
@@ -22,7 +26,9 @@ pytestmark = pytest.mark.gpu
 if not torch.cuda.is_available():
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
+from bench import make_workload  # noqa: E402
 from diff_tritracer import _C, scenes  # noqa: E402
+from diff_tritracer.batch import ViewBatch  # noqa: E402
 from gpu_helpers import DEV, MARGIN, T, rel_norm  # noqa: E402
 
 P, VIEWS, H, W = 1_000_000, 4, 800, 800
@@ -141,3 +147,55 @@ def test_replayed_adjoint_equals_retraced(c2):
     tr.device_status()
     for a, b in zip(replayed, retraced):
         assert rel_norm(a, b) < 1e-6
+
+
+def test_batched_views_sample_matches_fp64_oracle(oracle):
+    sc, rays, _ = make_workload("c4_3M_16views")
+    shapes = [r[0].shape[:2] for r in rays]
+    sizes = [h * w for h, w in shapes]
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    ro_all = np.concatenate([r[0].reshape(-1, 3) for r in rays])
+    rd_all = np.concatenate([r[1].reshape(-1, 3) for r in rays])
+    idx = np.sort(np.random.default_rng(11).choice(starts[-1], N_SAMPLE, replace=False))
+    view = np.searchsorted(starts, idx, side="right") - 1
+    ro_s, rd_s = ro_all[idx][None].copy(), rd_all[idx][None].copy()
+    ref = oracle.forward(sc, ro_s, rd_s, precision=64, exact=True, canonical=True, record=1, nthreads=8)
+    ok = ref.margin > MARGIN
+    assert ok.mean() > 0.97, ok.mean()
+    g_s, go_s = scenes.upstream_grads(1, N_SAMPLE, seed=13, others_std=1.0)
+    g_s, go_s = g_s * ok[None, None], go_s * ok[None, None]
+    ups = [(np.zeros((3, h, w), np.float32), np.zeros((7, h, w), np.float32)) for h, w in shapes]
+    for j, (v, i) in enumerate(zip(view, idx)):
+        y, x = divmod(int(i - starts[v]), shapes[v][1])
+        ups[v][0][:, y, x] = g_s[:, 0, j]
+        ups[v][1][:, y, x] = go_s[:, 0, j]
+    P = sc.P
+    scene = dict(triangles_points=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), num_points_per_triangle=T(sc.num_points),
+                 cumsum_of_points_per_triangle=T(sc.cumsum), number_of_points=P, shs=T(sc.shs),
+                 opacities=T(sc.opacities), scaling=torch.zeros(P, device=DEV), density_factor=torch.zeros(P, device=DEV))
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.set_traversal("packets", 32, 0)
+    vb = ViewBatch(tr, shapes, scene, 3, torch.zeros(3, device=DEV), graph=True)
+    vb.set_rays([(T(a), T(b)) for a, b in rays])
+    vb.set_upstream([(T(a), T(b)) for a, b in ups])
+    use = vb.fit_hit_cache()
+    assert use["pool_used"] <= use["pool_cap"]
+    tr.reset_stats()
+    vb.step()
+    torch.cuda.synchronize()
+    tr.device_status()
+    st = tr.stats()
+    assert st["hit_cache_replays"] == st["queries"] > starts[-1]  # every query replayed
+    for key, ch in (("color", 0), ("others", 1)):
+        got = np.concatenate([vb.outputs[v][ch].reshape(vb.outputs[v][ch].shape[0], -1).cpu().numpy()
+                              for v in range(len(shapes))], 1)[:, idx][:, ok]
+        want = getattr(ref, key).reshape(got.shape[0], -1)[:, ok]
+        err = np.abs(got - want)
+        assert np.all(err <= RTOL * np.abs(want) + ATOL), (key, float((err / (RTOL * np.abs(want) + ATOL)).max()))
+    rb = oracle.backward(sc, ro_s, rd_s, ref.color, ref.others, g_s, go_s, precision=64, exact=True, canonical=True,
+                         nthreads=8)
+    for got, key in zip(vb.grads, ("dtri", "dsigma", "dopac", "dsh")):
+        want = getattr(rb, key)
+        assert np.linalg.norm(want) > 0, key
+        e = rel_norm(got.cpu().numpy(), want)
+        assert e < GRAD_RTOL, (key, e)
