@@ -173,6 +173,20 @@ size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long poo
   return tt::hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)pool_queries;
 }
 
+int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream) {
+  if (!h) return TT_ERR_INVALID;
+  TT_REQUIRE(h, cams != nullptr && n_cams >= 1 && n_cams <= tt::kMaxViews, "1 to 32 cameras");
+  for (int c = 0; c < n_cams; ++c) {
+    TT_REQUIRE(h, cams[c].H > 0 && cams[c].W > 0, "camera H and W must be > 0");
+    TT_REQUIRE(h, cams[c].ray_o != nullptr && cams[c].ray_d != nullptr, "camera ray_o / ray_d are null");
+    TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(cams[c].ray_o) & 3u) == 0 &&
+                      (reinterpret_cast<uintptr_t>(cams[c].ray_d) & 3u) == 0,
+               "camera ray_o / ray_d must be 4-byte aligned");
+  }
+  TT_CUDA(h, tt::launch_camera_rays(cams, n_cams, as_stream(stream)));
+  return TT_OK;
+}
+
 int tt_hit_cache_usage(tt_tracer* h, const void* hit_cache, void* stream, int* k, long long* pool_cap,
                        long long* pool_used) {
   if (!h) return TT_ERR_INVALID;

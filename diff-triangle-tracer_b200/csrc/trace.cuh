@@ -4,6 +4,8 @@
 
 #include "tt_device.cuh"
 
+struct tt_camera;  // include/tritracer.h
+
 namespace tt {
 
 // One camera image: its rays ([H][W][3]) and per-pixel outputs/inputs
@@ -168,5 +170,7 @@ cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_primary(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s);
 cudaError_t launch_sec_backward(const TraceParams& p, int grid, cudaStream_t s);
+// camera.cu: primary rays of up to kMaxViews pinhole cameras (tt_camera_rays)
+cudaError_t launch_camera_rays(const tt_camera* cams, int n, cudaStream_t s);
 
 }  // namespace tt

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -168,6 +169,33 @@ class OptixTracer:
         if k is not None:
             n = max(n, 32 + (int(k) + 1) * 8 * rays + (int(k) + 2) * 8 * pool)
         return torch.empty((n,), dtype=torch.uint8, device=self.device)
+
+    def camera_rays(self, cameras, outputs=None):
+        """Primary rays of pinhole cameras (diff_tritracer.scenes.Camera: origin,
+        forward/right/up basis, H, W, vertical fov_deg) generated on the device
+        in one launch (tt_camera_rays), bit for bit the rays of
+        scenes.camera_rays. Returns [(ray_o, ray_d)] per camera, [H, W, 3]
+        each, written into `outputs` when given. No reference counterpart: the
+        reference's callers build the ray tensors themselves."""
+        cams = list(cameras)
+        if outputs is None:
+            outputs = [(torch.empty((c.H, c.W, 3), dtype=torch.float32, device=self.device),
+                        torch.empty((c.H, c.W, 3), dtype=torch.float32, device=self.device)) for c in cams]
+        if len(outputs) != len(cams):
+            raise RuntimeError("one (ray_o, ray_d) pair per camera")
+        arr = (_lib.TtCamera * max(len(cams), 1))()
+        for a, c, (ro, rd) in zip(arr, cams, outputs):
+            for t in (ro, rd):
+                if t.dtype != torch.float32 or t.device != self.device or not t.is_contiguous() \
+                        or tuple(t.shape) != (c.H, c.W, 3):
+                    raise RuntimeError("camera ray outputs must be contiguous float32 [H, W, 3] on the tracer's device")
+            for name in ("origin", "forward", "right", "up"):
+                getattr(a, name)[:] = [float(x) for x in getattr(c, name)]
+            a.tan_half_fov = float(np.tan(np.deg2rad(c.fov_deg) / 2.0))  # as scenes.camera_rays
+            a.H, a.W = int(c.H), int(c.W)
+            a.ray_o, a.ray_d = _ptr(ro), _ptr(rd)
+        check(self._h, lib.tt_camera_rays(self._h, arr, len(cams), _stream()))
+        return outputs
 
     def hit_cache_usage(self, hit_cache):
         """The header of a hit cache a forward has filled (synchronises the

@@ -80,6 +80,12 @@ class TtView(ctypes.Structure):
                 ("dL_dpixels", _vp), ("dL_dothers", _vp), ("interval", _vp), ("record", _vp)]
 
 
+class TtCamera(ctypes.Structure):
+    _fields_ = [("origin", ctypes.c_double * 3), ("forward", ctypes.c_double * 3), ("right", ctypes.c_double * 3),
+                ("up", ctypes.c_double * 3), ("tan_half_fov", ctypes.c_double), ("H", ctypes.c_int),
+                ("W", ctypes.c_int), ("ray_o", _vp), ("ray_d", _vp)]
+
+
 class TtStats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_ulonglong), ("evaluated_hits", ctypes.c_ulonglong),
                 ("blended_hits", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong),
@@ -116,6 +122,7 @@ EXPORTS = (
     "tt_backward_views", "tt_set_traversal", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
     "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree", "tt_bvh_save",
     "tt_bvh_load", "tt_hit_cache_bytes", "tt_hit_cache_bytes_pool", "tt_hit_cache_usage",
+    "tt_camera_rays",
 )
 
 
@@ -152,6 +159,7 @@ def _load():
                                      ctypes.POINTER(_vp), ctypes.c_float, ctypes.c_float, ctypes.c_float, _vp]
     lib.tt_hit_cache_bytes.argtypes = [_vp, ctypes.c_longlong]
     lib.tt_hit_cache_bytes_pool.argtypes = [_vp, ctypes.c_longlong, ctypes.c_longlong]
+    lib.tt_camera_rays.argtypes = [_vp, ctypes.POINTER(TtCamera), ctypes.c_int, _vp]
     lib.tt_hit_cache_usage.argtypes = [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:

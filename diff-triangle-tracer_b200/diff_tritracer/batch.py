@@ -107,6 +107,12 @@ class ViewBatch:
             so.copy_(ro, non_blocking=True)
             sd.copy_(rd, non_blocking=True)
 
+    def set_cameras(self, cameras):
+        """Generates the views' rays on the device from pinhole cameras
+        (scenes.Camera, one per view, of the batch's shapes) into the static
+        ray buffers: one launch, no host copy (OptixTracer.camera_rays)."""
+        self.tracer.camera_rays(cameras, outputs=self.rays)
+
     def set_upstream(self, upstream):
         for (g, go), (sg, sgo) in zip(upstream, self.upstream):
             sg.copy_(g, non_blocking=True)

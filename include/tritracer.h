@@ -250,6 +250,29 @@ size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long poo
 int tt_hit_cache_usage(tt_tracer* h, const void* hit_cache, void* stream, int* k, long long* pool_cap,
                        long long* pool_used);
 
+/* A pinhole camera whose rays tt_camera_rays writes. Pixel (x, y) of its
+ * H x W image starts at `origin` and looks along normalize(forward + u right +
+ * v up), u = (2 (x + 0.5) / W - 1) t (W / H), v = (1 - 2 (y + 0.5) / H) t,
+ * t = tan_half_fov (half the vertical field of view), each step an FP64
+ * operation in that order, the result rounded to FP32. ray_o / ray_d:
+ * [H][W][3] float32 on the device. */
+typedef struct tt_camera {
+  double origin[3];
+  double forward[3];
+  double right[3];
+  double up[3];
+  double tan_half_fov;
+  int H, W;
+  float* ray_o;
+  float* ray_d;
+} tt_camera;
+
+/* Writes the rays of 1 to 32 cameras in one launch on `stream`; capturable
+ * in a CUDA graph. This is the caller's side of the path: the reference takes
+ * ray tensors (tritracer/tracer.cpp:36-37) and leaves generating them to the
+ * training code. No reference counterpart. */
+int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream);
+
 /* Message of the last failed call on this handle (never NULL). */
 const char* tt_last_error(const tt_tracer* h);
 

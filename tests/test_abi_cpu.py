@@ -41,7 +41,7 @@ def test_struct_layout_matches_header():
 
     structs = {"tt_config": _lib.TtConfig, "tt_fwd_args": _lib.TtFwdArgs, "tt_bwd_args": _lib.TtBwdArgs,
                "tt_view": _lib.TtView, "tt_stats": _lib.TtStats, "tt_mlp": _lib.TtMlp,
-               "tt_mlp_step": _lib.TtMlpStep, "tt_secondary": _lib.TtSecondary}
+               "tt_mlp_step": _lib.TtMlpStep, "tt_secondary": _lib.TtSecondary, "tt_camera": _lib.TtCamera}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
