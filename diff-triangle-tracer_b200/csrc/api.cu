@@ -7,6 +7,8 @@
 #include <new>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/tritracer.h"
 #include "bvh.cuh"
 #include "proposal.cuh"
@@ -62,6 +64,16 @@ int cuda_fail(tt_tracer* h, cudaError_t e, const char* what) {
   } while (0)
 
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+// NVTX range over an entry point, named after it: a profiler shows the
+// launches the call enqueues under that name. Free when no tool is attached.
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+#define TT_RANGE() const Range tt_range_(__func__)
 
 int accel_step(tt_tracer* h, const float* verts, int num_vertices, const int* cumsum, int P, int mode,
                cudaStream_t s) {
@@ -174,6 +186,7 @@ size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long poo
 }
 
 int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   TT_REQUIRE(h, cams != nullptr && n_cams >= 1 && n_cams <= tt::kMaxViews, "1 to 32 cameras");
   for (int c = 0; c < n_cams; ++c) {
@@ -218,6 +231,7 @@ const char* tt_last_error(const tt_tracer* h) { return h ? h->err.c_str() : "nul
 
 int tt_build(tt_tracer* h, const float* vertices, int num_vertices, const int* cumsum, int P, int mode,
              void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   return accel_step(h, vertices, num_vertices, cumsum, P, mode, as_stream(stream));
 }
@@ -341,6 +355,7 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
 }
 
 int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
   TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
@@ -357,6 +372,7 @@ int tt_forward(tt_tracer* h, const tt_fwd_args* a, void* stream) {
 }
 
 int tt_forward_views(tt_tracer* h, const tt_fwd_args* a, const tt_view* views, int n_views, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a || !views) return fail(h, TT_ERR_INVALID, "null argument block or view list");
   return forward_impl(h, a, views, n_views, stream);
@@ -429,6 +445,7 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
 }
 
 int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
   TT_REQUIRE(h, a->H > 0 && a->W > 0, "ray_o must be [H, W, 3] with H, W > 0");
@@ -448,6 +465,7 @@ int tt_backward(tt_tracer* h, const tt_bwd_args* a, void* stream) {
 }
 
 int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, int n_views, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a || !views) return fail(h, TT_ERR_INVALID, "null argument block or view list");
   return backward_impl(h, a, views, n_views, stream);
@@ -495,6 +513,7 @@ int tt_reset_stats(tt_tracer* h, void* stream) {
 
 int tt_hit_stream(tt_tracer* h, const float* ray_o, const float* ray_d, int R, int max_hits, uint32_t* ids,
                   float* ts, int* counts, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   TT_REQUIRE(h, R >= 0 && max_hits >= 0, "R and max_hits must be >= 0");
   TT_REQUIRE(h, R == 0 || (ray_o && ray_d && counts && (max_hits == 0 || (ids && ts))), "null pointer");
@@ -524,6 +543,7 @@ static int check_mlp(tt_tracer* h, const tt_mlp* net) {
 }
 
 int tt_mlp_update(tt_tracer* h, const tt_mlp* net, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   int rc = check_mlp(h, net);
   if (rc != TT_OK) return rc;
@@ -539,6 +559,7 @@ int tt_mlp_update(tt_tracer* h, const tt_mlp* net, void* stream) {
 
 int tt_mlp_train_step(tt_tracer* h, const tt_mlp* net, const tt_mlp_step* st, const float* rays,
                       const float* targets, int n, float* loss, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   int rc = check_mlp(h, net);
   if (rc != TT_OK) return rc;
@@ -612,6 +633,7 @@ static int mlp_infer(tt_tracer* h, const tt_mlp* net, tt::mlp::InferParams& p, f
 }
 
 int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, float* out, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   int rc = check_mlp(h, net);
   if (rc != TT_OK) return rc;
@@ -634,6 +656,7 @@ int tt_mlp_predict(tt_tracer* h, const tt_mlp* net, const float* rays, int n, fl
 
 int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int n_views, float* const* intervals,
                      float margin_near, float margin_far, float far_cap, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   int rc = check_mlp(h, net);
   if (rc != TT_OK) return rc;
@@ -689,6 +712,7 @@ static void sec_layout(tt::SecParams& sp, const tt_secondary* sec, tt::SecRecord
 }
 
 int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary* sec, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
   int rc = check_secondary(h, sec, a->P);
@@ -792,6 +816,7 @@ int tt_secondary_tree(tt_tracer* h, void* dst, unsigned long long dst_bytes, int
 }
 
 int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary* sec, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   if (!a) return fail(h, TT_ERR_INVALID, "null argument block");
   int rc = check_secondary(h, sec, a->P);
@@ -864,6 +889,7 @@ int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary
 
 // ---------------------------------------------------------------- BVH files
 int tt_bvh_save(tt_tracer* h, void* dst, unsigned long long capacity, unsigned long long* bytes, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   TT_REQUIRE(h, bytes != nullptr, "null size pointer");
   if (!h->bvh.built() || h->bvh.P() <= 0) return fail(h, TT_ERR_STATE, "no acceleration structure to save");
@@ -877,6 +903,7 @@ int tt_bvh_save(tt_tracer* h, void* dst, unsigned long long capacity, unsigned l
 
 int tt_bvh_load(tt_tracer* h, const void* src, unsigned long long bytes, const float* vertices, int num_vertices,
                 const int* cumsum, int P, void* stream) {
+  TT_RANGE();
   if (!h) return TT_ERR_INVALID;
   TT_REQUIRE(h, src && vertices && cumsum && P > 0 && num_vertices >= 3, "need a blob, vertices and cumsum");
   cudaError_t e = cudaSuccess;
