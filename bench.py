@@ -369,6 +369,85 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
     }
 
 
+def widened_leg(dev, d, P, cams, cfg, steps=3):
+    """The rows around the traced path, timed on the headline workload with
+    CUDA events (same traversal configuration, hit cache on): the exact
+    adjoint's step (full chain rule, depth/middepth/distortion), the step with
+    precomputed per-triangle colours instead of SH, BVH build / refit / save /
+    load, and primary rays generated on the device from the cameras.
+    `d` holds the workload's device tensors."""
+    import torch
+
+    from diff_tritracer import _C
+
+    R = int(d["ro"].shape[0] * d["ro"].shape[1])
+
+    def timed(fn, n=steps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    def tracer(**kw):
+        tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", **kw)
+        if cfg:
+            tr.set_traversal(cfg["traversal"], cfg["k"], cfg["stack_depth"])
+        tr.build_tri_accel(d["verts"], d["cums"], P, True)
+        return tr
+
+    def step_fn(tr, shs, cols):
+        def step():
+            cache = tr.new_hit_cache(R)
+            out = tr.trace_forward(d["ro"], d["rd"], d["verts"], d["sig"], d["npts"], d["cums"], P, shs, 3,
+                                   cols if cols is not None else d["empty"], d["opac"], d["scaling"], d["density"],
+                                   d["bg"], d["extra"], 1, False, hit_cache=cache).data
+            tr.trace_backward(d["ro"], d["rd"], d["bg"], d["verts"], d["sig"], d["npts"], d["cums"], out[0], out[1],
+                              P, shs, 3, d["opac"], d["g"], d["go"], d["scaling"], False, colors_precomp=cols,
+                              hit_cache=cache)
+        return step
+
+    res = {}
+    tr = tracer(exact_adjoint=True)
+    ms = timed(step_fn(tr, d["shs"], None))
+    tr.device_status()
+    res["exact_adjoint"] = {"ms_per_step": ms, "mrays": R / ms / 1e3,
+                            "step": "refit + forward (depth, middepth, distortion) + exact adjoint, hit cache"}
+    del tr
+    cols = torch.rand((P, 3), generator=torch.Generator(device=dev).manual_seed(0), device=dev)
+    tr = tracer()
+    ms = timed(step_fn(tr, d["empty"], cols))
+    tr.device_status()
+    res["colors_precomp"] = {"ms_per_step": ms, "mrays": R / ms / 1e3,
+                             "step": "refit + forward + adjoint with [P, 3] colours instead of SH, hit cache"}
+    build_ms = timed(lambda: tr.build_tri_accel(d["verts"], d["cums"], P, True))
+    refit_ms = timed(lambda: tr.build_tri_accel(d["verts"], d["cums"], P, False))
+    t0 = time.perf_counter()
+    blob = tr.save_bvh()
+    save_ms = (time.perf_counter() - t0) * 1e3
+    other = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    other.load_bvh(blob, d["verts"], d["cums"], P)
+    torch.cuda.synchronize()
+    load_ms = (time.perf_counter() - t0) * 1e3
+    res["bvh"] = {"triangles": P, "build_ms": build_ms, "refit_ms": refit_ms, "save_ms": save_ms,
+                  "load_ms": load_ms, "blob_mb": len(blob) / 1e6,
+                  "note": "save: device to host blob; load: host blob to device + refit (wall clock, synchronised)"}
+    del tr, other
+    outs = [(torch.empty((c.H, c.W, 3), device=dev), torch.empty((c.H, c.W, 3), device=dev)) for c in cams]
+    gen = _C.OptixTracer()
+    ms = timed(lambda: gen.camera_rays(cams, outputs=outs), n=10)
+    n_rays = sum(c.H * c.W for c in cams)
+    res["camera_rays"] = {"cameras": len(cams), "rays": n_rays, "ms": ms, "mrays": n_rays / ms / 1e3,
+                          "bytes_written_gb_s": n_rays * 24 / (ms / 1e3) / 1e9}
+    return res
+
+
 def secondary_leg(dev, steps=3, seed=0):
     """Secondary-ray passes on their benchmark configuration: 500k
     triangles, 20 % dielectric (IOR ~ U[1.3, 1.6]), a 512x1024 lat-long
@@ -515,6 +594,8 @@ def main():
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
+    ap.add_argument("--no-widened", action="store_true",
+                    help="skip the leg timing the exact adjoint, precomputed colours, BVH files and camera rays")
     ap.add_argument("--no-hit-cache", action="store_true",
                     help="adjoint re-traverses every query instead of replaying the forward's")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
@@ -715,6 +796,23 @@ def main():
         color.backward(g_d)
         main.wait_stream(copy_stream)
 
+    def link_gbs():
+        # pinned host <-> device bandwidth as this run sees it (the machine is
+        # shared: other jobs' traffic shows here and in the e2e number alike)
+        out = []
+        for src, dst in ((ro_h, ray_bufs[0][0]), (color, color_h)):
+            with torch.cuda.stream(copy_stream):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(copy_stream)
+                for _ in range(3):
+                    dst.copy_(src, non_blocking=True)
+                b.record(copy_stream)
+            torch.cuda.synchronize()
+            out.append(3 * src.numel() * 4 / (a.elapsed_time(b) / 1e3) / 1e9)
+        return out
+
+    color = torch.empty((3, HH, WW), device=dev)
+    link_before = link_gbs()
     upload_rays(0)
     for i in range(2):
         e2e_step(i)
@@ -733,6 +831,7 @@ def main():
     e2e_value = world * R * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     h2d = ro_h.numel() * 4 + rd_h.numel() * 4 + g_h.numel() * 4
     d2h = color_h.numel() * 4
+    link_after = link_gbs()
 
     # ---------------- CPU baseline (rank 0, N = 1)
     prop = None
@@ -741,6 +840,13 @@ def main():
     secondary = None
     if rank == 0 and world == 1 and not args.no_secondary:
         secondary = secondary_leg(dev)
+    widened = None
+    if rank == 0 and world == 1 and not args.no_widened:
+        from diff_tritracer import scenes
+
+        tensors = dict(verts=verts, sig=sig, npts=npts, cums=cums, shs=shs, opac=opac, ro=ro, rd=rd, g=g, go=go,
+                       bg=bg, extra=extra, empty=empty, scaling=scaling, density=density)
+        widened = widened_leg(dev, tensors, P, scenes.sphere_cameras(views, H, W, seed=0), tuned)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -772,7 +878,11 @@ def main():
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "path": "diff_tritracer.Tracer autograd forward+backward, pinned host rays/grads in, image out "
                         "(on a copy stream: gradient upload under the forward; image download and the next "
-                        "step's ray upload, double-buffered, under the adjoint)"},
+                        "step's ray upload, double-buffered, under the adjoint)",
+                "link_gbs": {"h2d_before": link_before[0], "d2h_before": link_before[1], "h2d_after": link_after[0],
+                             "d2h_after": link_after[1],
+                             "note": "pinned copies of one step's rays / image timed alone before and after the "
+                                     "e2e steps (the host link is shared with other jobs)"}},
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
@@ -783,6 +893,7 @@ def main():
         "cpu_baseline": cpu,
         "proposal": prop,
         "secondary": secondary,
+        "widened": widened,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
