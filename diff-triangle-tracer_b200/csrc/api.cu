@@ -135,7 +135,8 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
   if ((e = cudaGetDevice(&h->device)) != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
       (e = h->scratch.reserve(128)) != cudaSuccess || (e = cudaMemset(h->scratch.p, 0, 128)) != cudaSuccess ||
-      (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+      (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess ||
+      (e = tt::trace_init()) != cudaSuccess) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
   }

@@ -1006,6 +1006,11 @@ constexpr size_t smem_bytes_for() {
                     : (size_t)kTraceThreads * (C::SD * 8 + kChunk * 8);
 }
 
+// Exact-adjoint forward: per-thread shared-memory words after the traversal's
+// shared memory (FwdShader<true>).
+constexpr int kXD = 0, kXWsum = 1, kXWt2 = 2, kXMid = 3, kXDist2 = 4, kXMidSet = 5, kExactSlots = 6;
+constexpr size_t kExactSmemBytes = (size_t)kTraceThreads * kExactSlots * 4;
+
 template <int CFG, class Shader>
 __device__ __forceinline__ void run(const TraceParams& p, Shader& sh, Counters& cnt) {
   using C = TraversalCfg<CFG>;
@@ -1041,12 +1046,20 @@ struct FwdShader {
   int pix;
   float3 o, d;
   float C0, C1, C2, N0, N1, N2, T;
-  float D, Wsum, Wt2, mid, dist2;  // EXACT only
-  bool mid_set;
+  // EXACT only: the ray's depth sums, middepth and distortion live in a
+  // per-thread shared-memory slot (kExactSlots words, stride blockDim.x), so
+  // the traversal between two shading passes does not carry them in registers
+  float* xs = nullptr;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
   unsigned first_eval = 0;  // value of n_eval at the ray's first hit (record only)
 
-  __device__ explicit FwdShader(const TraceParams& params) : p(params) {}
+  __device__ FwdShader(const TraceParams& params, size_t exact_offset) : p(params) {
+    if (EXACT) {
+      extern __shared__ __align__(16) unsigned char smem_raw[];
+      xs = reinterpret_cast<float*>(smem_raw + exact_offset) + threadIdx.x;
+    }
+  }
+  __device__ __forceinline__ float& x(int i) { return xs[i * blockDim.x]; }
 
   __device__ __forceinline__ bool begin(const ViewDesc* view, int pixel, float3 ro, float3 rd) {
     v = view;
@@ -1054,8 +1067,10 @@ struct FwdShader {
     o = ro;
     d = rd;
     C0 = C1 = C2 = N0 = N1 = N2 = 0.f;
-    D = Wsum = Wt2 = mid = dist2 = 0.f;
-    mid_set = false;
+    if (EXACT) {
+#pragma unroll
+      for (int i = 0; i < kExactSlots; ++i) x(i) = 0.f;
+    }
     T = 1.0f;
     ++n_rays;
     if (v->record) {
@@ -1100,13 +1115,14 @@ struct FwdShader {
     N2 += g.n.z * w;
     if (EXACT) {
       const float ht = g.t;
-      dist2 += w * (ht * ht * Wsum - 2.0f * ht * D + Wt2);
-      Wsum += w;
-      D += w * ht;
-      Wt2 += w * ht * ht;
-      if (!mid_set && test_T <= 0.5f) {
-        mid = ht;
-        mid_set = true;
+      const float D = x(kXD), Wsum = x(kXWsum), Wt2 = x(kXWt2);
+      x(kXDist2) += w * (ht * ht * Wsum - 2.0f * ht * D + Wt2);
+      x(kXWsum) = Wsum + w;
+      x(kXD) = D + w * ht;
+      x(kXWt2) = Wt2 + w * ht * ht;
+      if (x(kXMidSet) == 0.f && test_T <= 0.5f) {
+        x(kXMid) = ht;
+        x(kXMidSet) = 1.f;
       }
     }
     float3 c;
@@ -1130,13 +1146,13 @@ struct FwdShader {
     v->out_color[pix] = C0 + T * p.bg[0];
     v->out_color[HW + pix] = C1 + T * p.bg[1];
     v->out_color[2 * HW + pix] = C2 + T * p.bg[2];
-    v->out_others[kDepthCh * HW + pix] = EXACT ? D : 0.0f;  // the reference never accumulates depth
+    v->out_others[kDepthCh * HW + pix] = EXACT ? x(kXD) : 0.0f;  // the reference never accumulates depth
     v->out_others[kAlphaCh * HW + pix] = 1.0f - T;
     v->out_others[(kNormalCh + 0) * HW + pix] = N0;
     v->out_others[(kNormalCh + 1) * HW + pix] = N1;
     v->out_others[(kNormalCh + 2) * HW + pix] = N2;
-    v->out_others[kMidDepthCh * HW + pix] = EXACT ? mid : 0.0f;
-    v->out_others[kDistortionCh * HW + pix] = EXACT ? dist2 : 0.0f;
+    v->out_others[kMidDepthCh * HW + pix] = EXACT ? x(kXMid) : 0.0f;
+    v->out_others[kDistortionCh * HW + pix] = EXACT ? x(kXDist2) : 0.0f;
   }
 };
 
@@ -1144,7 +1160,7 @@ template <int CFG, bool EXACT>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
   cache_header<TraversalCfg<CFG>::K>(p);
   Counters cnt;
-  FwdShader<EXACT> sh(p);
+  FwdShader<EXACT> sh(p, smem_bytes_for<CFG>());
   run<CFG>(p, sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
@@ -2267,13 +2283,29 @@ int trace_blocks_per_sm(int which, int cfg) {
   return n > 0 ? n : 1;
 }
 
+// The exact-adjoint forward's accumulators take kExactSmemBytes after the
+// traversal's shared memory, which takes the lane configurations past the
+// default 48 KB of dynamic shared memory: opt those kernels in.
+cudaError_t trace_init() {
+  cudaError_t e = cudaSuccess;
+  auto opt_in = [&](const void* fn, size_t bytes) {
+    if (e == cudaSuccess && bytes > 48 * 1024)
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  };
+  opt_in((const void*)k_forward<kCfgPackets16, true>, smem_bytes_for<kCfgPackets16>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgPackets32, true>, smem_bytes_for<kCfgPackets32>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgLanes24, true>, smem_bytes_for<kCfgLanes24>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgLanes32, true>, smem_bytes_for<kCfgLanes32>() + kExactSmemBytes);
+  return e;
+}
+
 template <bool EXACT>
 cudaError_t launch_forward_t(const TraceParams& p, int grid, cudaStream_t s) {
   switch (p.cfg) {
-    case kCfgPackets16: k_forward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
-    case kCfgPackets32: k_forward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
-    case kCfgLanes24: k_forward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
-    default: k_forward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+    case kCfgPackets16: k_forward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
+    case kCfgPackets32: k_forward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
+    case kCfgLanes24: k_forward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
+    default: k_forward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
   }
   return cudaGetLastError();
 }

@@ -160,6 +160,8 @@ constexpr int kNumCfgs = 4;
 size_t trace_smem_bytes(int cfg);
 // Resident blocks per SM of the forward / adjoint / variant kernels.
 int trace_blocks_per_sm(int which /*0 forward, 1 adjoint, 2 variant*/, int cfg);
+// once per handle: kernel attributes (dynamic shared memory opt-ins)
+cudaError_t trace_init();
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);
