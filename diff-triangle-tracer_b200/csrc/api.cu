@@ -107,7 +107,8 @@ long long cache_pool_cap(int k, long long rays, size_t bytes) {
 int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P, const float* cols = nullptr) {
   if (cols && !shs) return TT_OK;  // precomputed colours in place of SH
   TT_REQUIRE(h, deg >= 0 && deg <= 3, "sh_degree must be in [0, 3]");
-  TT_REQUIRE(h, M >= (deg + 1) * (deg + 1), "shs has fewer coefficients per triangle than sh_degree needs");
+  // an empty scene reads no SH
+  TT_REQUIRE(h, P == 0 || M >= (deg + 1) * (deg + 1), "shs has fewer coefficients per triangle than sh_degree needs");
   TT_REQUIRE(h, P == 0 || shs != nullptr, "shs is empty and no colors_precomp was given");
   return TT_OK;
 }
