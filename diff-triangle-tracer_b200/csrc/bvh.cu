@@ -12,6 +12,7 @@
 //              leaves (a contiguous run of Morton-ordered records)
 //   boxes      each wide node's 8 child boxes from the binary boxes
 // A refit re-runs prep/records/bottom-up/boxes over the same topology.
+#include <cstddef>
 #include <cstdio>
 
 #include <cstring>
@@ -602,18 +603,25 @@ cudaError_t Bvh::refit(const float* verts, const int* cumsum, int P, cudaStream_
   return boxes(s);
 }
 
+// BVH blob: the topology only. Every box (binary nodes' lo/hi, the wide
+// nodes' 12 child-box words) is recomputed by the refit that follows a load,
+// so a blob holds the Morton permutation, the binary nodes' child/range
+// fields, the parent links, the wide slots' binary sources and the wide
+// nodes' child references: 28 bytes per triangle + 64 per wide node.
 namespace {
 struct BlobHeader {
-  char magic[8];  // "TTBVH\0\0\1"
+  char magic[8];  // "TTBVH\0\0\2"
   int P, nw;      // triangles, wide nodes
   long long pad;
 };
-constexpr char kBlobMagic[8] = {'T', 'T', 'B', 'V', 'H', 0, 0, 1};
+constexpr char kBlobMagic[8] = {'T', 'T', 'B', 'V', 'H', 0, 0, 2};
+constexpr size_t kBinTopoOff = offsetof(BinNode, left), kBinTopoBytes = sizeof(BinNode) - kBinTopoOff;
+constexpr size_t kWideRefOff = 12 * sizeof(float4), kWideRefBytes = (kNodeF4 - 12) * sizeof(float4);
 
 size_t blob_bytes(int P, int nw) {
   const size_t p = (size_t)P, b = P > 1 ? (size_t)P - 1 : 1;
-  return sizeof(BlobHeader) + p * 4 + b * sizeof(BinNode) + b * 4 + p * 4 + (size_t)nw * kWide * 4 +
-         (size_t)nw * kNodeF4 * sizeof(float4);
+  return sizeof(BlobHeader) + p * 4 + b * kBinTopoBytes + b * 4 + p * 4 + (size_t)nw * kWide * 4 +
+         (size_t)nw * kWideRefBytes;
 }
 }  // namespace
 
@@ -643,12 +651,19 @@ cudaError_t Bvh::save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s)
     if (e == cudaSuccess) e = cudaMemcpyAsync(o, buf.p, n, cudaMemcpyDeviceToHost, s);
     o += n;
   };
+  // rows of `width` bytes at `off` within records of `pitch` bytes
+  auto d2h_rows = [&](const DevBuf& buf, size_t off, size_t width, size_t pitch, size_t rows) {
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(o, width, static_cast<const char*>(buf.p) + off, pitch, width, rows,
+                            cudaMemcpyDeviceToHost, s);
+    o += width * rows;
+  };
   d2h(vals_, p * 4);
-  d2h(bnode_, b * sizeof(BinNode));
+  d2h_rows(bnode_, kBinTopoOff, kBinTopoBytes, sizeof(BinNode), b);
   d2h(bparent_, b * 4);
   d2h(lparent_, p * 4);
   d2h(wsrc_, (size_t)nw * kWide * 4);
-  d2h(wnodes_, (size_t)nw * kNodeF4 * sizeof(float4));
+  d2h_rows(wnodes_, kWideRefOff, kWideRefBytes, kNodeF4 * sizeof(float4), (size_t)nw);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return e;
 }
@@ -671,12 +686,18 @@ int Bvh::load(const void* src, size_t bytes, const float* verts, const int* cums
     if (e == cudaSuccess) e = cudaMemcpyAsync(buf.p, in, n, cudaMemcpyHostToDevice, s);
     in += n;
   };
+  auto h2d_rows = [&](DevBuf& buf, size_t off, size_t width, size_t pitch, size_t rows) {
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(static_cast<char*>(buf.p) + off, pitch, in, width, width, rows, cudaMemcpyHostToDevice,
+                            s);
+    in += width * rows;
+  };
   h2d(vals_, p * 4);
-  h2d(bnode_, b * sizeof(BinNode));
+  h2d_rows(bnode_, kBinTopoOff, kBinTopoBytes, sizeof(BinNode), b);
   h2d(bparent_, b * 4);
   h2d(lparent_, p * 4);
   h2d(wsrc_, (size_t)hd.nw * kWide * 4);
-  h2d(wnodes_, (size_t)hd.nw * kNodeF4 * sizeof(float4));
+  h2d_rows(wnodes_, kWideRefOff, kWideRefBytes, kNodeF4 * sizeof(float4), (size_t)hd.nw);
   const int cnt[4] = {hd.nw, 0, 0, 0};
   if (e == cudaSuccess) e = cudaMemcpyAsync(counters_.p, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s);
   // the host blob and cnt may go away on return
