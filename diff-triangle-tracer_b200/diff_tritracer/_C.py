@@ -134,9 +134,11 @@ class OptixTracer:
         written to `path` when given). No reference counterpart."""
         n = ctypes.c_ulonglong(0)
         check(self._h, lib.tt_bvh_save(self._h, None, 0, ctypes.byref(n), _stream()))
-        buf = ctypes.create_string_buffer(n.value)
-        check(self._h, lib.tt_bvh_save(self._h, buf, n.value, ctypes.byref(n), _stream()))
-        blob = buf.raw[:n.value]
+        out = bytearray(n.value)
+        if n.value:
+            check(self._h, lib.tt_bvh_save(self._h, (ctypes.c_char * n.value).from_buffer(out), n.value,
+                                           ctypes.byref(n), _stream()))
+        blob = bytes(out)
         if path is not None:
             with open(path, "wb") as f:
                 f.write(blob)
@@ -152,9 +154,10 @@ class OptixTracer:
                 blob = f.read()
         verts = _f32(triangles_points, "triangles_points", self.device)
         cumsum = _i32(cumsum_of_points_per_triangle, "cumsum_of_points_per_triangle", self.device)
-        buf = ctypes.create_string_buffer(bytes(blob), len(blob))
-        check(self._h, lib.tt_bvh_load(self._h, buf, len(blob), _ptr(verts), verts.numel() // 3, _ptr(cumsum),
-                                       int(number_of_points), _stream()))
+        # the C side only reads the blob: pass the bytes object's own storage
+        src = ctypes.c_char_p(bytes(blob) if isinstance(blob, bytearray) else blob)
+        check(self._h, lib.tt_bvh_load(self._h, ctypes.cast(src, ctypes.c_void_p), len(blob), _ptr(verts),
+                                       verts.numel() // 3, _ptr(cumsum), int(number_of_points), _stream()))
         self._keep = (verts, cumsum)
 
     def new_hit_cache(self, rays, k=None, pool=None):
