@@ -480,6 +480,7 @@ int tt_device_status(tt_tracer* h, void* stream) {
   TT_CUDA(h, cudaMemcpyAsync(&st, h->scratch.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
   TT_CUDA(h, cudaStreamSynchronize(s));
   TT_CUDA(h, cudaMemsetAsync(h->scratch.as<int>() + 1, 0, sizeof(int), s));
+  if (st & tt::kStatusBounds) return fail(h, TT_ERR_BOUNDS, "a device index check failed (TT_BOUNDS_CHECK build)");
   if (st & tt::kStatusStack) return fail(h, TT_ERR_STACK, "traversal stack overflow made no progress on some ray");
   if (st & tt::kStatusTimeout) return fail(h, TT_ERR_TIMEOUT, "a bounded device loop gave up");
   return TT_OK;

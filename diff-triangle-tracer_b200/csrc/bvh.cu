@@ -727,6 +727,7 @@ BvhView Bvh::view() const {
   v.tri_prim = tri_prim_.as<float4>();
   v.P = P_;
   v.has_root = (built_ && P_ > 0) ? 1 : 0;
+  v.wide_cap = P_ > 1 ? P_ - 1 : 1;
   return v;
 }
 
@@ -823,6 +824,7 @@ BvhView bvh_storage_view(const BvhStorage& st, int P) {
   v.tri_prim = st.tri_prim;
   v.P = P;
   v.has_root = P > 0 ? 1 : 0;
+  v.wide_cap = P > 1 ? P - 1 : 1;
   return v;
 }
 

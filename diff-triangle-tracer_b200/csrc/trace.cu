@@ -173,6 +173,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
     if ((sp < SD ? st.tn[sp * st.stride] : xtn[sp - SD]) > tmax) continue;
     if (ref_is_leaf(ref)) {
       const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
+      if (!TT_IN_BOUNDS(status, first + ntri <= (uint32_t)bvh.P)) continue;
       cnt.tris += ntri;
       for (uint32_t j = 0; j < ntri; ++j) {
         const float4* tr = bvh.tris + 3 * (size_t)(first + j);
@@ -188,6 +189,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
       }
       continue;
     }
+    if (!TT_IN_BOUNDS(status, ref < (uint32_t)bvh.wide_cap)) continue;
     ++cnt.nodes;
     const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
     float tn[8], tf[8];
@@ -290,6 +292,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     const unsigned m = ws.mask[sp] & __ballot_sync(full, tmax >= emin);
     __syncwarp();
     if (m == 0) continue;
+    if (!TT_IN_BOUNDS(status, ref < (uint32_t)bvh.wide_cap)) continue;  // ref is the same in every lane
     const bool on = (m >> lane) & 1u;
     if (on) ++cnt.nodes;
     if (lane == 0) ++cnt.warp_nodes;
@@ -320,6 +323,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
       const uint32_t lref = __shfl_sync(full, my_ref, lc);
       const bool lon = (__shfl_sync(full, mymask, lc) >> lane) & 1u;
       const uint32_t first = leaf_first(lref), ntri = leaf_count(lref);
+      if (!TT_IN_BOUNDS(status, first + ntri <= (uint32_t)bvh.P)) continue;  // the same in every lane
       if (lon) cnt.tris += ntri;
       with_perm(wperm, r, [&](const auto& pm) {
         for (uint32_t j = 0; j < ntri; ++j) {
@@ -348,7 +352,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     for (int c = 0; c < 8; ++c) rank += __shfl_sync(full, key, c) < key ? 1 : 0;
     const int avail = kWarpStack - sp;
     const int npush = nh < avail ? nh : avail;
-    if (pmask != 0u && rank < npush) {
+    if (pmask != 0u && rank < npush && TT_IN_BOUNDS(status, sp + npush - 1 - rank < kWarpStack)) {
       const int pos = sp + npush - 1 - rank;  // nearest on top
       ws.ref[pos] = my_ref;
       ws.mask[pos] = pmask;
@@ -651,6 +655,7 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
     // fmaxf(last + STEP_EPSILON, t) with the sum in double (forward.cu:111)
     cur.last_hit_t = fmaxf(__double2float_rn(__dadd_rn((double)cur.last_hit_t, kStepEps)), t);
     ++cur.ref_pos;
+    if (!TT_IN_BOUNDS(status, key_prim(key) < (uint32_t)sh.p.bvh.P)) return true;
     if (t >= kNear && sh.visit(key_prim(key), t)) return true;
     if (cur.ref_pos == kChunk) {
       // the reference's next optixTrace starts at last_hit_t

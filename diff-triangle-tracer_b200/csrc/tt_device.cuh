@@ -29,6 +29,16 @@ constexpr int kMaxWideLevels = 72;  // > 64-bit key depth of the binary tree
 // device status bits (tt_device_status)
 constexpr int kStatusTimeout = 1;
 constexpr int kStatusStack = 2;
+constexpr int kStatusBounds = 4;
+
+// Debug builds (-DTT_BOUNDS_CHECK, `make bounds`): device index checks that
+// record a violation in the status word and let the caller skip the access,
+// instead of faulting. In normal builds the check is the constant true.
+#ifdef TT_BOUNDS_CHECK
+#define TT_IN_BOUNDS(status, cond) ((cond) ? true : (atomicOr((status), kStatusBounds), false))
+#else
+#define TT_IN_BOUNDS(status, cond) true
+#endif
 
 // Empty k-buffer slot: larger than every (t, id) key with t <= far.
 constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
@@ -52,6 +62,7 @@ struct BvhView {
   const float4* tri_prim;  // primitive-ordered triangle records
   int P;
   int has_root;
+  int wide_cap;  // wide nodes the node array holds (index bound)
 };
 
 // ---------------------------------------------------------------- key order

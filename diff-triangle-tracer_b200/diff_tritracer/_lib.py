@@ -10,7 +10,9 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libtritracer.so")
+# TRITRACER_LIB selects another build of the library, e.g. the index-checked
+# libtritracer_bounds.so (`make bounds`)
+LIB_PATH = os.environ.get("TRITRACER_LIB") or os.path.join(_HERE, "libtritracer.so")
 
 TT_OK = 0
 TT_ERR_INVALID = 1

@@ -40,6 +40,7 @@ extern "C" {
 #define TT_ERR_CUDA 5    /* CUDA runtime error */
 #define TT_ERR_STATE 6   /* call order (e.g. trace before any BVH build) */
 #define TT_ERR_TOO_LARGE 7 /* more triangles than tt_forward_noalloc's fixed capacity */
+#define TT_ERR_BOUNDS 8  /* a device index check failed (library built with TT_BOUNDS_CHECK) */
 
 /* Which raygen program the forward pass runs: the reference selects one by
  * the PTX file handed to OptixTracer (tritracer/pipeline.cpp:289-296). */
@@ -277,8 +278,8 @@ int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream
 const char* tt_last_error(const tt_tracer* h);
 
 /* Synchronises `stream` and returns the device-side status word of the
- * handle's kernels since the last call (TT_OK, TT_ERR_TIMEOUT or
- * TT_ERR_STACK), then clears it. No reference counterpart: the reference's
+ * handle's kernels since the last call (TT_OK, TT_ERR_TIMEOUT, TT_ERR_STACK
+ * or, in a TT_BOUNDS_CHECK build, TT_ERR_BOUNDS), then clears it. No reference counterpart: the reference's
  * device code has no bounded loops to report on. */
 int tt_device_status(tt_tracer* h, void* stream);
 
