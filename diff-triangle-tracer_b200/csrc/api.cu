@@ -911,8 +911,9 @@ int tt_bvh_load(tt_tracer* h, const void* src, unsigned long long bytes, const f
   TT_REQUIRE(h, src && vertices && cumsum && P > 0 && num_vertices >= 3, "need a blob, vertices and cumsum");
   cudaError_t e = cudaSuccess;
   ++h->bvh_gen;
-  if (h->bvh.load(src, (size_t)bytes, vertices, cumsum, P, as_stream(stream), &e) != 0)
-    return fail(h, TT_ERR_INVALID, "not a BVH blob for this triangle count");
+  const int bad = h->bvh.load(src, (size_t)bytes, vertices, cumsum, P, as_stream(stream), &e);
+  if (bad == 1) return fail(h, TT_ERR_INVALID, "not a BVH blob for this triangle count");
+  if (bad == 2) return fail(h, TT_ERR_INVALID, "corrupted BVH blob: an index or link is out of place");
   if (e != cudaSuccess) return cuda_fail(h, e, "bvh load");
   return TT_OK;
 }

@@ -16,6 +16,7 @@
 #include <cstdio>
 
 #include <cstring>
+#include <vector>
 
 #include "bvh.cuh"
 
@@ -623,6 +624,71 @@ size_t blob_bytes(int P, int nw) {
   return sizeof(BlobHeader) + p * 4 + b * kBinTopoBytes + b * 4 + p * 4 + (size_t)nw * kWide * 4 +
          (size_t)nw * kWideRefBytes;
 }
+
+// Host check of a blob's contents before anything reaches the device: every
+// index in range, the Morton order a permutation, the binary hierarchy a
+// tree rooted at node 0 whose parent links match its child links (the
+// refit's bottom-up pass walks them), and every wide child reference
+// pointing to a later wide node (so the wide hierarchy has no cycle).
+bool blob_contents_valid(const char* in, int P, int nw) {
+  const size_t p = (size_t)P, b = P > 1 ? (size_t)P - 1 : 1;
+  const uint32_t* vals = reinterpret_cast<const uint32_t*>(in);
+  const int* topo = reinterpret_cast<const int*>(in + p * 4);  // left, right, first, last per binary node
+  const int* bparent = reinterpret_cast<const int*>(in + p * 4 + b * kBinTopoBytes);
+  const int* lparent = bparent + b;
+  const int* wsrc = lparent + p;
+  const uint32_t* wref = reinterpret_cast<const uint32_t*>(wsrc + (size_t)nw * kWide);
+  std::vector<char> seen(p, 0);
+  for (size_t i = 0; i < p; ++i) {
+    if (vals[i] >= (uint32_t)P || seen[vals[i]]) return false;
+    seen[vals[i]] = 1;
+  }
+  if (P >= 2) {
+    const int nb = P - 1;
+    std::vector<char> leaf_seen(p, 0), node_seen(b, 0);
+    std::vector<int> todo{0};
+    if (bparent[0] != -1) return false;
+    int nodes = 0, leaves = 0;
+    while (!todo.empty()) {
+      const int n = todo.back();
+      todo.pop_back();
+      if (node_seen[n]) return false;
+      node_seen[n] = 1;
+      ++nodes;
+      const int* t = topo + 4 * (size_t)n;
+      if (t[2] < 0 || t[3] >= P || t[2] >= t[3]) return false;
+      for (int c = 0; c < 2; ++c) {
+        const int ch = t[c];
+        if (ch >= 0) {
+          if (ch >= nb || bparent[ch] != n) return false;
+          todo.push_back(ch);
+        } else {
+          const int l = ~ch;
+          if (l >= P || leaf_seen[l] || lparent[l] != n) return false;
+          leaf_seen[l] = 1;
+          ++leaves;
+        }
+      }
+    }
+    if (nodes != nb || leaves != P) return false;
+  }
+  for (size_t i = 0; i < (size_t)nw * kWide; ++i) {
+    const int v = wsrc[i];
+    if (v != (int)0x80000000 && !(v >= 0 && v < (P > 1 ? P - 1 : 0)) && !(v < 0 && ~v < P)) return false;
+  }
+  for (size_t w = 0; w < (size_t)nw; ++w) {
+    for (int i = 0; i < kWide; ++i) {
+      const uint32_t r = wref[w * kWide + i];
+      if (r == kEmptyRef) continue;
+      if (ref_is_leaf(r)) {
+        if (leaf_count(r) > (uint32_t)kLeafMax || leaf_first(r) + leaf_count(r) > (uint32_t)P) return false;
+      } else if (r <= w || r >= (uint32_t)nw) {
+        return false;
+      }
+    }
+  }
+  return true;
+}
 }  // namespace
 
 cudaError_t Bvh::save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s) {
@@ -677,6 +743,7 @@ int Bvh::load(const void* src, size_t bytes, const float* verts, const int* cums
   if (std::memcmp(hd.magic, kBlobMagic, 8) != 0 || hd.P != P || P <= 0 || hd.nw < 1 ||
       hd.nw > (P > 1 ? P - 1 : 1) || bytes != blob_bytes(P, hd.nw))
     return 1;
+  if (!blob_contents_valid(static_cast<const char*>(src) + sizeof(hd), P, hd.nw)) return 2;
   built_ = false;
   if ((*err = reserve(P)) != cudaSuccess) return 0;
   const size_t p = (size_t)P, b = P > 1 ? (size_t)P - 1 : 1;
