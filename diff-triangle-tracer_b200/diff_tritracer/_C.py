@@ -93,6 +93,8 @@ class OptixTracer:
         self.variant = _VARIANTS[forward]
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.use_hit_cache = False  # set by diff_tritracer.Tracer (its autograd path passes a hit cache)
+        self._pool_frac = 0.25  # autograd hit caches: pool size as a fraction of the rays (observe_hit_cache)
+        self._cache_calls = 0
         cfg = _lib.TtConfig()
         cfg.variant = self.variant
         cfg.tmin_inclusive = 1 if tmin_inclusive else 0
@@ -199,6 +201,25 @@ class OptixTracer:
             a.ray_o, a.ray_d = _ptr(ro), _ptr(rd)
         check(self._h, lib.tt_camera_rays(self._h, arr, len(cams), _stream()))
         return outputs
+
+    def autograd_hit_cache(self, rays):
+        """The autograd module's hit cache for one forward: its pool holds the
+        fraction of the rays that earlier forwards' later queries needed
+        (observe_hit_cache), a quarter at first."""
+        return self.new_hit_cache(rays, pool=max(int(self._pool_frac * rays), 1))
+
+    def observe_hit_cache(self, hit_cache, rays):
+        """After the first two autograd forwards, and every 1024th after that,
+        reads how many later queries the pool was asked for (one stream
+        synchronisation) and grows the pool fraction when they did not fit.
+        The calls in between read nothing."""
+        n = self._cache_calls
+        self._cache_calls += 1
+        if n >= 2 and n % 1024:
+            return
+        use = self.hit_cache_usage(hit_cache)
+        if use["pool_used"] > use["pool_cap"]:
+            self._pool_frac = max(self._pool_frac, 1.25 * use["pool_used"] / max(int(rays), 1))
 
     def hit_cache_usage(self, hit_cache):
         """The header of a hit cache a forward has filled (synchronises the

@@ -60,10 +60,13 @@ class _Tracer(torch.autograd.Function):
                 st.extra_params, st.rebuild_gas, st.debug)
         # every ray's first hit query, kept for the adjoint like an activation
         cache = None
-        if tracer.use_hit_cache and tracer.variant == _C._lib.TT_VARIANT_PLAIN and ray_o.dim() >= 2:
-            cache = tracer.new_hit_cache(int(ray_o.shape[0]) * int(ray_o.shape[1]))
+        rays = int(ray_o.shape[0]) * int(ray_o.shape[1]) if ray_o.dim() >= 2 else 0
+        if tracer.use_hit_cache and tracer.variant == _C._lib.TT_VARIANT_PLAIN and rays:
+            cache = tracer.autograd_hit_cache(rays)
         fwd = tracer.trace_forward if cache is None else (lambda *a: tracer.trace_forward(*a, hit_cache=cache))
         res = _call_with_snapshot(fwd, args, st.debug, "snapshot_fw.dump", "forward")
+        if cache is not None:
+            tracer.observe_hit_cache(cache, rays)  # sizes the next forwards' pools
         color, others, gpu_time, scaling, density_factor, max_blending = res.data
         ctx.hit_cache = cache
         ctx.tracer_settings = st

@@ -209,3 +209,25 @@ def test_usage_reports_pool_capacity_and_demand(setup):
     assert use["pool_cap"] == 0 and 0 < use["pool_used"] <= queries - R
     _, n = backward(tr, sc, s, ro, rd, *forward(tr, sc, s, ro, rd, none, rebuild=2), g, go, none)
     assert n == R
+
+
+def test_autograd_pool_grows_to_the_later_queries(setup):
+    """The autograd module starts with a pool of a quarter of the rays, reads
+    what its first forwards asked for and sizes later pools to fit: from the
+    third step on the adjoint replays every query."""
+    sc, s, ro, rd, g, go = setup
+    tracer = diff_tritracer.Tracer("forward.ptx", "backward.ptx")
+    tracer.tracer.set_traversal("packets", k=16)
+    opac = s["opac"].clone().requires_grad_(True)
+    seen = []
+    for _ in range(3):
+        tracer.tracer.reset_stats()
+        out = tracer(ro, rd, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, opac,
+                     torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), s["shs"], None, settings())
+        (out[0] * g).sum().backward()
+        torch.cuda.synchronize()
+        tracer.tracer.device_status()
+        st = tracer.tracer.stats()
+        seen.append((st["hit_cache_replays"], st["queries"]))
+    assert seen[0][0] < seen[0][1], seen  # the quarter-of-the-rays pool did not hold every later query
+    assert seen[2][0] == seen[2][1], seen
