@@ -46,22 +46,39 @@ def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int
         best = cache[full_key]
         tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
         return best
-    timings = []
-    for cand in CANDIDATES:
-        tracer.set_traversal(cand["traversal"], cand["k"], cand["stack_depth"])
+    name = lambda c: f"{c['traversal']}/k{c['k']}/s{c['stack_depth']}"  # noqa: E731
+
+    def apply(c):
+        tracer.set_traversal(c["traversal"], c["k"], c["stack_depth"])
         if prepare is not None:
             prepare()
-        step()  # warm-up
-        start = torch.cuda.Event(enable_timing=True)
-        end = torch.cuda.Event(enable_timing=True)
-        start.record()
-        for _ in range(iters):
-            step()
-        end.record()
-        torch.cuda.synchronize()
-        timings.append((start.elapsed_time(end) / iters, cand))
+        step()  # untimed: first launches, allocations of this configuration
+
+    # An untimed pass over every candidate first: in a fresh process the
+    # candidates timed first otherwise read slow (kernels loaded on first
+    # launch, clocks leaving idle); one C2 run timed packets k = 32 at
+    # 29.6 ms a step in second place against 23.5 ms in its timed loop.
+    for cand in CANDIDATES:
+        apply(cand)
+    torch.cuda.synchronize()
+    # then two timed rounds in opposite orders; each candidate keeps its
+    # faster round
+    best_ms = {}
+    for order in (CANDIDATES, CANDIDATES[::-1]):
+        for cand in order:
+            apply(cand)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(iters):
+                step()
+            end.record()
+            torch.cuda.synchronize()
+            ms = start.elapsed_time(end) / iters
+            best_ms[name(cand)] = min(best_ms.get(name(cand), float("inf")), ms)
+    timings = [(best_ms[name(c)], c) for c in CANDIDATES]
     ms, best = min(timings, key=lambda x: x[0])
-    best = dict(best, ms=ms, all={f"{c['traversal']}/k{c['k']}/s{c['stack_depth']}": t for t, c in timings})
+    best = dict(best, ms=ms, all={name(c): t for t, c in timings})
     tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
     cache[full_key] = best
     os.makedirs(os.path.dirname(cache_path), exist_ok=True)
