@@ -81,9 +81,19 @@ def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int
     best = dict(best, ms=ms, all={name(c): t for t, c in timings})
     tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
     cache[full_key] = best
-    os.makedirs(os.path.dirname(cache_path), exist_ok=True)
-    tmp = cache_path + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(cache, f, indent=1)
-    os.replace(tmp, cache_path)
+    _store(cache_path, cache)
     return best
+
+
+def _store(cache_path, cache):
+    """Writes the cache through a temporary file of this process: ranks of a
+    multi-GPU run tune at the same time and write the same cache. The cache
+    is only a shortcut, so a failed write is not an error."""
+    tmp = f"{cache_path}.{os.getpid()}.tmp"
+    try:
+        os.makedirs(os.path.dirname(cache_path) or ".", exist_ok=True)
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1)
+        os.replace(tmp, cache_path)
+    except OSError:
+        pass
