@@ -12,6 +12,7 @@
 //              leaves (a contiguous run of Morton-ordered records)
 //   boxes      each wide node's 8 child boxes from the binary boxes
 // A refit re-runs prep/records/bottom-up/boxes over the same topology.
+#include <algorithm>
 #include <cstddef>
 #include <cstdio>
 
@@ -717,11 +718,16 @@ cudaError_t Bvh::save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s)
     if (e == cudaSuccess) e = cudaMemcpyAsync(o, buf.p, n, cudaMemcpyDeviceToHost, s);
     o += n;
   };
-  // rows of `width` bytes at `off` within records of `pitch` bytes
+  // rows of `width` bytes at `off` within records of `pitch` bytes: packed on
+  // the device first (a strided copy into pageable host memory goes row by row)
+  void* pack = nullptr;
+  const size_t pack_bytes = std::max(b * kBinTopoBytes, (size_t)nw * kWideRefBytes);
+  if ((e = cudaMallocAsync(&pack, pack_bytes, s)) != cudaSuccess) return e;
   auto d2h_rows = [&](const DevBuf& buf, size_t off, size_t width, size_t pitch, size_t rows) {
     if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(o, width, static_cast<const char*>(buf.p) + off, pitch, width, rows,
-                            cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpy2DAsync(pack, width, static_cast<const char*>(buf.p) + off, pitch, width, rows,
+                            cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(o, pack, width * rows, cudaMemcpyDeviceToHost, s);
     o += width * rows;
   };
   d2h(vals_, p * 4);
@@ -730,6 +736,8 @@ cudaError_t Bvh::save(void* dst, size_t capacity, size_t* bytes, cudaStream_t s)
   d2h(lparent_, p * 4);
   d2h(wsrc_, (size_t)nw * kWide * 4);
   d2h_rows(wnodes_, kWideRefOff, kWideRefBytes, kNodeF4 * sizeof(float4), (size_t)nw);
+  const cudaError_t ef = cudaFreeAsync(pack, s);
+  if (e == cudaSuccess) e = ef;
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return e;
 }
@@ -753,6 +761,8 @@ int Bvh::load(const void* src, size_t bytes, const float* verts, const int* cums
     if (e == cudaSuccess) e = cudaMemcpyAsync(buf.p, in, n, cudaMemcpyHostToDevice, s);
     in += n;
   };
+  // (uploads into strided destinations go straight from the host: measured
+  // faster than staging them on the device, unlike the downloads of save)
   auto h2d_rows = [&](DevBuf& buf, size_t off, size_t width, size_t pitch, size_t rows) {
     if (e == cudaSuccess)
       e = cudaMemcpy2DAsync(static_cast<char*>(buf.p) + off, pitch, in, width, width, rows, cudaMemcpyHostToDevice,
