@@ -44,9 +44,25 @@ WORKLOADS = {
 C4_SIDES = (256, 512, 768, 1024)
 
 
+def scenes_module():
+    """The seeded scene generator (diff_tritracer/scenes.py), loaded from its
+    file. It needs only numpy; importing it through the package would run the
+    package's __init__, which loads the tracer library, and the reference arm
+    must not map that library."""
+    import importlib.util
+
+    name = "_tt_bench_scenes"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(PKG, "diff_tritracer", "scenes.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def c4_views(seed=0):
     """16 cameras on the radius-3 sphere, side lengths drawn from {256, 512, 768, 1024}."""
-    from diff_tritracer import scenes
+    scenes = scenes_module()
 
     rng = np.random.default_rng(seed + 4)
     sides = rng.choice(C4_SIDES, size=16)
@@ -55,7 +71,7 @@ def c4_views(seed=0):
 
 
 def make_workload(name, seed=0):
-    from diff_tritracer import scenes
+    scenes = scenes_module()
 
     P, views, H, W = WORKLOADS[name]
     sc = scenes.make_scene(P, seed=seed)
@@ -146,18 +162,30 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_run(runner, sc, ro, rd, g, go, rows, nthreads):
-    """One forward + backward of the CPU implementation over `rows` of the image."""
-    H, W = ro.shape[:2]
-    f = runner.forward(sc, ro, rd, nthreads=nthreads, rows=rows)
-    runner.backward(sc, ro, rd, f.color, f.others, g, go, nthreads=nthreads, rows=rows)
+def sample_rows(H, n):
+    """n rows spread evenly over all H rows of the stacked views (every view
+    contributes in proportion to its height)."""
+    n = int(max(1, min(H, n)))
+    return (np.arange(n, dtype=np.int64) * H) // n + (H // n) // 2
+
+
+def row_sample(ro, rd, g, go, idx):
+    """The rays and upstream gradients of the sampled rows, as one image."""
+    c = np.ascontiguousarray
+    return c(ro[idx]), c(rd[idx]), c(g[:, idx]), c(go[:, idx])
+
+
+def cpu_run(runner, sc, sample, nthreads):
+    """One forward + backward of the CPU implementation over a row sample."""
+    ro, rd, g, go = sample
+    f = runner.forward(sc, ro, rd, nthreads=nthreads)
+    runner.backward(sc, ro, rd, f.color, f.others, g, go, nthreads=nthreads)
 
 
 def cpu_baseline(name, sc, ro, rd, g, go, budget_s=12.0):
     """Times the reference's own per-ray code built for the host (oracle/_ref)
     if it was built, else the oracle's FP32 port, on all host cores, over a
-    bounded band of rows of the stacked views (centred on the first view's
-    middle row)."""
+    bounded sample of rows spread evenly across all stacked views."""
     from oracle import pyoracle
 
     if pyoracle.reference_available():
@@ -171,36 +199,33 @@ def cpu_baseline(name, sc, ro, rd, g, go, budget_s=12.0):
     runner._scene(sc)  # CPU BVH over the same triangles (not timed)
     build_s = time.time() - t0
 
-    def band(n):  # n rows centred on view 0's middle row, inside the stacked views
-        n = int(max(1, min(H, n)))
-        start = max(0, min(view_h // 2 - n // 2, H - n))
-        return (start, start + n)
-
     # the host code deals whole rows to its threads in turn: the probe gives
-    # every thread two rows, and the band is rescaled until it fills at least
-    # half the budget (or covers every view)
-    rows = band(2 * nthreads)
+    # every thread two rows, and the sample is rescaled until it fills at
+    # least half the budget (or holds every row)
+    n = 2 * nthreads
     for _ in range(3):
+        sample = row_sample(ro, rd, g, go, sample_rows(H, n))
         t0 = time.time()
-        cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+        cpu_run(runner, sc, sample, nthreads)
         dt = max(time.time() - t0, 1e-3)
-        n = rows[1] - rows[0]
-        if dt >= 0.5 * budget_s or n == H:
+        if dt >= 0.5 * budget_s or n >= H:
             break
-        rows = band(n * budget_s / dt)
+        n = int(min(H, n * budget_s / dt))
+    n = sample[0].shape[0]
     reps = 1
-    if dt < 0.5 * budget_s:  # every view is in the band: repeat whole passes
+    if dt < 0.5 * budget_s:  # every row is in the sample: repeat whole passes
         reps = int(np.ceil(budget_s / dt))
         t0 = time.time()
         for _ in range(reps):
-            cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+            cpu_run(runner, sc, sample, nthreads)
         dt = time.time() - t0
-    nrays = (rows[1] - rows[0]) * W
+    nrays = n * W
     runner.close()
     return {"value": reps * nrays / dt / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": kind,
-            "sample": f"rows {rows[0]}..{rows[1] - 1} of the {H // view_h} stacked {view_h}-row views "
-                      f"({nrays} rays, fwd+bwd) x {reps}, {dt:.1f} s; CPU BVH build {build_s:.1f} s untimed"}, \
-        runner, kind, nthreads, rows
+            "sample": f"{n} of the {H} rows of the {H // view_h} stacked {view_h}-row views, spread evenly "
+                      f"over all views ({nrays} rays, fwd+bwd) x {reps}, {dt:.1f} s; CPU BVH build "
+                      f"{build_s:.1f} s untimed"}, \
+        runner, kind, nthreads, sample
 
 
 def slowest_rank_ms(ms, world, dev):
@@ -222,19 +247,19 @@ def reference_arm(args, rank):
         return
     name = args.workload
     sc, ro, rd, g, go = make_workload(name)
-    base, runner, kind, nthreads, rows = cpu_baseline(name, sc, ro, rd, g, go, budget_s=args.ref_budget)
+    base, runner, kind, nthreads, sample = cpu_baseline(name, sc, ro, rd, g, go, budget_s=args.ref_budget)
     from oracle import pyoracle
 
     runner = pyoracle.Reference() if kind == "reference" else pyoracle.Oracle()
     runner._scene(sc)
     for _ in range(args.warmup):
-        cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+        cpu_run(runner, sc, sample, nthreads)
     times = []
     for _ in range(args.steps):
         t0 = time.time()
-        cpu_run(runner, sc, ro, rd, g, go, rows, nthreads)
+        cpu_run(runner, sc, sample, nthreads)
         times.append(time.time() - t0)
-    nrays = (rows[1] - rows[0]) * ro.shape[1]
+    nrays = sample[0].shape[0] * sample[0].shape[1]
     total = sum(times)
     value = nrays * args.steps / total / 1e6
     P, views, H, W = WORKLOADS[name]
@@ -243,7 +268,9 @@ def reference_arm(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "triangles": P, "views": views, "H": H, "W": W,
-                   "sample_rays_per_step": nrays},
+                   "rays_per_step": views * H * W, "sample_rays_per_step": nrays,
+                   "sample": "rows spread evenly over all views of the workload; Mrays/s of the sample",
+                   "step": "forward + adjoint of the reference's per-ray code on the host cores"},
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": nthreads, "kind": kind,
                          "sample": base["sample"]},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
