@@ -341,14 +341,16 @@ __global__ void k_bottom_up(const float4* __restrict__ tri, int P, BinNode* bn, 
 }
 
 // ------------------------------------------------------------- collapse
+// counters: [0] wide nodes, [1] depth overflow flag, [2] level the collapse
+// is at, [3] wide nodes in the levels above it, [4] blocks of the current
+// k_collapse_big launch that finished
+constexpr int kCtrLevel = 2, kCtrBase = 3, kCtrDone = 4, kNumCounters = 8;
+
 __global__ void k_collapse_init(int P, int* levels, int* wbin, int* counters) {
   const int i = threadIdx.x;
   if (i < kMaxWideLevels + 1) levels[i] = (i == 0) ? 1 : 0;
-  if (i == 0) {
-    wbin[0] = (P >= 2) ? 0 : ~0;  // root: binary node 0, or the single leaf
-    counters[0] = 0;
-    counters[1] = 0;
-  }
+  if (i < kNumCounters) counters[i] = 0;
+  if (i == 0) wbin[0] = (P >= 2) ? 0 : ~0;  // root: binary node 0, or the single leaf
 }
 
 __device__ __forceinline__ float half_area(const BinNode* bn, int r) {
@@ -357,75 +359,129 @@ __device__ __forceinline__ float half_area(const BinNode* bn, int r) {
   return x * y + y * z + z * x;
 }
 
-__global__ void k_collapse_level(int level, const BinNode* __restrict__ bn, int* levels, int* wbin,
-                                 int* __restrict__ wsrc, float4* __restrict__ wnodes, int* counters) {
-  int base = 0;
-  for (int l = 0; l < level; ++l) base += levels[l];
-  const int cnt = levels[level];
-  const int next_base = base + cnt;
-  if (level == kMaxWideLevels - 1 && cnt > 0 && blockIdx.x == 0 && threadIdx.x == 0) counters[1] = 1;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
-    const int w = base + k;
-    const int b = wbin[w];
-    int slot[kWide];
-    int n;
-    if (b < 0) {
-      slot[0] = b;
-      n = 1;
-    } else {
-      slot[0] = bn[b].left;
-      slot[1] = bn[b].right;
-      n = 2;
-    }
-    while (n < kWide) {
-      int best = -1;
-      float best_a = -1.f;
-      for (int i = 0; i < n; ++i) {
-        const int r = slot[i];
-        if (r >= 0) {
-          const float a = half_area(bn, r);
-          if (a > best_a) {
-            best_a = a;
-            best = i;
-          }
+// Wide node w of `level` (its binary source in wbin[w]): opens the child of
+// largest surface area until 8 slots are filled, turns subtrees of at most
+// kLeafMax triangles into leaves and appends the others to the next level
+// (from index next_base on).
+__device__ __forceinline__ void collapse_node(int w, int level, int next_base, const BinNode* __restrict__ bn,
+                                              int* levels, int* wbin, int* __restrict__ wsrc,
+                                              float4* __restrict__ wnodes) {
+  const int b = wbin[w];
+  int slot[kWide];
+  int n;
+  if (b < 0) {
+    slot[0] = b;
+    n = 1;
+  } else {
+    slot[0] = bn[b].left;
+    slot[1] = bn[b].right;
+    n = 2;
+  }
+  while (n < kWide) {
+    int best = -1;
+    float best_a = -1.f;
+    for (int i = 0; i < n; ++i) {
+      const int r = slot[i];
+      if (r >= 0) {
+        const float a = half_area(bn, r);
+        if (a > best_a) {
+          best_a = a;
+          best = i;
         }
       }
-      if (best < 0) break;
-      const int r = slot[best];
-      slot[best] = bn[r].left;
-      slot[n++] = bn[r].right;
     }
-    uint32_t refs[kWide];
+    if (best < 0) break;
+    const int r = slot[best];
+    slot[best] = bn[r].left;
+    slot[n++] = bn[r].right;
+  }
+  uint32_t refs[kWide];
 #pragma unroll
-    for (int i = 0; i < kWide; ++i) {
-      uint32_t ref = kEmptyRef;
-      int src = (int)0x80000000;
-      if (i < n) {
-        const int r = slot[i];
-        src = r;
-        if (r < 0) {
-          ref = leaf_ref((uint32_t)~r, 1u);
+  for (int i = 0; i < kWide; ++i) {
+    uint32_t ref = kEmptyRef;
+    int src = (int)0x80000000;
+    if (i < n) {
+      const int r = slot[i];
+      src = r;
+      if (r < 0) {
+        ref = leaf_ref((uint32_t)~r, 1u);
+      } else {
+        const int first = bn[r].first, size = bn[r].last - first + 1;
+        if (size <= kLeafMax) {
+          ref = leaf_ref((uint32_t)first, (uint32_t)size);
         } else {
-          const int first = bn[r].first, size = bn[r].last - first + 1;
-          if (size <= kLeafMax) {
-            ref = leaf_ref((uint32_t)first, (uint32_t)size);
-          } else {
-            const int idx = next_base + atomicAdd(&levels[level + 1], 1);
-            wbin[idx] = r;
-            ref = (uint32_t)idx;
-          }
+          const int idx = next_base + atomicAdd(&levels[level + 1], 1);
+          wbin[idx] = r;
+          ref = (uint32_t)idx;
         }
       }
-      refs[i] = ref;
-      wsrc[(size_t)w * kWide + i] = src;
     }
-    float4* nd = wnodes + (size_t)w * kNodeF4;
-    nd[12] = make_float4(__uint_as_float(refs[0]), __uint_as_float(refs[1]), __uint_as_float(refs[2]),
-                         __uint_as_float(refs[3]));
-    nd[13] = make_float4(__uint_as_float(refs[4]), __uint_as_float(refs[5]), __uint_as_float(refs[6]),
-                         __uint_as_float(refs[7]));
+    refs[i] = ref;
+    wsrc[(size_t)w * kWide + i] = src;
+  }
+  float4* nd = wnodes + (size_t)w * kNodeF4;
+  nd[12] = make_float4(__uint_as_float(refs[0]), __uint_as_float(refs[1]), __uint_as_float(refs[2]),
+                       __uint_as_float(refs[3]));
+  nd[13] = make_float4(__uint_as_float(refs[4]), __uint_as_float(refs[5]), __uint_as_float(refs[6]),
+                       __uint_as_float(refs[7]));
+}
+
+// The top-down collapse runs level by level, and the host does not know the
+// tree's depth without a synchronisation. So the levels go through a fixed,
+// short sequence of launches that find their level on the device:
+// k_collapse_small (one block) takes consecutive levels of at most `limit`
+// nodes, with a block barrier between levels; each k_collapse_big (full
+// grid) takes one level of any size and its last block to finish moves the
+// level on; a final k_collapse_small with no limit takes whatever is left.
+__global__ void __launch_bounds__(1024) k_collapse_small(const BinNode* __restrict__ bn, int* levels, int* wbin,
+                                                         int* __restrict__ wsrc, float4* __restrict__ wnodes,
+                                                         int* counters, int limit) {
+  int level = counters[kCtrLevel], base = counters[kCtrBase];
+  while (level < kMaxWideLevels) {
+    const int cnt = *(volatile int*)&levels[level];
+    if (cnt == 0 || cnt > limit) break;
+    if (level == kMaxWideLevels - 1 && threadIdx.x == 0) counters[1] = 1;
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x)
+      collapse_node(base + k, level, base + cnt, bn, levels, wbin, wsrc, wnodes);
+    __syncthreads();  // the next level's count and sources are complete
+    base += cnt;
+    ++level;
+  }
+  if (threadIdx.x == 0) {
+    counters[kCtrLevel] = level;
+    counters[kCtrBase] = base;
   }
 }
+
+__global__ void k_collapse_big(const BinNode* __restrict__ bn, int* levels, int* wbin, int* __restrict__ wsrc,
+                               float4* __restrict__ wnodes, int* counters) {
+  // every block reads the level before any block can have finished: the
+  // last block moves it on only after all blocks have counted themselves out
+  const int level = *(volatile int*)&counters[kCtrLevel], base = *(volatile int*)&counters[kCtrBase];
+  const int cnt = level < kMaxWideLevels ? *(volatile int*)&levels[level] : 0;
+  if (level == kMaxWideLevels - 1 && cnt > 0 && blockIdx.x == 0 && threadIdx.x == 0) counters[1] = 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+    collapse_node(base + k, level, base + cnt, bn, levels, wbin, wsrc, wnodes);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int done = atomicAdd(&counters[kCtrDone], 1);
+    if (done == (int)gridDim.x - 1) {
+      counters[kCtrDone] = 0;
+      if (cnt > 0) {
+        counters[kCtrLevel] = level + 1;
+        counters[kCtrBase] = base + cnt;
+      }
+      __threadfence();
+    }
+  }
+}
+
+// Launches of k_collapse_big between the two k_collapse_small: the levels of
+// more than kSmallLevel nodes of a large scene (a 3M-triangle LBVH has about
+// 4), with room to spare; further ones fall to the final one-block pass.
+constexpr int kSmallLevel = 4096;
+__host__ __forceinline__ int collapse_big_launches(int P) { return P > 8 * kSmallLevel ? 8 : 0; }
 
 __global__ void k_collapse_total(const int* levels, int* counters) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -478,6 +534,18 @@ __global__ void k_wide_boxes(const int* __restrict__ wsrc, const BinNode* __rest
 
 inline int blocks_for(long long n) { return (int)((n + kBlock - 1) / kBlock); }
 
+cudaError_t launch_collapse(int P, const BinNode* bn, int* levels, int* wbin, int* wsrc, float4* wnodes,
+                            int* counters, cudaStream_t s) {
+  k_collapse_init<<<1, 128, 0, s>>>(P, levels, wbin, counters);
+  k_collapse_small<<<1, 1024, 0, s>>>(bn, levels, wbin, wsrc, wnodes, counters, kSmallLevel);
+  const int wcap = P > 1 ? P - 1 : 1;
+  const int grid = blocks_for(wcap) < 148 * 4 ? blocks_for(wcap) : 148 * 4;
+  for (int i = 0; i < collapse_big_launches(P); ++i)
+    k_collapse_big<<<grid, kBlock, 0, s>>>(bn, levels, wbin, wsrc, wnodes, counters);
+  k_collapse_small<<<1, 1024, 0, s>>>(bn, levels, wbin, wsrc, wnodes, counters, 0x7FFFFFFF);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t Bvh::reserve(int P) {
@@ -505,7 +573,7 @@ cudaError_t Bvh::reserve(int P) {
   TT_RES(wsrc_, wcap * kWide * 4);
   TT_RES(wbin_, wcap * 4);
   TT_RES(levels_, (kMaxWideLevels + 1) * 4);
-  TT_RES(counters_, 4 * 4);
+  TT_RES(counters_, kNumCounters * 4);
 #undef TT_RES
   cap_ = P;
   return cudaSuccess;
@@ -550,7 +618,7 @@ cudaError_t Bvh::build(const float* verts, const int* cumsum, int P, cudaStream_
   if (e != cudaSuccess) return e;
   if ((e = prep(verts, cumsum, P, true, s)) != cudaSuccess) return e;
   // morton + 4 x (hist, scan, scatter) + records + karras + bottom-up + collapse init/levels/total + boxes
-  launches_ += 1 + 12 + 1 + (P >= 2 ? 2 : 0) + 1 + kMaxWideLevels + 1 + 1;
+  launches_ += 1 + 12 + 1 + (P >= 2 ? 2 : 0) + 1 + (2 + collapse_big_launches(P)) + 1 + 1;
   k_morton<<<blocks_for(P), kBlock, 0, s>>>(centroid_.as<float4>(), bounds_.as<int>(), P, keys_.as<uint32_t>(),
                                             vals_.as<uint32_t>());
   // 30-bit keys: four 8-bit passes, ending back in keys_/vals_
@@ -579,12 +647,10 @@ cudaError_t Bvh::build(const float* verts, const int* cumsum, int P, cudaStream_
     k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(tri_sorted_.as<float4>(), P, bnode_.as<BinNode>(),
                                                  bparent_.as<int>(), lparent_.as<int>(), flags_.as<int>());
   }
-  k_collapse_init<<<1, 128, 0, s>>>(P, levels_.as<int>(), wbin_.as<int>(), counters_.as<int>());
+  if ((e = launch_collapse(P, bnode_.as<BinNode>(), levels_.as<int>(), wbin_.as<int>(), wsrc_.as<int>(),
+                           wnodes_.as<float4>(), counters_.as<int>(), s)) != cudaSuccess)
+    return e;
   const int wcap = P > 1 ? P - 1 : 1;
-  const int cgrid = blocks_for(wcap) < 148 * 4 ? blocks_for(wcap) : 148 * 4;
-  for (int level = 0; level < kMaxWideLevels; ++level)
-    k_collapse_level<<<cgrid, kBlock, 0, s>>>(level, bnode_.as<BinNode>(), levels_.as<int>(), wbin_.as<int>(),
-                                              wsrc_.as<int>(), wnodes_.as<float4>(), counters_.as<int>());
   k_collapse_total<<<1, 32, 0, s>>>(levels_.as<int>(), counters_.as<int>());
   const int grid = blocks_for(wcap) < 148 * 8 ? blocks_for(wcap) : 148 * 8;
   k_wide_boxes<<<grid, kBlock, 0, s>>>(wsrc_.as<int>(), bnode_.as<BinNode>(), tri_sorted_.as<float4>(),
@@ -846,7 +912,7 @@ BvhStorage carve(char* base, int P, size_t* total) {
   st.wsrc = c.take<int>(inner * kWide);
   st.wbin = c.take<int>(inner);
   st.levels = c.take<int>(kMaxWideLevels + 1);
-  st.counters = c.take<int>(4);
+  st.counters = c.take<int>(kNumCounters);
   if (total) *total = (c.off + 255) & ~size_t(255);
   return st;
 }
@@ -884,11 +950,9 @@ cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* 
     if ((e = cudaMemsetAsync(st.flags, 0, (size_t)(P - 1) * 4, s)) != cudaSuccess) return e;
     k_bottom_up<<<blocks_for(P), kBlock, 0, s>>>(st.tri_sorted, P, bn, st.bparent, st.lparent, st.flags);
   }
-  k_collapse_init<<<1, 128, 0, s>>>(P, st.levels, st.wbin, st.counters);
+  if ((e = launch_collapse(P, bn, st.levels, st.wbin, st.wsrc, st.wnodes, st.counters, s)) != cudaSuccess) return e;
   const int wcap = P > 1 ? P - 1 : 1;
   const int grid = blocks_for(wcap) < 148 * 4 ? blocks_for(wcap) : 148 * 4;
-  for (int level = 0; level < kMaxWideLevels; ++level)
-    k_collapse_level<<<grid, kBlock, 0, s>>>(level, bn, st.levels, st.wbin, st.wsrc, st.wnodes, st.counters);
   k_collapse_total<<<1, 32, 0, s>>>(st.levels, st.counters);
   k_wide_boxes<<<grid, kBlock, 0, s>>>(st.wsrc, bn, st.tri_sorted, st.counters, wcap, st.wnodes);
   return cudaGetLastError();
