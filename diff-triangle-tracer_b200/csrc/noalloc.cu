@@ -25,7 +25,13 @@
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (a host-side set-up, done once per device with that
 //    device current); make that first call before any stream capture;
-//  * `debug` timing is not available here (*gpu_time_ms is set to 0).
+//  * `debug` timing is not available here (*gpu_time_ms is set to 0);
+//  * with no handle there is no tt_device_status: tt_noalloc_status reads
+//    (and clears) the status word the last call's kernels left in the array;
+//  * the cached address belongs to the device's primary context: after
+//    cudaDeviceReset (or anything else that destroys that context) the
+//    address is stale, so this entry point must not be used again in that
+//    process.
 #include <cstring>
 #include <mutex>
 
@@ -82,10 +88,13 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   if (a->P > kMaxTriangles) return TT_ERR_TOO_LARGE;
   if (tt::bvh_storage_bytes(kMaxTriangles) + kCounterBytes > kScratchBytes) return TT_ERR_TOO_LARGE;
   if (!a->ray_o || !a->ray_d || !a->out_color || !a->out_others || !a->bg) return TT_ERR_INVALID;
+  // per-triangle colours in place of SH when shs is NULL, as tt_forward does
+  const float* cols = a->shs ? nullptr : a->colors_precomp;
   if (a->P > 0 && (!a->vertices || !a->cumsum || !a->num_points || !a->opacities || !a->sigma || !a->scaling ||
-                   !a->density_factor || !a->max_blending || !a->shs || a->num_vertices < 3))
+                   !a->density_factor || !a->max_blending || !(a->shs || cols) || a->num_vertices < 3))
     return TT_ERR_INVALID;
-  if (a->sh_degree < 0 || a->sh_degree > 3 || a->M < (a->sh_degree + 1) * (a->sh_degree + 1)) return TT_ERR_INVALID;
+  if (!cols && (a->sh_degree < 0 || a->sh_degree > 3 || a->M < (a->sh_degree + 1) * (a->sh_degree + 1)))
+    return TT_ERR_INVALID;
   if (a->debug && a->gpu_time_ms) *a->gpu_time_ms = 0.0f;
 
   DeviceSetup* dev = nullptr;
@@ -119,6 +128,7 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   p.cumsum = a->cumsum;
   p.num_points = a->num_points;
   p.shs = a->shs;
+  p.cols = cols;
   p.sh_degree = a->sh_degree;
   p.M = a->M;
   p.opac = a->opacities;
@@ -134,5 +144,21 @@ extern "C" int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, vo
   p.status = reinterpret_cast<int*>(counters) + 1;
   p.stats = reinterpret_cast<unsigned long long*>(counters + 16);
   if (tt::launch_forward(p, dev->grid, s) != cudaSuccess) return TT_ERR_CUDA;
+  return TT_OK;
+}
+
+extern "C" int tt_noalloc_status(void* stream) {
+  DeviceSetup* dev = nullptr;
+  int rc = setup_current_device(&dev);
+  if (rc != TT_OK) return rc;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* word = reinterpret_cast<int*>(dev->base + (kScratchBytes - kCounterBytes)) + 1;
+  int st = 0;
+  if (cudaMemcpyAsync(&st, word, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return TT_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return TT_ERR_CUDA;
+  if (cudaMemsetAsync(word, 0, sizeof(int), s) != cudaSuccess) return TT_ERR_CUDA;
+  if (st & tt::kStatusBounds) return TT_ERR_BOUNDS;
+  if (st & tt::kStatusStack) return TT_ERR_STACK;
+  if (st & tt::kStatusTimeout) return TT_ERR_TIMEOUT;
   return TT_OK;
 }

@@ -441,7 +441,8 @@ int tt_secondary_tree(tt_tracer* h, void* dst, unsigned long long dst_bytes, int
  * the given triangles and runs the plain forward trace using one fixed,
  * file-scope device array (4 MiB on every GPU that loads this library, for
  * the life of the process) instead of allocated memory. The caller passes the
- * inputs and outputs as in tt_forward; the results match tt_forward's.
+ * inputs and outputs as in tt_forward (SH, or colors_precomp with shs NULL);
+ * the results match tt_forward's.
  *
  * Limits: at most TT_NOALLOC_MAX_TRIANGLES triangles (else TT_ERR_TOO_LARGE,
  * nothing enqueued); plain variant only (cfg may be NULL for the defaults);
@@ -449,9 +450,22 @@ int tt_secondary_tree(tt_tracer* h, void* dst, unsigned long long dst_bytes, int
  * not available (*gpu_time_ms is set to 0). All calls share the one array:
  * calls that overlap on the GPU race and must not be issued. The first call
  * on each device looks the array's address up once (host-side set-up, with
- * that device current); make it before any stream capture. */
+ * that device current); make it before any stream capture. That address
+ * belongs to the device's primary context: do not use this entry point again
+ * after cudaDeviceReset. With no handle there is no tt_last_error or
+ * tt_device_status; an invalid argument returns TT_ERR_INVALID without a
+ * message, and device-side failures are read with tt_noalloc_status. */
 #define TT_NOALLOC_MAX_TRIANGLES 8192
 int tt_forward_noalloc(const tt_config* cfg, const tt_fwd_args* a, void* stream);
+
+/* Status of the last tt_forward_noalloc on the current device, for that
+ * handle-free entry point what tt_device_status is for a handle: synchronises
+ * `stream`, returns TT_OK, or TT_ERR_TIMEOUT / TT_ERR_STACK if a bounded
+ * device loop of that call gave up (its rays were cut short), or
+ * TT_ERR_BOUNDS from a TT_BOUNDS_CHECK build, and clears the word. Read it
+ * after a call and before the next one, which clears it again. Allocates
+ * nothing. No counterpart in the reference. */
+int tt_noalloc_status(void* stream);
 
 #ifdef __cplusplus
 }
