@@ -528,9 +528,10 @@ def secondary_leg(dev, steps=3, seed=0):
             "step": "forward (3 trace levels + 3 resolves) + adjoint (all levels, one launch)"}
 
 
-def run_views(args, world, rank, local, dev):
+def views_leg(dev, name, steps, warmup=3, no_autotune=False, world=1, local=0, sample_clocks=False):
     """Batched uneven views: every step is one CUDA-graph replay of refit +
-    forward + adjoint over all 16 views (ViewBatch), after autotuning."""
+    forward + adjoint over all 16 views (ViewBatch), after autotuning.
+    Returns the timed figures (the caller reports them)."""
     import torch
     import torch.distributed as dist
 
@@ -538,7 +539,6 @@ def run_views(args, world, rank, local, dev):
     from diff_tritracer.autotune import autotune
     from diff_tritracer.batch import ViewBatch
 
-    name = args.workload
     P = WORKLOADS[name][0]
     sc, rays_np, ups_np = make_workload(name)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -552,47 +552,45 @@ def run_views(args, world, rank, local, dev):
     eager = ViewBatch(tr, shapes, scene, 3, bg, graph=False)
     eager.set_rays([(T(a), T(b)) for a, b in rays_np])
     eager.set_upstream([(T(a), T(b)) for a, b in ups_np])
-    tuned = None if args.no_autotune else autotune(tr, eager.step, key=name, iters=2, prepare=eager.fit_hit_cache)
+    tuned = None if no_autotune else autotune(tr, eager.step, key=name, iters=2, prepare=eager.fit_hit_cache)
     # kernels per step, counted on an eager step (graph replays are not seen by the host counter)
     eager.fit_hit_cache()
     tr.reset_stats()
     eager.step()
     per_step = tr.stats()["kernel_launches"]
+    del eager
     vb = ViewBatch(tr, shapes, scene, 3, bg, graph=True)
     vb.set_rays([(T(a), T(b)) for a, b in rays_np])
     vb.set_upstream([(T(a), T(b)) for a, b in ups_np])
     cache_use = vb.fit_hit_cache()
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         vb.step()
     torch.cuda.synchronize()
     tr.device_status()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local) if sample_clocks else None
     tr.reset_stats()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler.start()
+    if sampler:
+        sampler.start()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         vb.step()
     t1.record()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop() if sampler else None
     ms = t0.elapsed_time(t1)
     st = tr.stats()
+    tr.device_status()
     ms = slowest_rank_ms(ms, world, dev)
-    if world > 1:
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    print(json.dumps({
-        "metric": METRIC, "value": world * R * args.steps / (ms / 1e3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+    return {
+        "value": world * R * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps, "steps": steps,
+        "gpu_launches": int(per_step * steps), "clocks": clocks,
         "config": {"workload": name, "triangles": P, "views": len(shapes),
                    "resolutions": [f"{h}x{w}" for h, w in shapes], "rays_per_step": R,
                    "step": "one CUDA-graph replay: refit + forward + adjoint over all views",
@@ -603,8 +601,70 @@ def run_views(args, world, rank, local, dev):
                                  "queries_per_ray": st["queries"] / max(st["rays"], 1)},
                    "hits_per_ray": {"evaluated": st["evaluated_hits"] / max(st["rays"], 1),
                                     "blended": st["blended_hits"] / max(st["rays"], 1)}},
-        "gpu_launches": int(per_step * args.steps), "clocks": clocks,
+    }
+
+
+def run_views(args, world, rank, local, dev):
+    """The batched workload as the bench's main line."""
+    import torch.distributed as dist
+
+    r = views_leg(dev, args.workload, args.steps, args.warmup, args.no_autotune, world, local, sample_clocks=True)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": r["value"], "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": r["config"],
+        "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
     }), flush=True)
+
+
+def c1_leg(dev, steps=50):
+    """The small plain-method configuration (100k triangles, one 400x400
+    view): refit + forward + adjoint per step, hit cache on, CUDA events."""
+    import torch
+
+    from diff_tritracer import _C
+
+    sc, ro_np, rd_np, g_np, go_np = make_workload("c1_100k_1x400")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ro, rd, g, go = T(ro_np), T(rd_np), T(g_np), T(go_np)
+    verts, sig, npts, cums = T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum)
+    shs, opac = T(sc.shs), T(sc.opacities)
+    P = sc.P
+    z = lambda: torch.zeros(P, device=dev)
+    bg, extra, empty, scaling, density = torch.zeros(3, device=dev), torch.zeros(5, device=dev), \
+        torch.empty(0, device=dev), z(), z()
+    R = ro.shape[0] * ro.shape[1]
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.build_tri_accel(verts, cums, P, True)
+
+    def step():
+        cache = tr.new_hit_cache(R)
+        out = tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg, extra,
+                               1, False, hit_cache=cache).data
+        tr.trace_backward(ro, rd, bg, verts, sig, npts, cums, out[0], out[1], P, shs, 3, opac, g, go, scaling, False,
+                          hit_cache=cache)
+
+    for _ in range(5):
+        step()
+    torch.cuda.synchronize()
+    tr.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = tr.stats()
+    tr.device_status()
+    return {"workload": "c1_100k_1x400", "rays_per_step": R, "ms_per_step": ms, "mrays": R / ms / 1e3,
+            "step": "refit + forward + adjoint, hit cache on, default traversal",
+            "hits_per_ray": {"evaluated": st["evaluated_hits"] / max(st["rays"], 1),
+                             "blended": st["blended_hits"] / max(st["rays"], 1)}}
 
 
 def main():
@@ -623,6 +683,8 @@ def main():
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the leg timing the exact adjoint, precomputed colours, BVH files and camera rays")
+    ap.add_argument("--no-c4", action="store_true", help="skip the batched 3M-triangle, 16-view leg")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 100k-triangle, one-view leg")
     ap.add_argument("--no-hit-cache", action="store_true",
                     help="adjoint re-traverses every query instead of replaying the forward's")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
@@ -875,6 +937,13 @@ def main():
                        bg=bg, extra=extra, empty=empty, scaling=scaling, density=density)
         widened = widened_leg(dev, tensors, P, scenes.sphere_cameras(views, H, W, seed=0), tuned)
 
+    c4 = c1 = None
+    if rank == 0 and world == 1 and not args.no_c4:
+        r = views_leg(dev, "c4_3M_16views", steps=5)
+        c4 = {"value_mrays": r["value"], "ms_per_step": r["ms_per_step"], "steps": r["steps"], **r["config"]}
+    if rank == 0 and world == 1 and not args.no_c1:
+        c1 = c1_leg(dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(name, sc, ro_np, rd_np, g_np, go_np)[0]
@@ -921,6 +990,8 @@ def main():
         "proposal": prop,
         "secondary": secondary,
         "widened": widened,
+        "c4": c4,
+        "c1": c1,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

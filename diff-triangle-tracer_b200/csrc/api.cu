@@ -128,7 +128,8 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
   def.tmin_inclusive = 1;
   h->cfg = cfg ? *cfg : def;
   if (h->cfg.variant < TT_VARIANT_PLAIN || h->cfg.variant > TT_VARIANT_ENVLIGHT ||
-      (h->cfg.exact_adjoint != 0 && h->cfg.variant != TT_VARIANT_PLAIN)) {
+      (h->cfg.exact_adjoint != 0 && h->cfg.variant != TT_VARIANT_PLAIN) ||
+      (h->cfg.reference_arithmetic != 0 && (h->cfg.variant != TT_VARIANT_PLAIN || h->cfg.exact_adjoint != 0))) {
     delete h;
     return TT_ERR_INVALID;
   }
@@ -243,7 +244,7 @@ static tt::TraceParams base_params(tt_tracer* h) {
   std::memset(&p, 0, sizeof(p));
   p.bvh = h->bvh.view();
   p.tmin_inclusive = h->cfg.tmin_inclusive;
-  p.exact = h->cfg.exact_adjoint;
+  p.mode = h->cfg.exact_adjoint ? tt::kShadeExact : (h->cfg.reference_arithmetic ? tt::kShadeRefArith : tt::kShadeRef);
   p.variant = h->cfg.variant;
   p.cfg = h->cfg_id;
   p.work = h->scratch.as<int>();

@@ -401,6 +401,82 @@ __device__ __forceinline__ float3 fcross(float3 a, float3 b) {
 __device__ __forceinline__ float flen(float3 v) { return sqrtf(fdot(v, v)); }
 __device__ __forceinline__ float3 fnormalize(float3 v) { return v * rsqrtf(fdot(v, v)); }
 
+// FP32 operations with explicit round-to-nearest and no contraction, for
+// code that repeats the reference's FP32 expression trees operation by
+// operation (the sphere variants' set-up, the reference-arithmetic window
+// function).
+namespace vf {
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return make_float3(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return make_float3(sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)); }
+__device__ __forceinline__ float3 scale(float3 a, float s) { return make_float3(mul(a.x, s), mul(a.y, s), mul(a.z, s)); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+  return make_float3(sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
+                     sub(mul(a.x, b.y), mul(a.y, b.x)));
+}
+__device__ __forceinline__ float3 normalize(float3 v) { return scale(v, div(1.0f, __fsqrt_rn(dot(v, v)))); }
+__device__ __forceinline__ float3 neg(float3 v) { return make_float3(-v.x, -v.y, -v.z); }
+// vecmath.h reflect: i - (2 n) dot(n, i)
+__device__ __forceinline__ float3 reflect(float3 i, float3 n) { return sub(i, scale(scale(n, 2.0f), dot(n, i))); }
+
+// common.h:116-141
+__device__ __forceinline__ bool hit_sphere(float r, float3 cnt, float3 o, float3 d, float& t) {
+  const float3 op = sub(o, cnt);
+  const float a = dot(d, d);
+  if (a <= 0.0f) return false;
+  const float b = dot(op, d);
+  const float c = sub(dot(op, op), mul(r, r));
+  float det = sub(mul(b, b), mul(c, a));
+  if (det < 0.0f) return false;
+  det = __fsqrt_rn(det);
+  t = div(sub(-b, det), a);
+  if ((double)t < kStepEps) {
+    t = div(add(-b, det), a);
+    if ((double)t < kStepEps) return false;
+  }
+  return true;
+}
+
+// refract.cu:24-45, kept as written (square roots where Snell's law has
+// squares; the same double/float mix)
+__device__ __forceinline__ bool refract_dir(float3& out, float3 in, float3 n, float eta_org) {
+  const float cos_i = dot(in, n);
+  float eta = eta_org;
+  if ((double)cos_i > 0.0) {
+    eta = __double2float_rn(__drcp_rn((double)eta_org));
+    n = neg(n);
+  }
+  const float sin2_i = __double2float_rn(fmax(0.0, __dsub_rn(1.0, (double)sqrtf(cos_i))));
+  const float sin2_t = div(sin2_i, __fsqrt_rn(eta));
+  if (sin2_t >= 1.0f) return false;
+  const float cos_t = __double2float_rn(sqrt(fmax(0.0, __dsub_rn(1.0, (double)sin2_t))));
+  out = add(scale(in, div(1.0f, eta)), scale(n, sub(div(-cos_i, eta), cos_t)));
+  return true;
+}
+
+// envlight.cu:25-51
+__device__ __forceinline__ float lcg(uint32_t& u) {
+  u = u * 1664525u + 1013904223u;
+  return mul((float)(u & 0x00FFFFFFu), 1.0f / 16777216.0f);
+}
+__device__ __forceinline__ float3 cosine_hemisphere(uint32_t& seed, float3 n) {
+  const float u = lcg(seed);
+  const float v = lcg(seed);
+  const float z = __fsqrt_rn(u);
+  const float rr = __fsqrt_rn(fmaxf(0.0f, __double2float_rn(__dsub_rn(1.0, (double)mul(z, z)))));
+  const float phi = mul(v, 6.2831853071795864769f);
+  const float3 dir = make_float3(mul(rr, cosf(phi)), mul(rr, sinf(phi)), z);
+  const float3 up = fabsf(n.z) < 0.999f ? make_float3(0.f, 0.f, 1.f) : make_float3(0.f, 1.f, 0.f);
+  const float3 t = normalize(cross(up, n));
+  const float3 b = normalize(cross(n, t));
+  return normalize(add(add(scale(t, dir.x), scale(b, dir.y)), scale(n, dir.z)));
+}
+}  // namespace vf
+
 // Window function of tritracer/common.h:57-114: edge normals
 // normalize(edge_cross x (p_i - p_{i+1})), edge 0 oriented by the incenter,
 // phi = max edge distance, phi_final = phi / dist(incenter, edge 0),
@@ -437,6 +513,65 @@ __device__ __forceinline__ Geom window_fn(float4 a, float4 b, float4 c, float3 o
   // __powf of the reference is NaN for a negative base and then clamped to 0
   g.Cx = (g.phi_final >= 0.0f) ? powf(g.phi_final, sigma) : 0.0f;
   return g;
+}
+
+// The window function in the reference's own FP32 arithmetic
+// (tritracer/common.h:57-114 on the hit point o + t d of forward.cu:118, t
+// the FP32 hit distance): absolute coordinates, each operation rounded to
+// nearest in the order of the reference's expressions, no multiply-add
+// fusion. It reproduces the reference's FP32 results, including the noise of
+// its edge distances (dot(n, hit) + offset cancels most of its digits on
+// small triangles far from the origin), for direct comparison with the
+// reference's code; the default mode solves the hit point in FP64 instead.
+__device__ __forceinline__ Geom window_fn_ref(float4 a4, float4 b4, float4 c4, float3 o, float3 d, float t,
+                                              float sigma) {
+  using namespace vf;
+  Geom g;
+  const float3 A = make_float3(a4.x, a4.y, a4.z), B = make_float3(b4.x, b4.y, b4.z), C = make_float3(c4.x, c4.y, c4.z);
+  const float3 hit = add(o, scale(d, t));
+  const float la = __fsqrt_rn(dot(sub(B, C), sub(B, C)));
+  const float lb = __fsqrt_rn(dot(sub(A, C), sub(A, C)));
+  const float lc = __fsqrt_rn(dot(sub(A, B), sub(A, B)));
+  const float3 num = add(add(scale(A, la), scale(B, lb)), scale(C, lc));
+  const float3 inc = scale(num, div(1.0f, add(add(la, lb), lc)));
+  const float3 ec = cross(sub(B, A), sub(C, A));
+  g.n = normalize(ec);
+  const float3 P[3] = {A, B, C};
+  float dist = 0.f, phi = -INFINITY;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float3 p1 = P[i], p2 = P[(i + 1) % 3];
+    float3 en = normalize(cross(ec, sub(p1, p2)));
+    float offset = -dot(en, p1);
+    if (i == 0) {
+      dist = add(dot(en, inc), offset);
+      if (dist > 0.0f) {
+        en = neg(en);
+        offset = -offset;
+        dist = -dist;
+      }
+    }
+    const float ed = add(dot(en, hit), offset);
+    phi = fmaxf(phi, ed);
+    g.d[i] = ed;
+  }
+  g.phi_max = phi;
+  g.phi_final = div(phi, dist);
+  g.Cx = (g.phi_final >= 0.0f) ? powf(g.phi_final, sigma) : 0.0f;
+  g.q = sub(hit, A);
+  g.e1 = sub(B, A);
+  g.e2 = sub(C, A);
+  g.t = t;
+  return g;
+}
+
+// Geometry of a hit in the given shading mode.
+template <int MODE>
+__device__ __forceinline__ Geom shade_geom(float4 a, float4 b, float4 c, float3 o, float3 d, float t, float sigma) {
+  if constexpr (MODE == kShadeRefArith)
+    return window_fn_ref(a, b, c, o, d, t, sigma);
+  else
+    return window_fn(a, b, c, o, d, sigma);
 }
 
 __device__ __constant__ float c_sh2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
@@ -1044,8 +1179,9 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned ra
 // counterpart) also fills the channels the reference leaves at 0: depth
 // sum w t, middepth (t of the hit after which T <= 0.5) and distortion
 // sum_{i<j} w_i w_j (t_i - t_j)^2 (running sums of w and w t^2).
-template <bool EXACT>
+template <int MODE>
 struct FwdShader {
+  static constexpr bool EXACT = MODE == kShadeExact;
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
@@ -1095,7 +1231,7 @@ struct FwdShader {
 
   __device__ __forceinline__ bool visit(uint32_t prim, float t) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, __ldg(p.sigma + prim));
+    const Geom g = shade_geom<MODE>(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, t, __ldg(p.sigma + prim));
     ++n_eval;
     float* rec = v->record;
     const int HW = v->H * v->W;
@@ -1161,11 +1297,11 @@ struct FwdShader {
   }
 };
 
-template <int CFG, bool EXACT>
+template <int CFG, int MODE>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
   cache_header<TraversalCfg<CFG>::K>(p);
   Counters cnt;
-  FwdShader<EXACT> sh(p, smem_bytes_for<CFG>());
+  FwdShader<MODE> sh(p, smem_bytes_for<CFG>());
   run<CFG>(p, sh, cnt);
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
@@ -1176,77 +1312,6 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 // is extra = [r, cx, cy, cz, samples]. The secondary-ray set-up repeats the
 // reference's FP32 expressions with explicit round-to-nearest operations (no
 // contraction), so the bent rays equal the oracle's.
-namespace vf {
-__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ float3 add(float3 a, float3 b) { return make_float3(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)); }
-__device__ __forceinline__ float3 sub(float3 a, float3 b) { return make_float3(sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)); }
-__device__ __forceinline__ float3 scale(float3 a, float s) { return make_float3(mul(a.x, s), mul(a.y, s), mul(a.z, s)); }
-__device__ __forceinline__ float dot(float3 a, float3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
-__device__ __forceinline__ float3 cross(float3 a, float3 b) {
-  return make_float3(sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
-                     sub(mul(a.x, b.y), mul(a.y, b.x)));
-}
-__device__ __forceinline__ float3 normalize(float3 v) { return scale(v, div(1.0f, __fsqrt_rn(dot(v, v)))); }
-__device__ __forceinline__ float3 neg(float3 v) { return make_float3(-v.x, -v.y, -v.z); }
-// vecmath.h reflect: i - (2 n) dot(n, i)
-__device__ __forceinline__ float3 reflect(float3 i, float3 n) { return sub(i, scale(scale(n, 2.0f), dot(n, i))); }
-
-// common.h:116-141
-__device__ __forceinline__ bool hit_sphere(float r, float3 cnt, float3 o, float3 d, float& t) {
-  const float3 op = sub(o, cnt);
-  const float a = dot(d, d);
-  if (a <= 0.0f) return false;
-  const float b = dot(op, d);
-  const float c = sub(dot(op, op), mul(r, r));
-  float det = sub(mul(b, b), mul(c, a));
-  if (det < 0.0f) return false;
-  det = __fsqrt_rn(det);
-  t = div(sub(-b, det), a);
-  if ((double)t < kStepEps) {
-    t = div(add(-b, det), a);
-    if ((double)t < kStepEps) return false;
-  }
-  return true;
-}
-
-// refract.cu:24-45, kept as written (square roots where Snell's law has
-// squares; the same double/float mix)
-__device__ __forceinline__ bool refract_dir(float3& out, float3 in, float3 n, float eta_org) {
-  const float cos_i = dot(in, n);
-  float eta = eta_org;
-  if ((double)cos_i > 0.0) {
-    eta = __double2float_rn(__drcp_rn((double)eta_org));
-    n = neg(n);
-  }
-  const float sin2_i = __double2float_rn(fmax(0.0, __dsub_rn(1.0, (double)sqrtf(cos_i))));
-  const float sin2_t = div(sin2_i, __fsqrt_rn(eta));
-  if (sin2_t >= 1.0f) return false;
-  const float cos_t = __double2float_rn(sqrt(fmax(0.0, __dsub_rn(1.0, (double)sin2_t))));
-  out = add(scale(in, div(1.0f, eta)), scale(n, sub(div(-cos_i, eta), cos_t)));
-  return true;
-}
-
-// envlight.cu:25-51
-__device__ __forceinline__ float lcg(uint32_t& u) {
-  u = u * 1664525u + 1013904223u;
-  return mul((float)(u & 0x00FFFFFFu), 1.0f / 16777216.0f);
-}
-__device__ __forceinline__ float3 cosine_hemisphere(uint32_t& seed, float3 n) {
-  const float u = lcg(seed);
-  const float v = lcg(seed);
-  const float z = __fsqrt_rn(u);
-  const float rr = __fsqrt_rn(fmaxf(0.0f, __double2float_rn(__dsub_rn(1.0, (double)mul(z, z)))));
-  const float phi = mul(v, 6.2831853071795864769f);
-  const float3 dir = make_float3(mul(rr, cosf(phi)), mul(rr, sinf(phi)), z);
-  const float3 up = fabsf(n.z) < 0.999f ? make_float3(0.f, 0.f, 1.f) : make_float3(0.f, 1.f, 0.f);
-  const float3 t = normalize(cross(up, n));
-  const float3 b = normalize(cross(n, t));
-  return normalize(add(add(scale(t, dir.x), scale(b, dir.y)), scale(n, dir.z)));
-}
-}  // namespace vf
 
 struct VarShader {
   const TraceParams& p;
@@ -1502,8 +1567,9 @@ __device__ __noinline__ void window_bwd_exact(const Geom& g, float3 dir, float d
 // backward.cu:191-350: the same march, running C/N/D that include the current
 // hit, dL/dalpha from the final values, scattered gradients. EXACT: the full
 // chain rule of window_bwd_exact, and no gradient through a clamped alpha.
-template <bool EXACT>
+template <int MODE>
 struct BwdShader {
+  static constexpr bool EXACT = MODE == kShadeExact;
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
@@ -1557,10 +1623,10 @@ struct BwdShader {
     }
   }
 
-  __device__ __forceinline__ bool visit(uint32_t prim, float) {
+  __device__ __forceinline__ bool visit(uint32_t prim, float t) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const float sig = __ldg(p.sigma + prim);
-    const Geom g = window_fn(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, sig);
+    const Geom g = shade_geom<MODE>(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, t, sig);
     const float opacity = __ldg(p.opac + prim);
     const float alpha = fminf(kAlphaMax, opacity * g.Cx);
     if (alpha < kAlphaMin) return false;
@@ -1661,10 +1727,10 @@ struct BwdShader {
   __device__ __forceinline__ void end() {}
 };
 
-template <int CFG, bool EXACT>
+template <int CFG, int MODE>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
   Counters cnt;
-  BwdShader<EXACT> sh(p);
+  BwdShader<MODE> sh(p);
   run<CFG>(p, sh, cnt);
   const unsigned s = __reduce_add_sync(0xFFFFFFFFu, cnt.replays);
   if ((threadIdx.x & 31) == 0 && s != 0u) atomicAdd(p.stats + kStatReplays, (unsigned long long)s);
@@ -2267,9 +2333,9 @@ size_t trace_smem_bytes(int cfg) {
 
 namespace {
 template <int CFG>
-const void* fwd_fn() { return (const void*)k_forward<CFG, false>; }
+const void* fwd_fn() { return (const void*)k_forward<CFG, kShadeRef>; }
 template <int CFG>
-const void* bwd_fn() { return (const void*)k_backward<CFG, false>; }
+const void* bwd_fn() { return (const void*)k_backward<CFG, kShadeRef>; }
 const void* kernel_for(int which, int cfg) {
   switch (cfg) {
     case kCfgPackets16: return which == 0 ? fwd_fn<kCfgPackets16>() : bwd_fn<kCfgPackets16>();
@@ -2297,31 +2363,32 @@ cudaError_t trace_init() {
     if (e == cudaSuccess && bytes > 48 * 1024)
       e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };
-  opt_in((const void*)k_forward<kCfgPackets16, true>, smem_bytes_for<kCfgPackets16>() + kExactSmemBytes);
-  opt_in((const void*)k_forward<kCfgPackets32, true>, smem_bytes_for<kCfgPackets32>() + kExactSmemBytes);
-  opt_in((const void*)k_forward<kCfgLanes24, true>, smem_bytes_for<kCfgLanes24>() + kExactSmemBytes);
-  opt_in((const void*)k_forward<kCfgLanes32, true>, smem_bytes_for<kCfgLanes32>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgPackets16, kShadeExact>, smem_bytes_for<kCfgPackets16>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgPackets32, kShadeExact>, smem_bytes_for<kCfgPackets32>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgLanes24, kShadeExact>, smem_bytes_for<kCfgLanes24>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgLanes32, kShadeExact>, smem_bytes_for<kCfgLanes32>() + kExactSmemBytes);
   return e;
 }
 
-template <bool EXACT>
+template <int MODE>
 cudaError_t launch_forward_t(const TraceParams& p, int grid, cudaStream_t s) {
+  const size_t extra = MODE == kShadeExact ? kExactSmemBytes : 0;
   switch (p.cfg) {
-    case kCfgPackets16: k_forward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
-    case kCfgPackets32: k_forward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
-    case kCfgLanes24: k_forward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
-    default: k_forward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>() + (EXACT ? kExactSmemBytes : 0), s>>>(p); break;
+    case kCfgPackets16: k_forward<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>() + extra, s>>>(p); break;
+    case kCfgPackets32: k_forward<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>() + extra, s>>>(p); break;
+    case kCfgLanes24: k_forward<kCfgLanes24, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>() + extra, s>>>(p); break;
+    default: k_forward<kCfgLanes32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>() + extra, s>>>(p); break;
   }
   return cudaGetLastError();
 }
 
-template <bool EXACT>
+template <int MODE>
 cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
   switch (p.cfg) {
-    case kCfgPackets16: k_backward<kCfgPackets16, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
-    case kCfgPackets32: k_backward<kCfgPackets32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
-    case kCfgLanes24: k_backward<kCfgLanes24, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
-    default: k_backward<kCfgLanes32, EXACT><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+    case kCfgPackets16: k_backward<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_backward<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_backward<kCfgLanes24, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_backward<kCfgLanes32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
   }
   return cudaGetLastError();
 }
@@ -2331,11 +2398,19 @@ cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {
     k_variant<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
     return cudaGetLastError();
   }
-  return p.exact ? launch_forward_t<true>(p, grid, s) : launch_forward_t<false>(p, grid, s);
+  switch (p.mode) {
+    case kShadeExact: return launch_forward_t<kShadeExact>(p, grid, s);
+    case kShadeRefArith: return launch_forward_t<kShadeRefArith>(p, grid, s);
+    default: return launch_forward_t<kShadeRef>(p, grid, s);
+  }
 }
 
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
-  return p.exact ? launch_backward_t<true>(p, grid, s) : launch_backward_t<false>(p, grid, s);
+  switch (p.mode) {
+    case kShadeExact: return launch_backward_t<kShadeExact>(p, grid, s);
+    case kShadeRefArith: return launch_backward_t<kShadeRefArith>(p, grid, s);
+    default: return launch_backward_t<kShadeRef>(p, grid, s);
+  }
 }
 
 int sec_blocks_per_sm(int which) {

@@ -87,6 +87,13 @@ struct SecParams {
   int* count;                      // [kMaxSecDepth + 1] records per level, levels >= 1 (device)
 };
 
+// Shading modes of the plain forward and adjoint (tt_config): the
+// reference's semantics with the hit point from an FP64 plane solve
+// (default); the exact adjoint; the reference's semantics in the reference's
+// own FP32 arithmetic (hit point o + t d, window function on absolute
+// coordinates), for comparison with the reference's code.
+constexpr int kShadeRef = 0, kShadeExact = 1, kShadeRefArith = 2;
+
 struct TraceParams {
   BvhView bvh;
   int nviews;
@@ -116,7 +123,7 @@ struct TraceParams {
   float sph_r, sph_cx, sph_cy, sph_cz;
   int samples;
   int tmin_inclusive;
-  int exact;    // 1: exact adjoint (and depth accumulated by the forward)
+  int mode;     // kShade*: how the plain forward / adjoint shade a hit
   int cfg;      // traversal configuration, kCfg*
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits

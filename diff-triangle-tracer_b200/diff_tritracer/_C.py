@@ -83,7 +83,8 @@ class OptixTracer:
     refract.ptx, envlight.ptx / backward.ptx)."""
 
     def __init__(self, pkg_dir: str = "", forward: str = "forward.ptx", backward: str = "backward.ptx",
-                 tmin_inclusive: bool = True, traversal: str = "auto", exact_adjoint: bool = False):
+                 tmin_inclusive: bool = True, traversal: str = "auto", exact_adjoint: bool = False,
+                 reference_arithmetic: bool = False):
         if forward not in _VARIANTS:
             raise RuntimeError(f"unknown forward program {forward!r}; expected one of {sorted(_VARIANTS)}")
         if backward != "backward.ptx":
@@ -103,6 +104,9 @@ class OptixTracer:
             raise RuntimeError(f"traversal must be one of {sorted(modes)}")
         cfg.traversal = modes[traversal]
         cfg.exact_adjoint = 1 if exact_adjoint else 0
+        # the reference's own FP32 arithmetic for the window function (see
+        # tt_config.reference_arithmetic); default: FP64 ray/plane solve
+        cfg.reference_arithmetic = 1 if reference_arithmetic else 0
         h = ctypes.c_void_p(0)
         rc = lib.tt_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != _lib.TT_OK:

@@ -124,15 +124,20 @@ class Tracer(nn.Module):
     "envlight.ptx" / "backward.ptx"); nothing is read from disk."""
 
     def __init__(self, forwad_ptx="forward.ptx", backward_ptx="backward.ptx", tmin_inclusive: bool = True,
-                 exact_adjoint: bool = False, hit_cache: bool = True) -> None:
+                 exact_adjoint: bool = False, hit_cache: bool = True, reference_arithmetic: bool = False) -> None:
         """hit_cache (no reference counterpart): the forward keeps its
         k-closest queries in a device buffer held by the autograd graph ((k + 1)
         * 8 bytes a ray for the first ones, plus a pool of a quarter of that for
         later ones) and the backward replays them instead of traversing the BVH
-        again; the gradients are the same either way."""
+        again; the gradients are the same either way.
+
+        reference_arithmetic (no reference counterpart): evaluate each hit's
+        window function in the reference's own FP32 arithmetic (hit point
+        o + t d) instead of from an FP64 ray/plane solve, to reproduce the
+        reference's numbers; the semantics are the same."""
         super().__init__()
         self.tracer = _C.OptixTracer("", forwad_ptx, backward_ptx, tmin_inclusive=tmin_inclusive,
-                                     exact_adjoint=exact_adjoint)
+                                     exact_adjoint=exact_adjoint, reference_arithmetic=reference_arithmetic)
         self.tracer.use_hit_cache = bool(hit_cache)
 
     def forward(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,

@@ -39,7 +39,7 @@ _vp = ctypes.c_void_p
 class TtConfig(ctypes.Structure):
     _fields_ = [("variant", ctypes.c_int), ("tmin_inclusive", ctypes.c_int), ("traversal", ctypes.c_int),
                 ("k", ctypes.c_int), ("stack_depth", ctypes.c_int), ("exact_adjoint", ctypes.c_int),
-                ("reserved", ctypes.c_int * 2)]
+                ("reference_arithmetic", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
 
 
 class TtFwdArgs(ctypes.Structure):

@@ -78,7 +78,16 @@ typedef struct tt_config {
                          distortion (sum over hit pairs i < j of w_i w_j (t_i - t_j)^2), all
                          differentiated by the adjoint. No reference counterpart; plain
                          program only */
-  int reserved[2];    /* zero */
+  int reference_arithmetic; /* 0 (default): each hit's point on its triangle comes from an
+                         FP64 ray/plane solve and the window function is evaluated
+                         relative to vertex A, which holds ~7 digits of the incircle; 1:
+                         the reference's own FP32 arithmetic instead (hit point o + t d,
+                         window function on absolute coordinates, every operation
+                         rounded in the order of tritracer/common.h:57-114), whose edge
+                         distances keep only ~3 digits on small triangles far from the
+                         origin. Same semantics either way; 1 reproduces the reference's
+                         numbers. Plain program only, not with exact_adjoint */
+  int reserved[1];    /* zero */
 } tt_config;
 
 /* Arguments of the forward trace: OptixTracer::trace_fwd

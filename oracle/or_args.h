@@ -45,5 +45,13 @@ struct or_args {
   int exact_adjoint;  // 1: full chain rule + forward depth (FP64 with exact geometry)
   const float* precomp;  // [P][3] precomputed colours in place of SH, or NULL
   void* dprecomp;        // their gradient (precision of the call), backward only
+  // optional log of every k-closest query a ray's forward made (host build of
+  // the reference only): per ray up to max_chunks queries, each its lower
+  // bound tmin and the 16 primitive ids the any-hit program left in the
+  // payload (0xFFFFFFFF for empty slots)
+  int max_chunks;
+  unsigned* chunk_ids;  // [H*W][max_chunks][16]
+  float* chunk_tmin;    // [H*W][max_chunks]
+  int* chunk_count;     // [H*W] queries made (may exceed max_chunks)
 };
 }

@@ -42,6 +42,8 @@ class OrArgs(ctypes.Structure):
         ("material", _ip), ("ior", _fp), ("env", _fp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
         ("max_depth", ctypes.c_int), ("exact_adjoint", ctypes.c_int),
         ("precomp", _fp), ("dprecomp", ctypes.c_void_p),
+        ("max_chunks", ctypes.c_int), ("chunk_ids", ctypes.POINTER(ctypes.c_uint32)), ("chunk_tmin", _fp),
+        ("chunk_count", _ip),
     ]
 
 
@@ -65,6 +67,9 @@ class FwdResult:
     rec_ids: np.ndarray | None = None
     rec_count: np.ndarray | None = None
     margin: np.ndarray | None = None
+    chunk_ids: np.ndarray | None = None  # [H*W, chunks, 16] (reference only, `chunks` > 0)
+    chunk_tmin: np.ndarray | None = None  # [H*W, chunks]
+    chunk_count: np.ndarray | None = None  # [H*W]
 
 
 @dataclass
@@ -149,7 +154,10 @@ class _Runner:
 
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
                 canonical=False, exact=False, nthreads=1, scaling=None, density=None, record=0, rows=None,
-                interval=None, secondary=None, exact_adjoint=False, precomp=None):
+                interval=None, secondary=None, exact_adjoint=False, precomp=None, chunks=0):
+        """`chunks` > 0 (the reference's own code only): also log, per ray, up
+        to that many of its k-closest queries (lower bound and the 16 ids the
+        any-hit program kept)."""
         a, keep = self._args(scene, ray_o, ray_d, bg, extra, variant, tmin_inclusive, canonical, exact, nthreads, rows)
         a.exact_adjoint = int(exact_adjoint)
         if precomp is not None:
@@ -170,6 +178,15 @@ class _Runner:
             rec_count = np.zeros(H * W, np.int32)
             margin = np.zeros(H * W, np.float32)
             a.max_rec, a.rec_ids, a.rec_count, a.margin = record, _ptr(rec_ids, _ip), _ptr(rec_count, _ip), _ptr(margin)
+        chunk_ids = chunk_tmin = chunk_count = None
+        if chunks:
+            assert self.prefix == "ref", "the query log is a hook of the reference's host build"
+            chunk_ids = np.full((H * W, chunks, 16), 0xFFFFFFFF, np.uint32)
+            chunk_tmin = np.full((H * W, chunks), np.nan, np.float32)
+            chunk_count = np.zeros(H * W, np.int32)
+            a.max_chunks = chunks
+            a.chunk_ids = _ptr(chunk_ids, ctypes.POINTER(ctypes.c_uint32))
+            a.chunk_tmin, a.chunk_count = _ptr(chunk_tmin), _ptr(chunk_count, _ip)
         t = ctypes.POINTER(ctypes.c_float if precision == 32 else ctypes.c_double)
         if self.prefix == "ref":
             assert precision == 32
@@ -181,7 +198,8 @@ class _Runner:
                 _ptr(others, t), _ptr(maxb, t))
         if rc != 0:
             raise RuntimeError(f"{self.prefix} forward failed ({rc})")
-        return FwdResult(color, others, scaling, density, maxb, rec_ids, rec_count, margin)
+        return FwdResult(color, others, scaling, density, maxb, rec_ids, rec_count, margin, chunk_ids, chunk_tmin,
+                         chunk_count)
 
     def backward(self, scene, ray_o, ray_d, colors, others, dL_dpixels, dL_dothers, bg=None, precision=32,
                  tmin_inclusive=True, canonical=False, exact=False, nthreads=1, rows=None, interval=None,

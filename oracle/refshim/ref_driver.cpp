@@ -43,6 +43,7 @@ struct ShimThread {
 thread_local ShimThread g;
 const tto::Scene* g_scene = nullptr;
 bool g_tmin_inclusive = true;
+const or_args* g_log = nullptr;  // forward calls that log their queries (or_args.chunk_*)
 
 }  // namespace
 
@@ -81,6 +82,16 @@ void optixTrace(OptixTraversableHandle, float3 o, float3 d, float tmin, float tm
     g.anyhit();
     return g.ignored ? tcur : t;
   });
+  if (g_log && g_log->chunk_count) {
+    // the payload after the trace: 16 (id, t) pairs, ids in the even words
+    const size_t pix = (size_t)g.idx.y * g.dim.x + g.idx.x;
+    const int c = g_log->chunk_count[pix]++;
+    if (c < g_log->max_chunks) {
+      const size_t q = pix * (size_t)g_log->max_chunks + (size_t)c;
+      g_log->chunk_tmin[q] = tmin;
+      for (int i = 0; i < 16; ++i) g_log->chunk_ids[q * 16 + i] = *g.pl[2 * i];
+    }
+  }
 }
 #undef TT_U
 
@@ -165,7 +176,9 @@ int ref_forward(void* scene, const or_args* a, float* scaling, float* density, f
   p->out_color = color;
   p->out_others = others;
   p->max_blending = maxb;
+  g_log = (a->max_chunks > 0 && a->chunk_ids && a->chunk_tmin && a->chunk_count) ? a : nullptr;
   launch(a, rg, ah);
+  g_log = nullptr;
   return 0;
 }
 

@@ -103,3 +103,21 @@ def test_multithreaded_matches_single(oracle, case):
     a = oracle.forward(sc, ro, rd, nthreads=1)
     b = oracle.forward(sc, ro, rd, nthreads=4)
     assert bits_equal(a.color, b.color) and bits_equal(a.max_blending, b.max_blending)
+
+
+@pytest.mark.parametrize("incl", [True, False], ids=["closed", "open"])
+def test_reference_queries_equal_the_hit_stream(oracle, reference, case, incl):
+    """The k-closest queries the reference's own any-hit program answers
+    (tritracer/closestk.h:17-149, logged per ray) hold, query by query, the
+    same hits as the (t, id)-ordered hit stream of the restated intersector
+    and BVH, except for the order inside groups of equal t. The GPU test
+    tests/test_gpu_vs_reference.py makes the same check against the GPU's
+    hit stream."""
+    from ref_chunks import compare_chunks
+
+    sc, ro, rd = case
+    f = reference.forward(sc, ro, rd, tmin_inclusive=incl, chunks=8)
+    ids, ts, cnt = oracle.hit_stream(sc, ro, rd, max_hits=256, nthreads=8)
+    assert (f.chunk_count > 1).mean() > 0.2  # re-traced chunks are logged too
+    n, _ = compare_chunks(f.chunk_ids, f.chunk_tmin, f.chunk_count, ids, ts, cnt, incl, 256)
+    assert n > 3000
