@@ -508,24 +508,31 @@ def secondary_leg(dev, steps=3, seed=0):
         tr.trace_backward_secondary(ro, rd, verts, sig, npts, cums, color, others, P, shs, 3, opac, g, go, mat,
                                     ior, env, 2)
 
-    for _ in range(2):
-        step()
-    torch.cuda.synchronize()
-    tr.reset_stats()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    st = tr.stats()
+    def timed():
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        tr.reset_stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, tr.stats()
+
+    tr.set_sort_secondary(False)
+    ms_unsorted, _ = timed()
+    tr.set_sort_secondary(True)
+    ms, st = timed()
     tr.device_status()
     R = 1600 * 800
     return {"workload": "500k triangles, 20% dielectric, env 512x1024, 2 views 800x800, 2 bounces",
             "pixels_per_step": R, "rays_per_step": st["rays"] / steps, "ms_per_step": ms,
             "primary_mrays": R / ms / 1e3, "all_rays_mrays": st["rays"] / steps / ms / 1e3,
-            "step": "forward (3 trace levels + 3 resolves) + adjoint (all levels, one launch)"}
+            "ms_per_step_spawn_order": ms_unsorted,
+            "step": "forward (3 trace levels, spawned levels sorted by direction octant and origin, + 3 resolves) "
+                    "+ adjoint (all levels, one launch)"}
 
 
 def views_leg(dev, name, steps, warmup=3, no_autotune=False, world=1, local=0, sample_clocks=False):

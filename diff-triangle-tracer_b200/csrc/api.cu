@@ -18,7 +18,10 @@ struct tt_tracer {
   tt_config cfg;
   int device = 0;
   int num_sms = 148;
-  int fwd_grid = 0, bwd_grid = 0;
+  int fwd_grid = 0, bwd_grid = 0, collect_grid = 0;
+  bool split_forward = true;  // plain forward with a hit cache: collecting pass + shading pass
+  bool sort_secondary = true; // secondary passes: spawned rays traced in sorted order
+  tt::DevBuf sec_sort;        // their sort keys / indices (2 x 2 x 4R words) and the sort's histogram
   int cfg_id = tt::kCfgPackets16;
   std::string err;
   tt::Bvh bvh;
@@ -174,7 +177,17 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth) {
   const int which = h->cfg.variant != TT_VARIANT_PLAIN ? 2 : 0;
   h->fwd_grid = h->num_sms * tt::trace_blocks_per_sm(which, id);
   h->bwd_grid = h->num_sms * tt::trace_blocks_per_sm(1, id);
+  h->collect_grid = h->num_sms * tt::trace_blocks_per_sm(3, id);
   return TT_OK;
+}
+
+int tt_set_option(tt_tracer* h, int option, int value) {
+  if (!h) return TT_ERR_INVALID;
+  switch (option) {
+    case TT_OPT_SPLIT_FORWARD: h->split_forward = value != 0; return TT_OK;
+    case TT_OPT_SORT_SECONDARY: h->sort_secondary = value != 0; return TT_OK;
+    default: return fail(h, TT_ERR_INVALID, "unknown option");
+  }
 }
 
 size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays) {
@@ -343,8 +356,16 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   p.sph_cz = ex[3];
   p.samples = (int)ex[4];
   if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
-  TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  if (p.hit_cache && h->split_forward) {
+    // traversal-only pass: every query of the march into the cache; the
+    // shading pass below replays them
+    TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+    TT_CUDA(h, tt::launch_collect(p, h->collect_grid, s));
+    ++h->trace_launches;
+    p.cache_mode = tt::kCacheRead;
+  }
+  TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   TT_CUDA(h, tt::launch_forward(p, h->fwd_grid, s));
   ++h->trace_launches;
   if (a->debug) {
@@ -776,9 +797,29 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
   h->sec_depth = -1;  // no valid tree until this call's launches are enqueued
   if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
   TT_CUDA(h, cudaMemsetAsync(count, 0, (tt::kMaxSecDepth + 1) * sizeof(int), s));
+  uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr, *hist = nullptr;
+  if (h->sort_secondary && sec->max_depth > 0) {
+    const long long cap = R << sec->max_depth;  // the deepest level's capacity
+    const size_t hw = tt::sort_pairs_hist_words((int)cap);
+    TT_CUDA(h, h->sec_sort.reserve((size_t)(4 * cap) * 4 + hw * 4));
+    keys = h->sec_sort.as<uint32_t>();
+    vals = keys + cap;
+    keys2 = vals + cap;
+    vals2 = keys2 + cap;
+    hist = vals2 + cap;
+  }
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
   for (int level = 0; level <= sec->max_depth; ++level) {
     p.sec.level = level;
+    p.sec.order = nullptr;
+    if (level > 0 && keys) {
+      // trace the spawned rays in (direction octant, origin Morton code) order
+      bool second = false;
+      TT_CUDA(h, tt::launch_sec_sort_keys(p, keys, vals, s));
+      TT_CUDA(h, tt::sort_pairs(keys, vals, keys2, vals2, hist, p.sec.cap[level], 32, &second, s));
+      p.sec.order = second ? vals2 : vals;
+      h->trace_launches += 1 + 3 * 4;
+    }
     TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
     TT_CUDA(h, level == 0 ? tt::launch_sec_primary(p, h->sec_primary_grid, s)
                           : tt::launch_sec_trace(p, h->sec_trace_grid, s));

@@ -958,6 +958,26 @@ cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* 
   return cudaGetLastError();
 }
 
+size_t sort_pairs_hist_words(int n) { return (size_t)256 * (size_t)((n + kSortTile - 1) / kSortTile); }
+
+cudaError_t sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2, uint32_t* hist, int n,
+                       int bits, bool* in_second, cudaStream_t s) {
+  *in_second = false;
+  if (n <= 0) return cudaSuccess;
+  const int tiles = (n + kSortTile - 1) / kSortTile;
+  uint32_t *ka = keys, *va = vals, *kb = keys2, *vb = vals2;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, n, shift, hist, tiles);
+    k_scan_excl<<<1, 1024, 0, s>>>(hist, 256 * tiles);
+    k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, n, shift, hist, tiles);
+    uint32_t* t;
+    t = ka; ka = kb; kb = t;
+    t = va; va = vb; vb = t;
+    *in_second = !*in_second;
+  }
+  return cudaGetLastError();
+}
+
 BvhView bvh_storage_view(const BvhStorage& st, int P) {
   BvhView v;
   v.nodes = st.wnodes;

@@ -765,9 +765,11 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
   };
   unsigned long long last_key = 0;
   bool any = false;
-  // the stream ran out below cur.t_hi; `next` is where it would resume
+  // the stream ran out below cur.t_hi; `next` is where it would resume. A
+  // shader that cannot end a ray (the collecting pass) stops there too: the
+  // shading pass decides on continuations and re-traces.
   auto exhausted = [&](unsigned long long next) {
-    if (cur.t_hi >= kFar) return true;
+    if (cur.t_hi >= kFar || Shader::kStopsAtClip) return true;
     cur.t_hi = kFar;
     if (!any && cur.chunks == 0) {
       cur.key_min = first_key(tmin_inclusive);
@@ -1182,6 +1184,7 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, unsigned ra
 template <int MODE>
 struct FwdShader {
   static constexpr bool EXACT = MODE == kShadeExact;
+  static constexpr bool kStopsAtClip = false;
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
@@ -1306,6 +1309,43 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
+// ---------------------------------------------------------------- collect
+// Traversal-only pass of the split forward (plain program with a hit cache).
+// It runs every ray's march with a shader that shades nothing and never ends
+// a ray early, so it makes, and stores in the hit cache, every k-closest
+// query the plain march would make. The shading pass (k_forward reading the
+// cache) then replays each query its own march asks for; a ray that ends on
+// the transmittance cut-off simply leaves its later queries unread, and a
+// query the cache could not hold (pool full) is traversed again there. With
+// no shading state or code the pass needs far fewer registers than the fused
+// kernel, so more warps per SM hide the latency of the node and triangle
+// loads, which is what bounds the traversal.
+#ifndef TT_COLLECT_BLOCKS
+#define TT_COLLECT_BLOCKS 6
+#endif
+constexpr int kCollectBlocks = TT_COLLECT_BLOCKS;
+
+struct MarchShader {
+  static constexpr bool kStopsAtClip = true;
+  const TraceParams& p;
+  __device__ explicit MarchShader(const TraceParams& params) : p(params) {}
+  __device__ __forceinline__ bool begin(const ViewDesc*, int, float3, float3) { return true; }
+  __device__ __forceinline__ bool next(float3&, float3&) { return false; }
+  __device__ __forceinline__ void prepare() {}
+  __device__ __forceinline__ bool visit(uint32_t, float) { return false; }
+  __device__ __forceinline__ void end() {}
+};
+
+template <int CFG>
+__global__ void __launch_bounds__(kTraceThreads, kCollectBlocks) k_collect(const __grid_constant__ TraceParams p) {
+  cache_header<TraversalCfg<CFG>::K>(p);
+  Counters cnt;
+  MarchShader sh(p);
+  run<CFG>(p, sh, cnt);
+  // traversal counters only: rays and hits are counted by the shading pass
+  add_stats(p.stats, 0u, 0u, 0u, cnt);
+}
+
 // ---------------------------------------------------------------- variants
 // Sphere variants of the reference (tritracer/reflect.cu, refract.cu,
 // envlight.cu, common.h:116-148), forward only as there. The analytic sphere
@@ -1314,6 +1354,7 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 // contraction), so the bent rays equal the oracle's.
 
 struct VarShader {
+  static constexpr bool kStopsAtClip = false;
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
@@ -1570,6 +1611,7 @@ __device__ __noinline__ void window_bwd_exact(const Geom& g, float3 dir, float d
 template <int MODE>
 struct BwdShader {
   static constexpr bool EXACT = MODE == kShadeExact;
+  static constexpr bool kStopsAtClip = false;
   const TraceParams& p;
   const ViewDesc* v;
   int pix;
@@ -1927,6 +1969,7 @@ __device__ __forceinline__ float3 env_lookup(const SecParams& s, float3 d) {
 
 // The rays of one level: trace, composite, spawn children into the next level.
 struct SecShader {
+  static constexpr bool kStopsAtClip = false;
   const TraceParams& p;
   const ViewDesc* v;
   int ridx, pix, level;
@@ -1939,7 +1982,7 @@ struct SecShader {
 
   __device__ __forceinline__ void begin_item(int i, float3& ro, float3& rd) {
     const SecParams& s = p.sec;
-    ridx = s.base[level] + i;
+    ridx = s.base[level] + (level > 0 && s.order ? (int)__ldg(s.order + i) : i);
     SecRecord* r = s.rec + ridx;
     if (level == 0) {
       pix = i;
@@ -2078,6 +2121,57 @@ __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_trace(const __grid_con
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
+// Sort keys of the spawned rays of level p.sec.level: the octant of the
+// direction (3 bits) over the Morton code of the origin (9 bits an axis)
+// within the root box of the BVH; slots past the level's count get
+// 0xFFFFFFFF and sort after every ray.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 9 bits -> every third of 27
+  v &= 0x1FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_sec_sort_keys(const __grid_constant__ TraceParams p, uint32_t* __restrict__ keys,
+                                uint32_t* __restrict__ vals) {
+  const SecParams& s = p.sec;
+  const int level = s.level, cap = s.cap[level];
+  const int n = min(__ldcg(s.count + level), cap);
+  // the root's box: the union of its 8 child boxes (empty slots are inverted)
+  float lo[3] = {0.f, 0.f, 0.f}, ext[3] = {1.f, 1.f, 1.f};
+  if (p.bvh.has_root && p.bvh.P >= 2) {
+    const float* nd = reinterpret_cast<const float*>(p.bvh.nodes);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float l = INFINITY, h = -INFINITY;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        l = fminf(l, __ldg(nd + 16 * a + c));
+        h = fmaxf(h, __ldg(nd + 16 * a + 8 + c));
+      }
+      if (l < h) {
+        lo[a] = l;
+        ext[a] = h - l;
+      }
+    }
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+    uint32_t key = 0xFFFFFFFFu;
+    if (i < n) {
+      const SecRecord& r = s.rec[s.base[level] + i];
+      uint32_t q[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) q[a] = (uint32_t)fminf(fmaxf((r.o[a] - lo[a]) / ext[a] * 512.f, 0.f), 511.f);
+      const uint32_t oct = (r.d[0] < 0.f ? 4u : 0u) | (r.d[1] < 0.f ? 2u : 0u) | (r.d[2] < 0.f ? 1u : 0u);
+      key = (oct << 27) | (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+    }
+    keys[i] = key;
+    vals[i] = (uint32_t)i;
+  }
+}
+
 // Adds each record's children's radiance to it (their level is complete) and,
 // for level 0, writes the pixel colours.
 __global__ void k_sec_resolve(const __grid_constant__ TraceParams p) {
@@ -2123,6 +2217,7 @@ __global__ void k_sec_resolve(const __grid_constant__ TraceParams p) {
 // upstream gradient tau dL/dpixel; the spawning hit's colour is the
 // children's resolved radiance and it has no SH gradient).
 struct SecBwdShader {
+  static constexpr bool kStopsAtClip = false;
   const TraceParams& p;
   const ViewDesc* v;
   int ridx, pix, level;
@@ -2336,6 +2431,14 @@ template <int CFG>
 const void* fwd_fn() { return (const void*)k_forward<CFG, kShadeRef>; }
 template <int CFG>
 const void* bwd_fn() { return (const void*)k_backward<CFG, kShadeRef>; }
+const void* collect_fn(int cfg) {
+  switch (cfg) {
+    case kCfgPackets16: return (const void*)k_collect<kCfgPackets16>;
+    case kCfgPackets32: return (const void*)k_collect<kCfgPackets32>;
+    case kCfgLanes24: return (const void*)k_collect<kCfgLanes24>;
+    default: return (const void*)k_collect<kCfgLanes32>;
+  }
+}
 const void* kernel_for(int which, int cfg) {
   switch (cfg) {
     case kCfgPackets16: return which == 0 ? fwd_fn<kCfgPackets16>() : bwd_fn<kCfgPackets16>();
@@ -2348,7 +2451,7 @@ const void* kernel_for(int which, int cfg) {
 
 int trace_blocks_per_sm(int which, int cfg) {
   int n = 0;
-  const void* fn = which == 2 ? (const void*)k_variant : kernel_for(which, cfg);
+  const void* fn = which == 2 ? (const void*)k_variant : (which == 3 ? collect_fn(cfg) : kernel_for(which, cfg));
   const size_t smem = which == 2 ? smem_bytes_for<kCfgLanes32>() : trace_smem_bytes(cfg);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem) != cudaSuccess) n = 1;
   return n > 0 ? n : 1;
@@ -2389,6 +2492,16 @@ cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
     case kCfgPackets32: k_backward<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
     case kCfgLanes24: k_backward<kCfgLanes24, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
     default: k_backward<kCfgLanes32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_collect(const TraceParams& p, int grid, cudaStream_t s) {
+  switch (p.cfg) {
+    case kCfgPackets16: k_collect<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_collect<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_collect<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_collect<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
   }
   return cudaGetLastError();
 }
@@ -2437,6 +2550,14 @@ cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s) {
   const int grid = (int)std::min<long long>((cap + 255) / 256, 4096);
   if (grid == 0) return cudaSuccess;
   k_sec_resolve<<<grid, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sec_sort_keys(const TraceParams& p, uint32_t* keys, uint32_t* vals, cudaStream_t s) {
+  const int cap = p.sec.cap[p.sec.level];
+  const int grid = std::min((cap + 255) / 256, 148 * 8);
+  if (grid == 0) return cudaSuccess;
+  k_sec_sort_keys<<<grid, 256, 0, s>>>(p, keys, vals);
   return cudaGetLastError();
 }
 

@@ -85,6 +85,11 @@ struct SecParams {
   int base[kMaxSecDepth + 1];      // first record of each level
   int cap[kMaxSecDepth + 1];       // records each level can hold
   int* count;                      // [kMaxSecDepth + 1] records per level, levels >= 1 (device)
+  // Order in which k_sec_trace takes the records of the level it traces
+  // (levels >= 1): item i is record base[level] + order[i]; nullptr = queue
+  // order. The spawned rays sorted by direction octant and origin (Morton
+  // code), so that the rays of a warp cross nearly the same BVH nodes.
+  const uint32_t* order;
 };
 
 // Shading modes of the plain forward and adjoint (tt_config): the
@@ -166,9 +171,11 @@ constexpr int kNumCfgs = 4;
 
 size_t trace_smem_bytes(int cfg);
 // Resident blocks per SM of the forward / adjoint / variant kernels.
-int trace_blocks_per_sm(int which /*0 forward, 1 adjoint, 2 variant*/, int cfg);
+int trace_blocks_per_sm(int which /*0 forward, 1 adjoint, 2 variant, 3 collecting pass*/, int cfg);
 // once per handle: kernel attributes (dynamic shared memory opt-ins)
 cudaError_t trace_init();
+// Traversal-only pass that fills the hit cache with every query of the march.
+cudaError_t launch_collect(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);
@@ -178,6 +185,9 @@ int sec_blocks_per_sm(int which /*0 trace (levels >= 1), 1 adjoint, 2 primary le
 cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_primary(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s);
+// Sort keys of the records of level p.sec.level (cap of them; the unused
+// slots get 0xFFFFFFFF and sort last) and their indices, for sort_pairs.
+cudaError_t launch_sec_sort_keys(const TraceParams& p, uint32_t* keys, uint32_t* vals, cudaStream_t s);
 cudaError_t launch_sec_backward(const TraceParams& p, int grid, cudaStream_t s);
 // camera.cu: primary rays of up to kMaxViews pinhole cameras (tt_camera_rays)
 cudaError_t launch_camera_rays(const tt_camera* cams, int n, cudaStream_t s);

@@ -393,6 +393,18 @@ class OptixTracer:
         modes = {"auto": _lib.TT_TRAVERSAL_AUTO, "packets": _lib.TT_TRAVERSAL_PACKETS, "lanes": _lib.TT_TRAVERSAL_LANES}
         check(self._h, lib.tt_set_traversal(self._h, modes[traversal], int(k), int(stack_depth)))
 
+    def set_split_forward(self, on: bool = True):
+        """With a hit cache, run the plain forward as a traversal-only pass
+        that stores every query followed by a shading pass that replays them
+        (default), or as one fused kernel (False). The results are the same."""
+        check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_SPLIT_FORWARD, 1 if on else 0))
+
+    def set_sort_secondary(self, on: bool = True):
+        """Trace each level of spawned secondary rays sorted by direction
+        octant and origin (default) or in spawn order (False). The results
+        are the same."""
+        check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_SORT_SECONDARY, 1 if on else 0))
+
     def _scene_fwd_args(self, triangles_points, sigma, num_points_per_triangle, cumsum_of_points_per_triangle,
                         number_of_points, shs, sh_degree, opacities, scaling, density_factor, bg_color,
                         rebuild_gas_opt, max_blending):

@@ -237,6 +237,22 @@ int tt_backward_views(tt_tracer* h, const tt_bwd_args* a, const tt_view* views, 
  * used by the autotuner. No reference counterpart. */
 int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
 
+/* Execution options of a handle (no reference counterpart); none changes a
+ * result, only how the work is scheduled.
+ * TT_OPT_SPLIT_FORWARD, 1 (default): a plain forward given a hit cache runs
+ *   as two kernels, a traversal-only pass that makes every k-closest query
+ *   of each ray's march and stores it in the cache, then a shading pass that
+ *   replays them. The first needs far fewer registers, so more warps hide
+ *   the latency of the node and triangle loads. 0: one fused kernel that
+ *   traverses and shades.
+ * TT_OPT_SORT_SECONDARY, 1 (default): the secondary-ray passes trace each
+ *   level of spawned rays in order of direction octant and origin (Morton
+ *   code), after a radix sort of the level, so the rays of a warp cross
+ *   nearly the same BVH nodes. 0: in the order they were spawned. */
+#define TT_OPT_SPLIT_FORWARD 1
+#define TT_OPT_SORT_SECONDARY 2
+int tt_set_option(tt_tracer* h, int option, int value);
+
 /* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the
  * handle's current traversal configuration, with a pool for later queries of
  * a quarter of the rays: 32 + (k + 1) * 8 * rays + (k + 2) * 8 * ceil(rays / 4).

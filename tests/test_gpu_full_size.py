@@ -199,3 +199,59 @@ def test_batched_views_sample_matches_fp64_oracle(oracle):
         assert np.linalg.norm(want) > 0, key
         e = rel_norm(got.cpu().numpy(), want)
         assert e < GRAD_RTOL, (key, e)
+
+
+def test_secondary_passes_sample_matches_fp64_oracle(oracle):
+    """The secondary-ray passes at their benchmark configuration: 500k
+    triangles, 20 % dielectric (IOR ~ U[1.3, 1.6]), a 512x1024 environment
+    map, 2 views of 800x800 stacked into one [1600, 800] image, up to 2
+    bounces. Pixels' ray trees are independent, so a seeded sample of 4096
+    pixels of the full launch must equal the FP64 oracle's sec_radiance of
+    those rays alone, and the full adjoint with the upstream gradient
+    non-zero only on the sample must equal the oracle's sec_backward of the
+    sample (same bars as the plain path)."""
+    P3 = 500_000
+    sc = scenes.make_scene(P3, seed=0)
+    sec = scenes.secondary_inputs(P3, seed=0)
+    cams = scenes.sphere_cameras(2, 800, 800, seed=3)
+    rays = [scenes.camera_rays(c) for c in cams]
+    ro = np.ascontiguousarray(np.concatenate([r[0] for r in rays], 0))
+    rd = np.ascontiguousarray(np.concatenate([r[1] for r in rays], 0))
+    HH, WW = ro.shape[:2]
+    idx = np.sort(np.random.default_rng(17).choice(HH * WW, N_SAMPLE, replace=False))
+    ro_s, rd_s = ro.reshape(-1, 3)[idx][None].copy(), rd.reshape(-1, 3)[idx][None].copy()
+    ref = oracle.forward(sc, ro_s, rd_s, precision=64, exact=True, canonical=True, record=256, nthreads=8,
+                         secondary=sec)
+    ok = ref.margin > MARGIN
+    assert ok.mean() > 0.95, ok.mean()
+    g_s, go_s = scenes.upstream_grads(1, N_SAMPLE, seed=21, others_std=1.0)
+    g_s, go_s = g_s * ok[None, None], go_s * ok[None, None]
+    g = np.zeros((3, HH, WW), np.float32)
+    go = np.zeros((7, HH, WW), np.float32)
+    g.reshape(3, -1)[:, idx] = g_s[:, 0]
+    go.reshape(7, -1)[:, idx] = go_s[:, 0]
+    dv = dict(verts=T(sc.verts.reshape(-1)), sigma=T(sc.sigma), npts=T(sc.num_points), cums=T(sc.cumsum),
+              shs=T(sc.shs), opac=T(sc.opacities), mat=T(sec["material"]), ior=T(sec["ior"]), env=T(sec["env"]))
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.reset_stats()
+    color, others, _ = tr.trace_forward_secondary(
+        T(ro), T(rd), dv["verts"], dv["sigma"], dv["npts"], dv["cums"], P3, dv["shs"], 3, dv["opac"],
+        torch.zeros(P3, device=DEV), torch.zeros(P3, device=DEV), dv["mat"], dv["ior"], dv["env"], 2)
+    grads = tr.trace_backward_secondary(
+        T(ro), T(rd), dv["verts"], dv["sigma"], dv["npts"], dv["cums"], color, others, P3, dv["shs"], 3, dv["opac"],
+        T(g), T(go), dv["mat"], dv["ior"], dv["env"], 2)
+    torch.cuda.synchronize()
+    tr.device_status()
+    assert tr.stats()["rays"] > HH * WW * 1.2  # spawned rays went through the queue
+    for got, want in ((color, ref.color), (others, ref.others)):
+        a = got.reshape(got.shape[0], -1)[:, idx].cpu().numpy()[:, ok]
+        b = want.reshape(want.shape[0], -1)[:, ok]
+        err = np.abs(a - b)
+        assert np.all(err <= RTOL * np.abs(b) + ATOL), float((err / (RTOL * np.abs(b) + ATOL)).max())
+    rb = oracle.backward(sc, ro_s, rd_s, ref.color, ref.others, g_s, go_s, precision=64, exact=True, canonical=True,
+                         nthreads=8, secondary=sec)
+    for got, key in zip(grads, ("dtri", "dsigma", "dopac", "dsh")):
+        want = getattr(rb, key)
+        assert np.linalg.norm(want) > 0, key
+        e = rel_norm(got.cpu().numpy(), want)
+        assert e < GRAD_RTOL, (key, e)

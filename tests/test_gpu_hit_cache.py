@@ -231,3 +231,49 @@ def test_autograd_pool_grows_to_the_later_queries(setup):
         seen.append((st["hit_cache_replays"], st["queries"]))
     assert seen[0][0] < seen[0][1], seen  # the quarter-of-the-rays pool did not hold every later query
     assert seen[2][0] == seen[2][1], seen
+
+
+@pytest.mark.parametrize("incl", [True, False], ids=["closed", "open"])
+@pytest.mark.parametrize("mode,k,sd", [("packets", 32, 0), ("packets", 16, 0), ("lanes", 16, 32), ("lanes", 16, 24)])
+def test_split_forward_equals_fused(setup, mode, k, sd, incl):
+    """With a hit cache the forward runs as a traversal-only pass that stores
+    every query and a shading pass that replays them. Its outputs equal the
+    fused kernel's bit for bit, its cache serves the adjoint as well (every
+    query replayed when the pool holds them all), and the gradients equal the
+    fused forward's up to the order of float atomics; also with proposed
+    intervals, whose continuations the shading pass traverses itself."""
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", tmin_inclusive=incl, traversal=mode)
+    tr.set_traversal(mode, k=k, stack_depth=sd or 32)
+    R = H * W
+    rng = np.random.default_rng(5)
+    # intervals: a far clip inside the hits for half the rays (continuations), none for the rest
+    far = np.where(rng.random((H, W)) < 0.5, 2.9, np.inf).astype(np.float32)
+    iv = T(np.stack([np.zeros((H, W), np.float32), far]))
+    for interval in (None, iv):
+        outs = {}
+        for split in (False, True):
+            tr.set_split_forward(split)
+            cache = tr.new_hit_cache(R, pool=4 * R)
+            if interval is None:
+                col, oth = forward(tr, sc, s, ro, rd, cache)
+                grads, replays = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+            else:
+                (col, oth), = [(c, o) for c, o in tr.trace_forward_views(
+                    [(ro, rd)], s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3, s["opac"],
+                    torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), torch.zeros(3, device=DEV), 0,
+                    intervals=[interval], hit_cache=cache)[0]]
+                tr.reset_stats()
+                grads = tr.trace_backward_views([(ro, rd)], [(col, oth)], [(g, go)], s["verts"], s["sigma"],
+                                                s["npts"], s["cums"], sc.P, s["shs"], 3, s["opac"],
+                                                torch.zeros(3, device=DEV), intervals=[interval], hit_cache=cache)
+                grads = [x.cpu().numpy() for x in grads]
+                replays = tr.stats()["hit_cache_replays"]
+                tr.device_status()
+            outs[split] = (col.cpu().numpy(), oth.cpu().numpy(), grads, replays)
+        a, b = outs[False], outs[True]
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
+        assert_grads_equal(b[2], a[2])
+        assert b[3] > 0
+    tr.set_split_forward(True)

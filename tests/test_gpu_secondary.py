@@ -158,3 +158,21 @@ def test_adjoint_replays_the_ray_tree_queries(setup):
     assert n0 == 0
     for x, y, name in zip(replayed, traced, ("dtri", "dsigma", "dopac", "dsh")):
         assert rel_norm(x, y) < 1e-6, name
+
+
+def test_sorted_levels_equal_spawn_order(setup):
+    """Tracing each level of spawned rays in sorted order (direction octant,
+    origin Morton code) changes only the schedule: the images are the same
+    bit for bit and the gradients up to the order of float atomics."""
+    sc, ro, rd, sec = setup
+    g, go = scenes.upstream_grads(H, W, seed=13, others_std=1.0)
+    outs = []
+    for on in (False, True):
+        tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+        tr.set_sort_secondary(on)
+        outs.append(gpu_secondary(tr, sc, ro, rd, sec, g, go, 2))
+    a, b = outs
+    for key in ("color", "others", "max_blending", "scaling", "density"):
+        np.testing.assert_array_equal(a[key], b[key])
+    for x, y, name in zip(a["grads"], b["grads"], ("dtri", "dsigma", "dopac", "dsh")):
+        assert rel_norm(x, y) < 1e-6, name
