@@ -340,7 +340,18 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
-    ms_plain = timed(lambda: fwd_bwd(None))
+    # every timing below in both forward schedules (one fused kernel, or a
+    # traversal-only pass and a shading pass); the better one counts
+    def both(fn):
+        out = {}
+        for split in (False, True):
+            tr.set_split_forward(split)
+            out["split" if split else "fused"] = timed(fn)
+        tr.set_split_forward(False)
+        return out
+
+    ms_plain_modes = both(lambda: fwd_bwd(None))
+    ms_plain = min(ms_plain_modes.values())
     recs = [torch.empty((3, ro.shape[0], ro.shape[1]), device=dev) for ro, _ in held]
     ref_outs, ref_g = fwd_bwd(None, recs)
     ref_col = torch.stack([c for c, _ in ref_outs]).clone()
@@ -349,8 +360,8 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
     perfect = [torch.stack([torch.where(torch.isfinite(r[0]), r[0], torch.zeros_like(r[0])),
                             torch.where(r[2] > 0.5, r[1], torch.full_like(r[1], float("inf")))]) for r in recs]
     perfect_far = [torch.stack([torch.zeros_like(p[0]), p[1]]) for p in perfect]
-    ms_perfect = timed(lambda: fwd_bwd(perfect))
-    ms_perfect_far = timed(lambda: fwd_bwd(perfect_far))
+    ms_perfect = min(both(lambda: fwd_bwd(perfect)).values())
+    ms_perfect_far = min(both(lambda: fwd_bwd(perfect_far)).values())
 
     center = tuple(float(x) for x in sc.verts.reshape(-1, 3).mean(0))
     prop = proposal.Proposal(tr, seed=seed, center=center)
@@ -366,7 +377,8 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
     n_steps = len(losses)
     ivs = prop.intervals(held)
     ms_infer = timed(lambda: prop.intervals(held, out=ivs))
-    ms_prop = timed(lambda: fwd_bwd(ivs))
+    ms_prop_modes = both(lambda: fwd_bwd(ivs))
+    ms_prop = min(ms_prop_modes.values())
     tr.reset_stats()
     outs, g = fwd_bwd(ivs)
     st = tr.stats()
@@ -383,6 +395,8 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
         "plain_mrays": R / ms_plain / 1e3,
         "proposal_mrays": R / (ms_prop + ms_infer) / 1e3,
         "speedup": ms_plain / (ms_prop + ms_infer),
+        "mrays_by_schedule": {"plain": {k: R / v / 1e3 for k, v in ms_plain_modes.items()},
+                              "proposal": {k: R / (v + ms_infer) / 1e3 for k, v in ms_prop_modes.items()}},
         "perfect_interval_mrays": R / ms_perfect / 1e3,
         "perfect_far_only_mrays": R / ms_perfect_far / 1e3,
         "image_rmse_vs_plain": rmse, "grad_rel_err_vs_plain": grad_rel,
@@ -694,6 +708,8 @@ def main():
     ap.add_argument("--no-c1", action="store_true", help="skip the 100k-triangle, one-view leg")
     ap.add_argument("--no-hit-cache", action="store_true",
                     help="adjoint re-traverses every query instead of replaying the forward's")
+    ap.add_argument("--split-forward", action="store_true",
+                    help="run the plain forward as a traversal-only pass plus a shading pass")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
                     help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
@@ -738,6 +754,7 @@ def main():
 
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
     tr.build_tri_accel(verts, cums, P, True)
+    tr.set_split_forward(args.split_forward)
     use_cache = not args.no_hit_cache
 
     def step(cached=use_cache):
@@ -824,6 +841,14 @@ def main():
     # ---------------- roofline of the dominant kernel (adjoint)
     fwd_ms, bwd_ms = timed_kernels(3)
     fwd_plain_ms, bwd_retrace_ms = timed_kernels(2, cached=False) if use_cache else (fwd_ms, bwd_ms)
+    fwd_split_ms = fwd_fused_ms = None
+    if use_cache:
+        tr.set_split_forward(not args.split_forward)
+        step()  # first launches of the other schedule's kernels, untimed
+        other_ms = timed_kernels(3)[0]
+        tr.set_split_forward(args.split_forward)
+        fwd_split_ms = fwd_ms if args.split_forward else other_ms
+        fwd_fused_ms = other_ms if args.split_forward else fwd_ms
     rays_step = st["rays"] / args.steps
     evals = st["evaluated_hits"] / args.steps
     blends = st["blended_hits"] / args.steps
@@ -992,6 +1017,7 @@ def main():
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
                      "forward_ms": fwd_ms, "adjoint_ms": bwd_ms,
                      "forward_without_cache_ms": fwd_plain_ms, "adjoint_retrace_ms": bwd_retrace_ms,
+                     "forward_split_ms": fwd_split_ms, "forward_fused_ms": fwd_fused_ms,
                      "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
         "cpu_baseline": cpu,
         "proposal": prop,

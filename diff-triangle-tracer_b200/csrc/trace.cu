@@ -676,6 +676,35 @@ __device__ __noinline__ void compute_scaling(float* __restrict__ scaling, const 
   scaling[prim] = (float)best;
 }
 
+// computeScaling in the reference's own FP32 arithmetic (forward.cu:25-74:
+// centroid as a sum times 1/n, angle = acos of the clamped cosine), for the
+// reference-arithmetic mode; the default computes it in FP64 above.
+__device__ __noinline__ void compute_scaling_ref(float* __restrict__ scaling, const float* __restrict__ verts,
+                                                 const int* __restrict__ cumsum, const int* __restrict__ num_points,
+                                                 int prim, float3 o) {
+  using namespace vf;
+  if (scaling[prim] > 0.0f) return;
+  const int off = cumsum[prim], np = num_points[prim];
+  float3 cen = make_float3(0.f, 0.f, 0.f);
+  for (int i = 0; i < np; ++i) {
+    const float* v = verts + 3 * (size_t)(off + i);
+    cen = add(cen, make_float3(v[0], v[1], v[2]));
+  }
+  cen = scale(cen, div(1.0f, (float)np));
+  const float3 t2o = sub(cen, o);
+  const float lt = __fsqrt_rn(dot(t2o, t2o));
+  float best = 0.0f;
+  for (int i = 0; i < np; ++i) {
+    const float* v = verts + 3 * (size_t)(off + i);
+    const float3 a = sub(make_float3(v[0], v[1], v[2]), o);
+    const float lab = mul(__fsqrt_rn(dot(a, a)), lt);
+    float ang = 0.0f;
+    if (!(lab < 1e-12f)) ang = acosf(fmaxf(-1.0f, fminf(1.0f, div(dot(a, t2o), lab))));
+    best = fmaxf(ang, best);
+  }
+  scaling[prim] = best;
+}
+
 // ---------------------------------------------------------------- the march
 // Per-thread shared memory: the traversal stack and the 16 keys of the
 // current chunk (staged out of registers before shading starts).
@@ -1251,7 +1280,10 @@ struct FwdShader {
     }
     ++n_blend;
     p.density[prim] = 1.0f;
-    compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
+    if constexpr (MODE == kShadeRefArith)
+      compute_scaling_ref(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
+    else
+      compute_scaling(p.scaling, p.verts, p.cumsum, p.num_points, (int)prim, o);
     const float w = alpha * T;
     atomicMax(reinterpret_cast<int*>(p.max_blending) + prim, __float_as_int(w));
     N0 += g.n.x * w;
@@ -1306,6 +1338,10 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
   Counters cnt;
   FwdShader<MODE> sh(p, smem_bytes_for<CFG>());
   run<CFG>(p, sh, cnt);
+  // queries = those the march used, traversed here or replayed from the
+  // collecting pass; hit_cache_replays counts the adjoint's replays only
+  cnt.queries += cnt.replays;
+  cnt.replays = 0;
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
@@ -1342,7 +1378,9 @@ __global__ void __launch_bounds__(kTraceThreads, kCollectBlocks) k_collect(const
   Counters cnt;
   MarchShader sh(p);
   run<CFG>(p, sh, cnt);
-  // traversal counters only: rays and hits are counted by the shading pass
+  // the traversal work (node visits, triangle tests) only: rays, hits and the
+  // queries the march used are counted by the shading pass
+  cnt.queries = 0;
   add_stats(p.stats, 0u, 0u, 0u, cnt);
 }
 

@@ -165,6 +165,6 @@ def test_backward_vs_reference(oracle, reference, c2, which):
         if mode == "reference_arithmetic":
             for k, v in errs.items():
                 assert v <= GRAD_RTOL, (k, v)
-        else:
+        else:  # the reference's own FP32 vertex gradient is the noisiest part
             for k, v in errs.items():
-                assert v <= 1e-2, (k, v)
+                assert v <= (5e-2 if k == "dtri" else 5e-3), (k, v)
