@@ -340,14 +340,17 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
-    # every timing below in both forward schedules (one fused kernel, or a
-    # traversal-only pass and a shading pass); the better one counts
+    # every timing below under each forward schedule (one fused kernel, or a
+    # traversal-only pass storing each ray's first query or all its queries
+    # plus a shading pass); the best one counts, for each arm separately
     def both(fn):
         out = {}
-        for split in (False, True):
+        for name, split, collect in (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0)):
             tr.set_split_forward(split)
-            out["split" if split else "fused"] = timed(fn)
-        tr.set_split_forward(False)
+            tr.set_collect_queries(collect)
+            out[name] = timed(fn)
+        tr.set_split_forward(True)
+        tr.set_collect_queries(1)
         return out
 
     ms_plain_modes = both(lambda: fwd_bwd(None))
@@ -615,7 +618,7 @@ def views_leg(dev, name, steps, warmup=3, no_autotune=False, world=1, local=0, s
         "config": {"workload": name, "triangles": P, "views": len(shapes),
                    "resolutions": [f"{h}x{w}" for h, w in shapes], "rays_per_step": R,
                    "step": "one CUDA-graph replay: refit + forward + adjoint over all views",
-                   "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
+                   "traversal": ({k: tuned.get(k) for k in ("traversal", "k", "stack_depth", "split", "collect")} if tuned else "default"),
                    "autotune_ms": tuned.get("all") if tuned else None,
                    "hit_cache": {"pool_queries": cache_use["pool_cap"], "later_queries": cache_use["pool_used"],
                                  "replays_per_ray": st["hit_cache_replays"] / max(st["rays"], 1),
@@ -710,6 +713,8 @@ def main():
                     help="adjoint re-traverses every query instead of replaying the forward's")
     ap.add_argument("--split-forward", action="store_true",
                     help="run the plain forward as a traversal-only pass plus a shading pass")
+    ap.add_argument("--collect-queries", type=int, default=None,
+                    help="split forward: queries per ray the traversal-only pass stores (0 = all)")
     ap.add_argument("--traversal", default=None, choices=["packets16", "packets32", "lanes32", "lanes24"],
                     help="fix the traversal configuration instead of autotuning it")
     args = ap.parse_args()
@@ -755,6 +760,8 @@ def main():
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
     tr.build_tri_accel(verts, cums, P, True)
     tr.set_split_forward(args.split_forward)
+    if args.collect_queries is not None:
+        tr.set_collect_queries(args.collect_queries)
     use_cache = not args.no_hit_cache
 
     def step(cached=use_cache):
@@ -998,7 +1005,7 @@ def main():
                                  if use_cache else "off: the adjoint re-traverses every query"),
                    "l2": "inputs larger than L2 (scene + BVH + rays ~0.5 GB per step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "traversal": ({k: tuned[k] for k in ("traversal", "k", "stack_depth")} if tuned else "default"),
+                   "traversal": ({k: tuned.get(k) for k in ("traversal", "k", "stack_depth", "split", "collect")} if tuned else "default"),
                    "hits_per_ray": {"evaluated": evals / max(rays_step, 1), "blended": blends / max(rays_step, 1)},
                    "traversal_per_ray": {k: st[k] / max(st["rays"], 1)
                                          for k in ("queries", "node_visits", "triangle_tests",

@@ -19,7 +19,8 @@ struct tt_tracer {
   int device = 0;
   int num_sms = 148;
   int fwd_grid = 0, bwd_grid = 0, collect_grid = 0;
-  bool split_forward = false; // plain forward with a hit cache: collecting pass + shading pass
+  bool split_forward = true;  // plain forward with a hit cache: collecting pass + shading pass
+  int collect_queries = 1;    // queries a ray's collecting pass stores at most (0 = all)
   bool sort_secondary = true; // secondary passes: spawned rays traced in sorted order
   tt::DevBuf sec_sort;        // their sort keys / indices (2 x 2 x 4R words) and the sort's histogram
   int cfg_id = tt::kCfgPackets16;
@@ -186,6 +187,10 @@ int tt_set_option(tt_tracer* h, int option, int value) {
   switch (option) {
     case TT_OPT_SPLIT_FORWARD: h->split_forward = value != 0; return TT_OK;
     case TT_OPT_SORT_SECONDARY: h->sort_secondary = value != 0; return TT_OK;
+    case TT_OPT_COLLECT_QUERIES:
+      TT_REQUIRE(h, value >= 0, "collect_queries must be >= 0");
+      h->collect_queries = value;
+      return TT_OK;
     default: return fail(h, TT_ERR_INVALID, "unknown option");
   }
 }
@@ -361,9 +366,10 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
     // traversal-only pass: every query of the march into the cache; the
     // shading pass below replays them
     TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
+    p.collect_queries = h->collect_queries;
     TT_CUDA(h, tt::launch_collect(p, h->collect_grid, s));
     ++h->trace_launches;
-    p.cache_mode = tt::kCacheRead;
+    p.cache_mode = tt::kCacheFill;
   }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   TT_CUDA(h, tt::launch_forward(p, h->fwd_grid, s));

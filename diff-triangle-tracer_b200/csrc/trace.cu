@@ -883,7 +883,7 @@ __device__ __forceinline__ unsigned long long* cache_pool(const TraceParams& p) 
 
 template <int K>
 __device__ __forceinline__ bool cache_replays(const TraceParams& p) {
-  if (p.cache_mode != kCacheRead) return false;
+  if (p.cache_mode != kCacheRead && p.cache_mode != kCacheFill) return false;
   const HitCacheHeader* h = cache_header_ptr(p);
   return h->magic == kHitCacheMagic && h->k == (uint32_t)K && h->rays == p.cache_rays && h->gen == p.cache_gen &&
          h->pool_cap == p.cache_pool_cap;
@@ -940,6 +940,15 @@ __device__ __forceinline__ float cache_get(const TraceParams& p, bool first, lon
   const unsigned long long w = __ldcs(rows + K * S);
   next = (uint32_t)(w >> 32);
   return __uint_as_float((uint32_t)w);
+}
+
+// Fill mode: the word where the entry of the query after the one replayed
+// from the main part (first) or from pool entry e gets linked.
+template <int K>
+__device__ __forceinline__ uint32_t* cache_link_of(const TraceParams& p, bool first, long long g, uint32_t e) {
+  unsigned long long* w = first ? cache_main(p) + g + (size_t)K * p.cache_rays
+                                : cache_pool<K>(p) + e + (size_t)K * p.cache_pool_cap;
+  return reinterpret_cast<uint32_t*>(w) + 1;
 }
 
 // Adjoint: does pool entry e hold the query that starts at key_min?
@@ -1018,13 +1027,14 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
     if (have) {
       const bool first = cur.chunks == 0;  // the ray's queries are numbered by its chunks
       if (replay && (first || cache_has<K>(p, next, cur.key_min))) {  // as the forward found it
+        if (p.cache_mode == kCacheFill) link = cache_link_of<K>(p, first, g, next);
         t_drop = cache_get<K>(p, first, g, next, sm, next);
         ++cnt.replays;
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
         query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
-        if (p.cache_mode == kCacheWrite) {
+        if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (first) {
             link = cache_put_first<K>(p, g, sm, t_drop);
           } else if (link) {
@@ -1041,6 +1051,8 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
         atomicOr(p.status, kStatusTimeout);
         done = true;
       }
+      // the collecting pass stores at most collect_queries queries a ray
+      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
       if (done) {
         if (sh.next(o, d)) {  // another ray of the same pixel (envlight samples)
           cur = first_cursor(p.tmin_inclusive);
@@ -1102,12 +1114,13 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       if (__any_sync(full, trav))
         packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
       if (rep) {
+        if (p.cache_mode == kCacheFill) link = cache_link_of<K>(p, first, g, next);
         t_drop = cache_get<K>(p, first, g, next, sm, next);
         ++cnt.replays;
       } else {
         next = kNoEntry;
       }
-      if (p.cache_mode == kCacheWrite) {
+      if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
         if (first) {
           if (trav) link = cache_put_first<K>(p, g, sm, t_drop);
         } else {
@@ -1122,6 +1135,8 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
           atomicOr(p.status, kStatusTimeout);
           done = true;
         }
+        // the collecting pass stores at most collect_queries queries a ray
+        if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
         if (done) {
           sh.end();
           active = false;
@@ -1356,8 +1371,12 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 // no shading state or code the pass needs far fewer registers than the fused
 // kernel, so more warps per SM hide the latency of the node and triangle
 // loads, which is what bounds the traversal.
+// 5 blocks of 128 threads (96 registers, no spills): 20 warps per SM
+// against the fused kernel's 16. At 6 blocks (80 registers) ~170 bytes a
+// thread spill and the pass is slower (1M triangles, 4 x 800^2 rays:
+// split forward 18.3 ms at 6 blocks, 16.0 at 5; fused 18.3).
 #ifndef TT_COLLECT_BLOCKS
-#define TT_COLLECT_BLOCKS 6
+#define TT_COLLECT_BLOCKS 5
 #endif
 constexpr int kCollectBlocks = TT_COLLECT_BLOCKS;
 
@@ -1904,6 +1923,8 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
         atomicOr(p.status, kStatusTimeout);
         done = true;
       }
+      // the collecting pass stores at most collect_queries queries a ray
+      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
       if (done) {
         sh.end();
         have = false;

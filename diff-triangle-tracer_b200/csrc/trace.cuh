@@ -55,7 +55,10 @@ __host__ __device__ inline size_t hit_cache_main_bytes(int k, long long rays) {
 __host__ __device__ inline size_t hit_cache_bytes(int k, long long rays) {
   return hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)((rays + 3) / 4);
 }
-constexpr int kCacheOff = 0, kCacheWrite = 1, kCacheRead = 2;
+// Cache modes: off; write (the forward stores its queries); read (the
+// adjoint replays them); fill (the shading pass of the split forward replays
+// what the collecting pass stored and stores the queries it traverses).
+constexpr int kCacheOff = 0, kCacheWrite = 1, kCacheRead = 2, kCacheFill = 3;
 
 // Secondary-ray passes: one record per ray of each pixel's ray tree
 // (64 bytes). Level 0 holds the primary rays (record i = pixel i of view 0;
@@ -130,6 +133,7 @@ struct TraceParams {
   int tmin_inclusive;
   int mode;     // kShade*: how the plain forward / adjoint shade a hit
   int cfg;      // traversal configuration, kCfg*
+  int collect_queries;  // collecting pass: queries stored per ray at most (0 = all the march makes)
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)

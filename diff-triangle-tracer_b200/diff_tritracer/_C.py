@@ -399,6 +399,11 @@ class OptixTracer:
         (default), or as one fused kernel (False). The results are the same."""
         check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_SPLIT_FORWARD, 1 if on else 0))
 
+    def set_collect_queries(self, n: int = 1):
+        """Queries per ray the split forward's traversal-only pass stores at
+        most (0: all of the march's); the shading pass traverses the rest."""
+        check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_COLLECT_QUERIES, int(n)))
+
     def set_sort_secondary(self, on: bool = True):
         """Trace each level of spawned secondary rays sorted by direction
         octant and origin (default) or in spawn order (False). The results

@@ -1,6 +1,8 @@
 """Autotuner of the traversal configuration: rays per warp (one 8x4-pixel
 packet per warp, or one independent ray per lane), hits gathered per traversal
-k (16 or 32) and the per-lane stack depth (32 or 24).
+k (16 or 32), the per-lane stack depth (32 or 24) and, for packets, the
+forward's schedule (one fused kernel, or a traversal-only pass plus a shading
+pass).
 
 `autotune(tracer, step)` times `step()` (a callable running the workload on
 `tracer`, e.g. ViewBatch.step or a forward+backward pass) under every
@@ -17,12 +19,26 @@ import os
 
 import torch
 
-CANDIDATES = (
-    {"traversal": "packets", "k": 16, "stack_depth": 0},
-    {"traversal": "packets", "k": 32, "stack_depth": 0},
-    {"traversal": "lanes", "k": 16, "stack_depth": 32},
-    {"traversal": "lanes", "k": 16, "stack_depth": 24},
+# Warp packets are also tried with the split forward (a traversal-only pass
+# that stores each ray's queries, then a shading pass that replays them),
+# storing the first query of each ray or all of them: which one wins depends
+# on how many rays end on the transmittance cut-off, whose later queries the
+# traversal-only pass cannot know to skip.
+CANDIDATES = tuple(
+    dict(c, split=split, collect=collect)
+    for c in ({"traversal": "packets", "k": 16, "stack_depth": 0}, {"traversal": "packets", "k": 32, "stack_depth": 0})
+    for split, collect in ((False, 1), (True, 1), (True, 0))
+) + (
+    {"traversal": "lanes", "k": 16, "stack_depth": 32, "split": False, "collect": 1},
+    {"traversal": "lanes", "k": 16, "stack_depth": 24, "split": False, "collect": 1},
 )
+
+
+def apply_config(tracer, c):
+    """Puts configuration `c` (a CANDIDATES entry) on `tracer`."""
+    tracer.set_traversal(c["traversal"], c["k"], c["stack_depth"])
+    tracer.set_split_forward(bool(c.get("split", False)))
+    tracer.set_collect_queries(int(c.get("collect", 1)))
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "diff_tritracer", "autotune.json")
 
@@ -44,12 +60,13 @@ def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int
     cache = _load(cache_path)
     if not force and full_key in cache:
         best = cache[full_key]
-        tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
+        apply_config(tracer, best)
         return best
-    name = lambda c: f"{c['traversal']}/k{c['k']}/s{c['stack_depth']}"  # noqa: E731
+    name = lambda c: (f"{c['traversal']}/k{c['k']}/s{c['stack_depth']}"  # noqa: E731
+                      + (f"/split{c['collect']}" if c.get("split") else ""))
 
     def apply(c):
-        tracer.set_traversal(c["traversal"], c["k"], c["stack_depth"])
+        apply_config(tracer, c)
         if prepare is not None:
             prepare()
         step()  # untimed: first launches, allocations of this configuration
@@ -79,7 +96,7 @@ def autotune(tracer, step, key: str, cache_path: str = DEFAULT_CACHE, iters: int
     timings = [(best_ms[name(c)], c) for c in CANDIDATES]
     ms, best = min(timings, key=lambda x: x[0])
     best = dict(best, ms=ms, all={name(c): t for t, c in timings})
-    tracer.set_traversal(best["traversal"], best["k"], best["stack_depth"])
+    apply_config(tracer, best)
     cache[full_key] = best
     _store(cache_path, cache)
     return best

@@ -248,9 +248,15 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  * TT_OPT_SORT_SECONDARY, 1 (default): the secondary-ray passes trace each
  *   level of spawned rays in order of direction octant and origin (Morton
  *   code), after a radix sort of the level, so the rays of a warp cross
- *   nearly the same BVH nodes. 0: in the order they were spawned. */
+ *   nearly the same BVH nodes. 0: in the order they were spawned.
+ * TT_OPT_COLLECT_QUERIES, n >= 0 (default 1): the traversal-only pass of the
+ *   split forward stores at most n k-closest queries per ray (0: every query
+ *   of the march, also those past the point where the ray's transmittance
+ *   would end it, which that pass cannot know); the shading pass traverses
+ *   for the queries not stored. */
 #define TT_OPT_SPLIT_FORWARD 1
 #define TT_OPT_SORT_SECONDARY 2
+#define TT_OPT_COLLECT_QUERIES 3
 int tt_set_option(tt_tracer* h, int option, int value);
 
 /* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the

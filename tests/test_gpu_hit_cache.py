@@ -233,18 +233,23 @@ def test_autograd_pool_grows_to_the_later_queries(setup):
     assert seen[2][0] == seen[2][1], seen
 
 
+@pytest.mark.parametrize("collect", [1, 0], ids=["first-query", "all-queries"])
 @pytest.mark.parametrize("incl", [True, False], ids=["closed", "open"])
 @pytest.mark.parametrize("mode,k,sd", [("packets", 32, 0), ("packets", 16, 0), ("lanes", 16, 32), ("lanes", 16, 24)])
-def test_split_forward_equals_fused(setup, mode, k, sd, incl):
+def test_split_forward_equals_fused(setup, mode, k, sd, incl, collect):
     """With a hit cache the forward runs as a traversal-only pass that stores
     every query and a shading pass that replays them. Its outputs equal the
     fused kernel's bit for bit, its cache serves the adjoint as well (every
     query replayed when the pool holds them all), and the gradients equal the
     fused forward's up to the order of float atomics; also with proposed
-    intervals, whose continuations the shading pass traverses itself."""
+    intervals, whose continuations the shading pass traverses itself. The
+    collecting pass stores each ray's first query or all of them; the
+    shading pass stores the queries it traverses, so the adjoint replays
+    every query of the march either way."""
     sc, s, ro, rd, g, go = setup
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", tmin_inclusive=incl, traversal=mode)
     tr.set_traversal(mode, k=k, stack_depth=sd or 32)
+    tr.set_collect_queries(collect)
     R = H * W
     rng = np.random.default_rng(5)
     # intervals: a far clip inside the hits for half the rays (continuations), none for the rest
@@ -257,7 +262,9 @@ def test_split_forward_equals_fused(setup, mode, k, sd, incl):
             cache = tr.new_hit_cache(R, pool=4 * R)
             if interval is None:
                 col, oth = forward(tr, sc, s, ro, rd, cache)
+                queries = tr.stats()["queries"]
                 grads, replays = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+                assert replays == queries, (split, replays, queries)
             else:
                 (col, oth), = [(c, o) for c, o in tr.trace_forward_views(
                     [(ro, rd)], s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3, s["opac"],

@@ -21,7 +21,9 @@ rays as the GPU:
     against the FP64 oracle. It is bounded loosely here: the reference's FP32
     edge distances on small triangles far from the origin keep only ~3
     digits, so the reference itself is that far from the FP64 answer.
-Rays whose FP32 threshold decisions (alpha vs 1/255, T(1 - alpha) vs 1e-4)
+`scaling` is written by the first ray that blends a triangle (a race in the
+reference too); it is compared for the one-camera cases, where every such
+ray starts at the same origin. Rays whose FP32 threshold decisions (alpha vs 1/255, T(1 - alpha) vs 1e-4)
 lie within 1e-5 (relative) of flipping are left out of the per-pixel checks,
 and their upstream gradients are zero.
 
@@ -100,7 +102,9 @@ def test_queries_equal_the_references(reference, c2, which, incl):
 
 
 def decisions_ok(oracle, sc, ro, rd, incl=True):
-    """Rays whose FP32 threshold decisions are clear of flipping (the FP32
+    """`scaling` is written by the first ray that blends a triangle (a race in the
+reference too); it is compared for the one-camera cases, where every such
+ray starts at the same origin. Rays whose FP32 threshold decisions are clear of flipping (the FP32
     oracle is bit-identical to the reference's code)."""
     H, W = ro.shape[:2]
     r = oracle.forward(sc, ro, rd, bg=BG, precision=32, tmin_inclusive=incl, record=256, nthreads=8)
@@ -140,7 +144,8 @@ def test_forward_vs_reference(oracle, reference, c2, which):
             skip[flagged_prims(rec, H, W, ok)] = True
             np.testing.assert_array_equal(out["density"][~skip], ref.density[~skip])
             np.testing.assert_allclose(out["max_blending"][~skip], ref.max_blending[~skip], rtol=RTOL, atol=ATOL)
-            np.testing.assert_allclose(out["scaling"][~skip], ref.scaling[~skip], rtol=1e-6, atol=1e-9)
+            if name != "c2_sample":  # one camera: every ray that may write a triangle's scaling agrees
+                np.testing.assert_allclose(out["scaling"][~skip], ref.scaling[~skip], rtol=1e-6, atol=1e-9)
 
 
 @pytest.mark.parametrize("which", ["dense3k", "random20k", "c2_sample"])
