@@ -289,13 +289,19 @@ def algorithmic_bytes(rays, evals, blends, cache_k=0):
     return fwd, bwd
 
 
-def proposal_leg(dev, steps=3, seed=0, small=False):
+def proposal_leg(dev, steps=3, seed=0, small=False, epochs=120):
     """The learned proposal against the plain traversal on the 3M-triangle
     workload: 64 training views of 256x256 (4.2M rays traced by the plain
     tracer), Adam on the tensor-core kernels, then forward + adjoint of 8
     held-out 1920x1080 views (one batched launch each) with and without the
     proposal's intervals, and with the perfect intervals of the plain
-    tracer's own hit records (the clip's upper bound)."""
+    tracer's own hit records (the clip's upper bound).
+
+    Choices made on 2 validation views (other cameras than the 8 test views,
+    same resolution): the far margin, the forward's schedule (fused, or split
+    storing first / all queries), and whether a near clip is used (only if its
+    image RMSE and gradient error against the plain trace stay <= 1e-3 there).
+    Each arm is then timed on the test views under its own best schedule."""
     import time
 
     import torch
@@ -315,75 +321,115 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
              for c in scenes.sphere_cameras(n_train, side, side, seed=1000)]
     held = [tuple(T(a) for a in scenes.camera_rays(c)) for c in scenes.sphere_cameras(n_held, hh, ww, seed=2000)]
     ups = [tuple(T(a) for a in scenes.upstream_grads(hh, ww, seed=3000 + i)) for i in range(n_held)]
+    val = [tuple(T(a) for a in scenes.camera_rays(c)) for c in scenes.sphere_cameras(2, hh, ww, seed=4000)]
+    val_ups = [tuple(T(a) for a in scenes.upstream_grads(hh, ww, seed=5000 + i)) for i in range(2)]
     bg = torch.zeros(3, device=dev)
     R = sum(ro.shape[0] * ro.shape[1] for ro, _ in held)
 
-    def fwd_bwd(intervals, records=None):
+    def fwd_bwd(views, upstream, intervals, records=None):
         z1, z2 = torch.zeros(sc.P, device=dev), torch.zeros(sc.P, device=dev)
-        cache = tr.new_hit_cache(R)  # both arms replay the forward's queries in the adjoint
-        outs, _ = tr.trace_forward_views(held, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"], 3,
+        rays = sum(ro.shape[0] * ro.shape[1] for ro, _ in views)
+        cache = tr.new_hit_cache(rays)  # both arms replay the forward's queries in the adjoint
+        outs, _ = tr.trace_forward_views(views, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"], 3,
                                          S["opac"], z1, z2, bg, 2, intervals=intervals, records=records,
                                          hit_cache=cache)
-        g = tr.trace_backward_views(held, outs, ups, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P, S["shs"],
-                                    3, S["opac"], bg, intervals=intervals, hit_cache=cache)
+        g = tr.trace_backward_views(views, outs, upstream, S["verts"], S["sigma"], S["npts"], S["cums"], sc.P,
+                                    S["shs"], 3, S["opac"], bg, intervals=intervals, hit_cache=cache)
         return outs, g
 
-    def timed(fn):
+    def timed(fn, n=steps):
         for _ in range(2):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(steps):
+        for _ in range(n):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+        return e0.elapsed_time(e1) / n
 
-    # every timing below under each forward schedule (one fused kernel, or a
-    # traversal-only pass storing each ray's first query or all its queries
-    # plus a shading pass); the best one counts, for each arm separately
-    def both(fn):
+    schedules = (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0))
+
+    def set_schedule(name):
+        _, split, collect = next(x for x in schedules if x[0] == name)
+        tr.set_split_forward(split)
+        tr.set_collect_queries(collect)
+
+    def by_schedule(fn, n=steps):
         out = {}
-        for name, split, collect in (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0)):
-            tr.set_split_forward(split)
-            tr.set_collect_queries(collect)
-            out[name] = timed(fn)
-        tr.set_split_forward(True)
-        tr.set_collect_queries(1)
+        for name, _, _ in schedules:
+            set_schedule(name)
+            out[name] = timed(fn, n)
         return out
 
-    ms_plain_modes = both(lambda: fwd_bwd(None))
-    ms_plain = min(ms_plain_modes.values())
+    def best(d):
+        k = min(d, key=d.get)
+        return k, d[k]
+
+    # ---- plain arm and the perfect intervals (plain tracer's own records)
+    ms_plain_modes = by_schedule(lambda: fwd_bwd(held, ups, None))
+    plain_sched, ms_plain = best(ms_plain_modes)
+    set_schedule(plain_sched)
     recs = [torch.empty((3, ro.shape[0], ro.shape[1]), device=dev) for ro, _ in held]
-    ref_outs, ref_g = fwd_bwd(None, recs)
+    ref_outs, ref_g = fwd_bwd(held, ups, None, recs)
     ref_col = torch.stack([c for c, _ in ref_outs]).clone()
     ref_g = [x.clone() for x in ref_g]
-    # perfect intervals: the plain tracer's own first hit and (for terminated rays) last hit
     perfect = [torch.stack([torch.where(torch.isfinite(r[0]), r[0], torch.zeros_like(r[0])),
                             torch.where(r[2] > 0.5, r[1], torch.full_like(r[1], float("inf")))]) for r in recs]
     perfect_far = [torch.stack([torch.zeros_like(p[0]), p[1]]) for p in perfect]
-    ms_perfect = min(both(lambda: fwd_bwd(perfect)).values())
-    ms_perfect_far = min(both(lambda: fwd_bwd(perfect_far)).values())
+    ms_perfect = best(by_schedule(lambda: fwd_bwd(held, ups, perfect)))[1]
+    ms_perfect_far = best(by_schedule(lambda: fwd_bwd(held, ups, perfect_far)))[1]
 
+    # ---- training
     center = tuple(float(x) for x in sc.verts.reshape(-1, 3).mean(0))
     prop = proposal.Proposal(tr, seed=seed, center=center)
     t0 = time.time()
     rays, targets, far_target = proposal.collect(prop, tr, S, train)
     torch.cuda.synchronize()
     t_collect = time.time() - t0
-    prop.far_target, prop.far_cap, prop.margin_far = far_target, far_target - 0.75, 0.3
+    prop.far_target, prop.far_cap = far_target, far_target - 0.75
     t0 = time.time()
-    losses = proposal.fit(prop, rays, targets, epochs=30, batch=65536, lr=1e-3)
+    losses = proposal.fit(prop, rays, targets, epochs=epochs, batch=65536, lr=1e-3)
     torch.cuda.synchronize()
     t_fit = time.time() - t0
     n_steps = len(losses)
+
+    # ---- choices on the validation views
+    set_schedule("fused")
+    val_out, val_g = fwd_bwd(val, val_ups, None)
+    val_col = torch.stack([c for c, _ in val_out]).clone()
+    val_g = [x.clone() for x in val_g]
+    choices = {}
+    for mf in (0.05, 0.1, 0.2, 0.3):
+        ivs = prop.intervals(val, margin_near=proposal.NO_NEAR_CLIP, margin_far=mf)
+        for name, ms in by_schedule(lambda: fwd_bwd(val, val_ups, ivs), n=2).items():
+            choices[(mf, name, "off")] = ms
+    mf_best, sched_best, _ = min(choices, key=choices.get)
+    near_eval = {}
+    for mn in (0.5, 0.25):
+        ivs = prop.intervals(val, margin_near=mn, margin_far=mf_best)
+        set_schedule(sched_best)
+        outs, g = fwd_bwd(val, val_ups, ivs)
+        col = torch.stack([c for c, _ in outs])
+        rmse = float(((col - val_col) ** 2).mean().sqrt())
+        gerr = max(float((a - b).norm() / b.norm()) for a, b in zip(g, val_g))
+        ms = timed(lambda: fwd_bwd(val, val_ups, ivs), n=2)
+        near_eval[mn] = {"rmse": rmse, "grad_rel_err": gerr, "ms": ms}
+        if rmse <= 1e-3 and gerr <= 1e-3:
+            choices[(mf_best, sched_best, mn)] = ms
+    mf_best, sched_best, near = min(choices, key=choices.get)
+    prop.margin_far = mf_best
+    prop.margin_near = proposal.NO_NEAR_CLIP if near == "off" else near
+
+    # ---- the learned arm on the test views
     ivs = prop.intervals(held)
     ms_infer = timed(lambda: prop.intervals(held, out=ivs))
-    ms_prop_modes = both(lambda: fwd_bwd(ivs))
-    ms_prop = min(ms_prop_modes.values())
+    ms_prop_modes = by_schedule(lambda: fwd_bwd(held, ups, ivs))
+    prop_sched, ms_prop = best(ms_prop_modes)
+    set_schedule(prop_sched)
     tr.reset_stats()
-    outs, g = fwd_bwd(ivs)
+    outs, g = fwd_bwd(held, ups, ivs)
     st = tr.stats()
     tr.device_status()
     col = torch.stack([c for c, _ in outs])
@@ -391,13 +437,16 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
     grad_rel = max(float((a - b).norm() / b.norm()) for a, b in zip(g, ref_g))
     hr, ht, _ = proposal.collect(prop, tr, S, held[:2], far_target=far_target)
     stats = proposal.interval_stats(prop, hr, ht)
+    tr.set_split_forward(True)
+    tr.set_collect_queries(1)
     flops_ray = 2 * (3 * 80 * 64 + 80 * 16)
     return {
         "workload": f"{P} triangles; train {n_train} views {side}x{side} ({int(rays.shape[0])} rays); "
-                    f"test {n_held} held-out views {ww}x{hh}",
+                    f"test {n_held} held-out views {ww}x{hh}; margins and schedule chosen on 2 other views",
         "plain_mrays": R / ms_plain / 1e3,
         "proposal_mrays": R / (ms_prop + ms_infer) / 1e3,
         "speedup": ms_plain / (ms_prop + ms_infer),
+        "schedule": {"plain": plain_sched, "proposal": prop_sched},
         "mrays_by_schedule": {"plain": {k: R / v / 1e3 for k, v in ms_plain_modes.items()},
                               "proposal": {k: R / (v + ms_infer) / 1e3 for k, v in ms_prop_modes.items()}},
         "perfect_interval_mrays": R / ms_perfect / 1e3,
@@ -405,9 +454,13 @@ def proposal_leg(dev, steps=3, seed=0, small=False):
         "image_rmse_vs_plain": rmse, "grad_rel_err_vs_plain": grad_rel,
         "intervals": {k: round(v, 4) for k, v in stats.items()},
         "continuations_per_ray": st["interval_continuations"] / max(st["rays"], 1),
-        "margin_far": prop.margin_far, "far_cap": prop.far_cap, "near_clip": "off",
-        "train": {"steps": n_steps, "batch": 65536, "lr": 1e-3, "seconds": t_fit, "collect_s": t_collect,
-                  "loss_first": float(losses[:5].mean()), "loss_last": float(losses[-5:].mean()),
+        "margin_far": prop.margin_far, "far_cap": prop.far_cap,
+        "near_clip": "off" if near == "off" else f"margin {near}",
+        "validation": {"ms": {f"far {k[0]} / {k[1]} / near {k[2]}": v for k, v in choices.items()},
+                       "near_clip": {str(k): v for k, v in near_eval.items()}},
+        "train": {"steps": n_steps, "epochs": epochs, "batch": 65536, "lr": 1e-3, "seconds": t_fit,
+                  "collect_s": t_collect, "loss_first": float(losses[:5].mean()),
+                  "loss_last": float(losses[-5:].mean()),
                   "tflops": 3 * flops_ray * 65536 * n_steps / max(t_fit, 1e-9) / 1e12},
         "inference": {"ms": ms_infer, "tflops": flops_ray * R / (ms_infer / 1e3) / 1e12},
     }
@@ -848,14 +901,26 @@ def main():
     # ---------------- roofline of the dominant kernel (adjoint)
     fwd_ms, bwd_ms = timed_kernels(3)
     fwd_plain_ms, bwd_retrace_ms = timed_kernels(2, cached=False) if use_cache else (fwd_ms, bwd_ms)
-    fwd_split_ms = fwd_fused_ms = None
+    # the forward under each schedule, and the device time of its two passes
+    # (debug events around the traversal-only pass and the shading pass)
+    schedules = {}
     if use_cache:
-        tr.set_split_forward(not args.split_forward)
-        step()  # first launches of the other schedule's kernels, untimed
-        other_ms = timed_kernels(3)[0]
-        tr.set_split_forward(args.split_forward)
-        fwd_split_ms = fwd_ms if args.split_forward else other_ms
-        fwd_fused_ms = other_ms if args.split_forward else fwd_ms
+        cur = (tuned or {}).get("split", args.split_forward), (tuned or {}).get("collect", args.collect_queries or 1)
+        for sname, split, collect in (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0)):
+            tr.set_split_forward(split)
+            tr.set_collect_queries(collect)
+            step()  # first launches of this schedule's kernels, untimed
+            f_ms = timed_kernels(3)[0]
+            passes = []
+            for _ in range(3):
+                cache = tr.new_hit_cache(R)
+                tr.trace_forward(ro, rd, verts, sig, npts, cums, P, shs, 3, empty, opac, scaling, density, bg, extra,
+                                 2, True, hit_cache=cache)
+                passes.append(tr.forward_pass_times())
+            schedules[sname] = {"forward_ms": f_ms, "collect_ms": float(np.mean([x[0] for x in passes])),
+                                "shade_ms": float(np.mean([x[1] for x in passes]))}
+        tr.set_split_forward(bool(cur[0]))
+        tr.set_collect_queries(int(cur[1]))
     rays_step = st["rays"] / args.steps
     evals = st["evaluated_hits"] / args.steps
     blends = st["blended_hits"] / args.steps
@@ -1019,12 +1084,14 @@ def main():
                              "note": "pinned copies of one step's rays / image timed alone before and after the "
                                      "e2e steps (the host link is shared with other jobs)"}},
         "gpu_launches": int(round(launches_per_step * args.steps)),
-        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": dominant + (" (traversal-only pass + shading pass)"
+                                                          if dominant == "forward" and (tuned or {}).get("split")
+                                                          else ""), "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
                      "forward_ms": fwd_ms, "adjoint_ms": bwd_ms,
                      "forward_without_cache_ms": fwd_plain_ms, "adjoint_retrace_ms": bwd_retrace_ms,
-                     "forward_split_ms": fwd_split_ms, "forward_fused_ms": fwd_fused_ms,
+                     "forward_by_schedule": schedules,
                      "forward_frac": fwd_b / (fwd_ms / 1e3) / 1e9 / peak},
         "cpu_baseline": cpu,
         "proposal": prop,

@@ -33,7 +33,8 @@ struct tt_tracer {
   size_t sec_cache_bytes = 0;  // its size for the last tree
   int sec_R = 0, sec_depth = -1;  // the ray tree the last tt_forward_secondary left
   int sec_trace_grid = 0, sec_bwd_grid = 0, sec_primary_grid = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_mid = nullptr;
+  float pass_ms[2] = {0.f, 0.f};  // last debug forward: collecting pass, shading pass (ms)
   unsigned long long trace_launches = 0;  // trace kernels enqueued
   unsigned long long launch_base = 0;     // launch count at the last stats reset
   unsigned long long bvh_gen = 0;         // BVH builds, refits and loads so far (hit cache validity)
@@ -142,6 +143,7 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
       (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
       (e = h->scratch.reserve(128)) != cudaSuccess || (e = cudaMemset(h->scratch.p, 0, 128)) != cudaSuccess ||
       (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess ||
+      (e = cudaEventCreate(&h->ev_mid)) != cudaSuccess ||
       (e = tt::trace_init()) != cudaSuccess) {
     delete h;
     return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
@@ -244,6 +246,7 @@ int tt_destroy(tt_tracer* h) {
   h->sec_cache.release();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->ev_mid) cudaEventDestroy(h->ev_mid);
   delete h;
   return TT_OK;
 }
@@ -362,7 +365,8 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   p.samples = (int)ex[4];
   if (a->P > 0) TT_CUDA(h, cudaMemsetAsync(a->max_blending, 0, (size_t)a->P * sizeof(float), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
-  if (p.hit_cache && h->split_forward) {
+  const bool split = p.hit_cache && h->split_forward;
+  if (split) {
     // traversal-only pass: every query of the march into the cache; the
     // shading pass below replays them
     TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
@@ -371,6 +375,7 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
     ++h->trace_launches;
     p.cache_mode = tt::kCacheFill;
   }
+  if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev_mid, s));
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   TT_CUDA(h, tt::launch_forward(p, h->fwd_grid, s));
   ++h->trace_launches;
@@ -380,7 +385,19 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
     float ms = 0.f;
     TT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (a->gpu_time_ms) *a->gpu_time_ms = ms;
+    float m0 = 0.f, m1 = 0.f;
+    TT_CUDA(h, cudaEventElapsedTime(&m0, h->ev0, h->ev_mid));
+    TT_CUDA(h, cudaEventElapsedTime(&m1, h->ev_mid, h->ev1));
+    h->pass_ms[0] = split ? m0 : 0.f;
+    h->pass_ms[1] = m1;
   }
+  return TT_OK;
+}
+
+int tt_forward_pass_times(tt_tracer* h, float* collect_ms, float* shade_ms) {
+  if (!h) return TT_ERR_INVALID;
+  if (collect_ms) *collect_ms = h->pass_ms[0];
+  if (shade_ms) *shade_ms = h->pass_ms[1];
   return TT_OK;
 }
 

@@ -40,7 +40,7 @@ constexpr int kActBytes = kTileRows * kIn * 2;  // one 128 x 80 BF16 activation 
 constexpr int kDzBytes = kTileRows * kHid * 2;  // one 128 x 64 BF16 gradient tile
 constexpr int kWBytes = kParams * 2;
 constexpr int kWaitLimit = 1 << 20;  // mbarrier polls before a wait gives up
-constexpr uint32_t kInferCols = 64;  // tensor-memory columns: one 128 x 64 accumulator
+constexpr uint32_t kInferCols = 128; // tensor-memory columns: two 128 x 64 accumulators (one per warp group)
 constexpr uint32_t kTrainCols = 512; // accumulator + 4 weight-gradient accumulators (64 + 4 * 80)
 
 __host__ __device__ constexpr int layer_rows(int l) { return l < 3 ? kHid : kOutRows; }
@@ -239,26 +239,51 @@ __device__ __forceinline__ int find_set(const InferParams& p, int tile) {
 }
 
 // ------------------------------------------------------------- inference
-__global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ InferParams p) {
+// Two groups of 4 warps per CTA, each with its own activation tile, mbarrier
+// and 64 tensor-memory columns, run independent tiles over the one shared
+// copy of the weights: while one group waits on its MMA chain (issue ->
+// commit -> mbarrier -> tcgen05.ld -> epilogue -> next layer) the other one
+// works, and the weights' shared memory is paid once for both. Groups
+// synchronise on their own named barriers (1 and 2), the CTA only at the
+// start and the end.
+constexpr int kInferGroups = 2;
+constexpr int kInferThreads = kThreads * kInferGroups;
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kThreads) : "memory");
+}
+__device__ __forceinline__ bool group_and(int g, bool v) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((int)v), "r"(1 + g), "r"(kThreads)
+      : "memory");
+  return r != 0;
+}
+
+__global__ void __launch_bounds__(kInferThreads, 3) k_infer(const __grid_constant__ InferParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* wsm = smem;
-  unsigned char* act = smem + kWBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(act + kActBytes);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + kWBytes + kInferGroups * kActBytes);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(mbars + kInferGroups);
+  const int warp = threadIdx.x >> 5, grp = warp >> 2, tid = threadIdx.x & (kThreads - 1);
+  unsigned char* act = smem + kWBytes + grp * kActBytes;
   load_weights(wsm, p.w);
-  if (tid == 0) mbar_init(smem_addr(mbar));
+  if (threadIdx.x < kInferGroups) mbar_init(smem_addr(mbars + threadIdx.x));
   if (warp == 0) tmem_alloc(smem_addr(slot), kInferCols);
   fence_smem();
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *slot;
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t mb = smem_addr(mbar), a_act = smem_addr(act), a_w = smem_addr(wsm);
+  const uint32_t tbase = *slot;
+  const uint32_t tmem = tbase + 64u * (uint32_t)grp;  // this group's accumulator columns
+  const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  const uint32_t mb = smem_addr(mbars + grp), a_act = smem_addr(act), a_w = smem_addr(wsm);
   uint32_t phase = 0;
   bool ok = true;
-  for (int tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x) {
+  for (int tile = blockIdx.x * kInferGroups + grp; tile < p.ntiles && ok; tile += gridDim.x * kInferGroups) {
     const RaySet& rs = p.sets[find_set(p, tile)];
     const int r = (tile - rs.tile_begin) * kTileRows + tid;
     const bool valid = r < rs.n;
@@ -275,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ I
     put_row<10>(act, tid, x);
     fence_smem();
     fence_before();
-    __syncthreads();
+    group_sync(grp);
     for (int l = 0; l < 4; ++l) {
       if (tid == 0) {
         fence_after();
@@ -284,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ I
       }
       ok = mbar_wait(mb, phase);
       phase ^= 1u;
-      ok = __syncthreads_and(ok);
+      ok = group_and(grp, ok);
       if (!ok) break;
       fence_after();
       if (l < 3) {
@@ -304,14 +329,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_infer(const __grid_constant__ I
         }
       }
       fence_before();
-      __syncthreads();
+      group_sync(grp);
     }
   }
   if (!ok && tid == 0) atomicOr(p.status, kStatusTimeout);
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) tmem_free(tmem, kInferCols);
+  if (warp == 0) tmem_free(tbase, kInferCols);
 }
 
 // ------------------------------------------------------------- training
@@ -504,7 +529,7 @@ __global__ void k_adam(const __grid_constant__ AdamParams p) {
 
 }  // namespace
 
-size_t infer_smem_bytes() { return (size_t)kWBytes + kActBytes + 16; }
+size_t infer_smem_bytes() { return (size_t)kWBytes + (size_t)kInferGroups * kActBytes + 8 * kInferGroups + 16; }
 size_t train_smem_bytes() { return (size_t)kWBytes + 4 * kActBytes + kDzBytes + 16; }
 
 namespace {
@@ -527,7 +552,8 @@ cudaError_t set_attrs() {
 int infer_blocks_per_sm() {
   if (set_attrs() != cudaSuccess) return 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_infer, kThreads, infer_smem_bytes()) != cudaSuccess) n = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_infer, kInferThreads, infer_smem_bytes()) != cudaSuccess)
+    n = 1;
   return n > 0 ? n : 1;
 }
 
@@ -535,7 +561,7 @@ cudaError_t launch_infer(const InferParams& p, int grid, cudaStream_t s) {
   cudaError_t e = set_attrs();
   if (e != cudaSuccess) return e;
   if (p.ntiles == 0) return cudaSuccess;
-  k_infer<<<grid, kThreads, infer_smem_bytes(), s>>>(p);
+  k_infer<<<grid, kInferThreads, infer_smem_bytes(), s>>>(p);
   return cudaGetLastError();
 }
 

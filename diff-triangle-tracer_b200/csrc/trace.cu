@@ -1051,8 +1051,10 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
         atomicOr(p.status, kStatusTimeout);
         done = true;
       }
-      // the collecting pass stores at most collect_queries queries a ray
-      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
+      // the collecting pass stores at most collect_queries queries of a ray
+      // without a far clip; a clipped ray's queries end at t_far anyway
+      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries && cur.t_hi >= kFar)
+        done = true;
       if (done) {
         if (sh.next(o, d)) {  // another ray of the same pixel (envlight samples)
           cur = first_cursor(p.tmin_inclusive);
@@ -1135,8 +1137,10 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
           atomicOr(p.status, kStatusTimeout);
           done = true;
         }
-        // the collecting pass stores at most collect_queries queries a ray
-        if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
+        // the collecting pass stores at most collect_queries queries of a
+        // ray without a far clip; a clipped ray's queries end at t_far anyway
+        if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries && cur.t_hi >= kFar)
+          done = true;
         if (done) {
           sh.end();
           active = false;
@@ -1923,8 +1927,10 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
         atomicOr(p.status, kStatusTimeout);
         done = true;
       }
-      // the collecting pass stores at most collect_queries queries a ray
-      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries) done = true;
+      // the collecting pass stores at most collect_queries queries of a ray
+      // without a far clip; a clipped ray's queries end at t_far anyway
+      if (Shader::kStopsAtClip && p.collect_queries > 0 && cur.chunks >= p.collect_queries && cur.t_hi >= kFar)
+        done = true;
       if (done) {
         sh.end();
         have = false;

@@ -399,6 +399,13 @@ class OptixTracer:
         (default), or as one fused kernel (False). The results are the same."""
         check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_SPLIT_FORWARD, 1 if on else 0))
 
+    def forward_pass_times(self):
+        """(collecting pass ms, shading pass ms) of the last forward run with
+        debug=True (0 for the first when the forward was fused)."""
+        a, b = ctypes.c_float(0.0), ctypes.c_float(0.0)
+        check(self._h, lib.tt_forward_pass_times(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def set_collect_queries(self, n: int = 1):
         """Queries per ray the split forward's traversal-only pass stores at
         most (0: all of the march's); the shading pass traverses the rest."""

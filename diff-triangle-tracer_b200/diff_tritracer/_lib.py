@@ -125,7 +125,8 @@ class TtSecondary(ctypes.Structure):
 EXPORTS = (
     "tt_create", "tt_destroy", "tt_build", "tt_forward", "tt_backward", "tt_last_error",
     "tt_device_status", "tt_hit_stream", "tt_get_stats", "tt_reset_stats", "tt_forward_views",
-    "tt_backward_views", "tt_set_traversal", "tt_set_option", "tt_mlp_update", "tt_mlp_train_step", "tt_mlp_predict",
+    "tt_backward_views", "tt_set_traversal", "tt_set_option", "tt_forward_pass_times", "tt_mlp_update",
+    "tt_mlp_train_step", "tt_mlp_predict",
     "tt_mlp_intervals", "tt_forward_secondary", "tt_backward_secondary", "tt_secondary_tree", "tt_bvh_save",
     "tt_bvh_load", "tt_hit_cache_bytes", "tt_hit_cache_bytes_pool", "tt_hit_cache_usage",
     "tt_camera_rays",
@@ -150,6 +151,7 @@ def _load():
     lib.tt_backward_views.argtypes = [_vp, ctypes.POINTER(TtBwdArgs), ctypes.POINTER(TtView), ctypes.c_int, _vp]
     lib.tt_set_traversal.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.tt_set_option.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    lib.tt_forward_pass_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
     lib.tt_get_stats.argtypes = [_vp, ctypes.POINTER(TtStats), _vp]
     lib.tt_reset_stats.argtypes = [_vp, _vp]
     lib.tt_hit_stream.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]

@@ -114,9 +114,11 @@ def test_autotune_chooses_and_caches(tmp_path):
     cache = tmp_path / "autotune.json"
     best = autotune(tr, vb.step, key="dense3000", cache_path=str(cache), iters=2)
     assert best["traversal"] in ("packets", "lanes") and cache.exists()
-    assert len(best["all"]) == 4
+    from diff_tritracer.autotune import CANDIDATES
+
+    assert len(best["all"]) == len(CANDIDATES) == 8  # 2 packet sizes x 3 forward schedules + 2 lane stacks
     again = autotune(tr, vb.step, key="dense3000", cache_path=str(cache))
-    assert again["traversal"] == best["traversal"] and again["k"] == best["k"]
+    assert all(again[k] == best[k] for k in ("traversal", "k", "stack_depth", "split", "collect"))
     vb.step()
     torch.cuda.synchronize()
     tr.device_status()
