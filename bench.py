@@ -1012,14 +1012,14 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.e2e_steps + 1)]
+    ev[0].record()
     for i in range(args.e2e_steps):  # each timed step uploads one step's rays, gradient and image
         e2e_step(2 + i)
-    e1.record()
+        ev[i + 1].record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = ev[0].elapsed_time(ev[-1])
+    e2e_step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.e2e_steps)]
     e2e_ms = slowest_rank_ms(e2e_ms, world, dev)
     e2e_value = world * R * args.e2e_steps / (e2e_ms / 1e3) / 1e6
     h2d = ro_h.numel() * 4 + rd_h.numel() * 4 + g_h.numel() * 4
@@ -1079,6 +1079,7 @@ def main():
                 "path": "diff_tritracer.Tracer autograd forward+backward, pinned host rays/grads in, image out "
                         "(on a copy stream: gradient upload under the forward; image download and the next "
                         "step's ray upload, double-buffered, under the adjoint)",
+                "step_ms": e2e_step_ms,
                 "link_gbs": {"h2d_before": link_before[0], "d2h_before": link_before[1], "h2d_after": link_after[0],
                              "d2h_after": link_after[1],
                              "note": "pinned copies of one step's rays / image timed alone before and after the "

@@ -253,8 +253,7 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  *   split forward stores at most n k-closest queries per ray (0: every query
  *   of the march, also those past the point where the ray's transmittance
  *   would end it, which that pass cannot know); the shading pass traverses
- *   for the queries not stored. A ray with a finite proposed t_far
- *   (tt_view.interval) has all its queries up to t_far stored. */
+ *   for the queries not stored. */
 /* Device time of the two passes of the last forward on the handle that ran
  * with `debug` (events, as gpu_time_ms): the traversal-only pass (0 for a
  * fused forward) and the shading pass. No reference counterpart. */
