@@ -942,6 +942,13 @@ __device__ __forceinline__ float cache_get(const TraceParams& p, bool first, lon
   return __uint_as_float((uint32_t)w);
 }
 
+// Fill mode: the pool is already exhausted (by the collecting pass). The
+// shading pass then asks for no entry, so a later query the collecting pass
+// was refused is not counted twice in pool_used.
+__device__ __forceinline__ bool cache_pool_full(const TraceParams& p) {
+  return __ldcg(&cache_header_ptr(p)->pool_used) >= p.cache_pool_cap;
+}
+
 // Fill mode: the word where the entry of the query after the one replayed
 // from the main part (first) or from pool entry e gets linked.
 template <int K>
@@ -1037,6 +1044,8 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
         if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (first) {
             link = cache_put_first<K>(p, g, sm, t_drop);
+          } else if (link && p.cache_mode == kCacheFill && cache_pool_full(p)) {
+            link = nullptr;
           } else if (link) {
             const uint32_t e = atomicAdd(&cache_header_ptr(p)->pool_used, 1u);
             link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
@@ -1124,7 +1133,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
         if (first) {
           if (trav) link = cache_put_first<K>(p, g, sm, t_drop);
         } else {
-          const bool more = trav && link != nullptr;
+          const bool more = trav && link != nullptr && !(p.cache_mode == kCacheFill && cache_pool_full(p));
           const uint32_t e = cache_alloc(p, more);
           if (more) link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
         }
@@ -1361,17 +1370,16 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 }
 
 // ---------------------------------------------------------------- collect
-// Traversal pass of the split forward (plain program with a hit cache). It
-// runs every ray's march with a shader that computes only what decides where
-// the march goes (each hit's alpha from the same window-function arithmetic
-// as the shading pass, and the transmittance), not colours or side outputs,
-// and stores every k-closest query in the hit cache. The shading pass
-// (k_forward in fill mode) then makes exactly the same march and replays
-// each query; only a query the cache could not hold (pool full) is
-// traversed again there. Without the shading state and code the pass needs
-// fewer registers than the fused kernel, so more warps per SM hide the
-// latency of the node and triangle loads, which is what bounds the
-// traversal.
+// Traversal-only pass of the split forward (plain program with a hit cache).
+// It runs every ray's march with a shader that shades nothing and never ends
+// a ray early, so it makes, and stores in the hit cache, every k-closest
+// query the plain march would make. The shading pass (k_forward reading the
+// cache) then replays each query its own march asks for; a ray that ends on
+// the transmittance cut-off simply leaves its later queries unread, and a
+// query the cache could not hold (pool full) is traversed again there. With
+// no shading state or code the pass needs far fewer registers than the fused
+// kernel, so more warps per SM hide the latency of the node and triangle
+// loads, which is what bounds the traversal.
 // 5 blocks of 128 threads (96 registers, no spills): 20 warps per SM
 // against the fused kernel's 16. At 6 blocks (80 registers) ~170 bytes a
 // thread spill and the pass is slower (1M triangles, 4 x 800^2 rays:
@@ -1381,40 +1389,22 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 #endif
 constexpr int kCollectBlocks = TT_COLLECT_BLOCKS;
 
-template <int MODE>
 struct MarchShader {
-  static constexpr bool kStopsAtClip = false;
+  static constexpr bool kStopsAtClip = true;
   const TraceParams& p;
-  float3 o, d;
-  float T;
   __device__ explicit MarchShader(const TraceParams& params) : p(params) {}
-  __device__ __forceinline__ bool begin(const ViewDesc*, int, float3 ro, float3 rd) {
-    o = ro;
-    d = rd;
-    T = 1.0f;
-    return true;
-  }
+  __device__ __forceinline__ bool begin(const ViewDesc*, int, float3, float3) { return true; }
   __device__ __forceinline__ bool next(float3&, float3&) { return false; }
   __device__ __forceinline__ void prepare() {}
-  // FwdShader::visit's decisions, with the same arithmetic
-  __device__ __forceinline__ bool visit(uint32_t prim, float t) {
-    const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
-    const Geom g = shade_geom<MODE>(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, t, __ldg(p.sigma + prim));
-    const float alpha = fminf(kAlphaMax, __ldg(p.opac + prim) * g.Cx);
-    if (alpha < kAlphaMin) return false;
-    const float test_T = T * (1.0f - alpha);
-    if (test_T < kTMin) return true;
-    T = test_T;
-    return false;
-  }
+  __device__ __forceinline__ bool visit(uint32_t, float) { return false; }
   __device__ __forceinline__ void end() {}
 };
 
-template <int CFG, int MODE>
+template <int CFG>
 __global__ void __launch_bounds__(kTraceThreads, kCollectBlocks) k_collect(const __grid_constant__ TraceParams p) {
   cache_header<TraversalCfg<CFG>::K>(p);
   Counters cnt;
-  MarchShader<MODE> sh(p);
+  MarchShader sh(p);
   run<CFG>(p, sh, cnt);
   // the traversal work (node visits, triangle tests) only: rays, hits and the
   // queries the march used are counted by the shading pass
@@ -2511,10 +2501,10 @@ template <int CFG>
 const void* bwd_fn() { return (const void*)k_backward<CFG, kShadeRef>; }
 const void* collect_fn(int cfg) {
   switch (cfg) {
-    case kCfgPackets16: return (const void*)k_collect<kCfgPackets16, kShadeRef>;
-    case kCfgPackets32: return (const void*)k_collect<kCfgPackets32, kShadeRef>;
-    case kCfgLanes24: return (const void*)k_collect<kCfgLanes24, kShadeRef>;
-    default: return (const void*)k_collect<kCfgLanes32, kShadeRef>;
+    case kCfgPackets16: return (const void*)k_collect<kCfgPackets16>;
+    case kCfgPackets32: return (const void*)k_collect<kCfgPackets32>;
+    case kCfgLanes24: return (const void*)k_collect<kCfgLanes24>;
+    default: return (const void*)k_collect<kCfgLanes32>;
   }
 }
 const void* kernel_for(int which, int cfg) {
@@ -2574,23 +2564,14 @@ cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int MODE>
-cudaError_t launch_collect_t(const TraceParams& p, int grid, cudaStream_t s) {
+cudaError_t launch_collect(const TraceParams& p, int grid, cudaStream_t s) {
   switch (p.cfg) {
-    case kCfgPackets16: k_collect<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
-    case kCfgPackets32: k_collect<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
-    case kCfgLanes24: k_collect<kCfgLanes24, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
-    default: k_collect<kCfgLanes32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
+    case kCfgPackets16: k_collect<kCfgPackets16><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
+    case kCfgPackets32: k_collect<kCfgPackets32><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;
+    case kCfgLanes24: k_collect<kCfgLanes24><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes24>(), s>>>(p); break;
+    default: k_collect<kCfgLanes32><<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p); break;
   }
   return cudaGetLastError();
-}
-
-cudaError_t launch_collect(const TraceParams& p, int grid, cudaStream_t s) {
-  switch (p.mode) {
-    case kShadeExact: return launch_collect_t<kShadeExact>(p, grid, s);
-    case kShadeRefArith: return launch_collect_t<kShadeRefArith>(p, grid, s);
-    default: return launch_collect_t<kShadeRef>(p, grid, s);
-  }
 }
 
 cudaError_t launch_forward(const TraceParams& p, int grid, cudaStream_t s) {

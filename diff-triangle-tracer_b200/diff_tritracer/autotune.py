@@ -21,13 +21,13 @@ import torch
 
 # Warp packets are also tried with the split forward (a traversal-only pass
 # that stores each ray's queries, then a shading pass that replays them),
-# storing the first query of each ray or all of them: which one wins depends
-# on how many rays end on the transmittance cut-off, whose later queries the
-# traversal-only pass cannot know to skip.
+# storing each ray's first query, its first two or all of them: which one
+# wins depends on how many rays end on the transmittance cut-off, whose later
+# queries the traversal-only pass cannot know to skip.
 CANDIDATES = tuple(
     dict(c, split=split, collect=collect)
     for c in ({"traversal": "packets", "k": 16, "stack_depth": 0}, {"traversal": "packets", "k": 32, "stack_depth": 0})
-    for split, collect in ((False, 1), (True, 1), (True, 0))
+    for split, collect in ((False, 1), (True, 1), (True, 2), (True, 0))
 ) + (
     {"traversal": "lanes", "k": 16, "stack_depth": 32, "split": False, "collect": 1},
     {"traversal": "lanes", "k": 16, "stack_depth": 24, "split": False, "collect": 1},

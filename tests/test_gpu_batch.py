@@ -116,7 +116,7 @@ def test_autotune_chooses_and_caches(tmp_path):
     assert best["traversal"] in ("packets", "lanes") and cache.exists()
     from diff_tritracer.autotune import CANDIDATES
 
-    assert len(best["all"]) == len(CANDIDATES) == 8  # 2 packet sizes x 3 forward schedules + 2 lane stacks
+    assert len(best["all"]) == len(CANDIDATES) == 10  # 2 packet sizes x 4 forward schedules + 2 lane stacks
     again = autotune(tr, vb.step, key="dense3000", cache_path=str(cache))
     assert all(again[k] == best[k] for k in ("traversal", "k", "stack_depth", "split", "collect"))
     vb.step()
