@@ -942,13 +942,6 @@ __device__ __forceinline__ float cache_get(const TraceParams& p, bool first, lon
   return __uint_as_float((uint32_t)w);
 }
 
-// Fill mode: the pool is already exhausted (by the collecting pass). The
-// shading pass then asks for no entry, so a later query the collecting pass
-// was refused is not counted twice in pool_used.
-__device__ __forceinline__ bool cache_pool_full(const TraceParams& p) {
-  return __ldcg(&cache_header_ptr(p)->pool_used) >= p.cache_pool_cap;
-}
-
 // Fill mode: the word where the entry of the query after the one replayed
 // from the main part (first) or from pool entry e gets linked.
 template <int K>
@@ -1044,8 +1037,6 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
         if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (first) {
             link = cache_put_first<K>(p, g, sm, t_drop);
-          } else if (link && p.cache_mode == kCacheFill && cache_pool_full(p)) {
-            link = nullptr;
           } else if (link) {
             const uint32_t e = atomicAdd(&cache_header_ptr(p)->pool_used, 1u);
             link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
@@ -1133,7 +1124,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
         if (first) {
           if (trav) link = cache_put_first<K>(p, g, sm, t_drop);
         } else {
-          const bool more = trav && link != nullptr && !(p.cache_mode == kCacheFill && cache_pool_full(p));
+          const bool more = trav && link != nullptr;
           const uint32_t e = cache_alloc(p, more);
           if (more) link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
         }

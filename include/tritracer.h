@@ -253,9 +253,11 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  *   split forward stores at most n k-closest queries per ray (0: every query
  *   of the march, also those past the point where the ray's transmittance
  *   would end it, which that pass cannot know); the shading pass traverses
- *   for the queries not stored. With a cap, pool_used of tt_hit_cache_usage
- *   counts the later queries of the shading pass's march; with 0 it counts
- *   those the traversal-only pass stored or was refused. */
+ *   for the queries not stored. pool_used of tt_hit_cache_usage counts the
+ *   pool entries both passes asked for: with a cap of 1 the later queries of
+ *   the shading pass's march; otherwise also those the traversal-only pass
+ *   made past a ray's cut-off, and a query it was refused counts again when
+ *   the shading pass asks for it. */
 /* Device time of the two passes of the last forward on the handle that ran
  * with `debug` (events, as gpu_time_ms): the traversal-only pass (0 for a
  * fused forward) and the shading pass. No reference counterpart. */

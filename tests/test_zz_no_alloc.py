@@ -191,7 +191,10 @@ def test_calls_in_a_row_on_different_scenes_allocate_nothing():
         before = device_memory_state()
         assert call.run() == 0
         after = device_memory_state()
-        assert after == before, (i, before, after)
+        # no allocation: the device's free memory did not shrink (the driver
+        # may release memory of its own meanwhile) and the torch allocator
+        # made no allocation and reserved no segment
+        assert after[0] >= before[0] and after[1:] == before[1:], (i, before, after)
         assert lib.tt_noalloc_status(stream()) == 0
         assert_same(call.result(), want, f"call {i}")
     # the smaller scene really differs from the others
