@@ -349,7 +349,7 @@ def proposal_leg(dev, steps=3, seed=0, small=False, epochs=120):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / n
 
-    schedules = (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0))
+    schedules = (("fused", False, 1), ("split_first", True, 1), ("split_two", True, 2), ("split_all", True, 0))
 
     def set_schedule(name):
         _, split, collect = next(x for x in schedules if x[0] == name)
@@ -401,7 +401,7 @@ def proposal_leg(dev, steps=3, seed=0, small=False, epochs=120):
     val_col = torch.stack([c for c, _ in val_out]).clone()
     val_g = [x.clone() for x in val_g]
     choices = {}
-    for mf in (0.05, 0.1, 0.2, 0.3):
+    for mf in (0.1, 0.2, 0.3, 0.5, 0.75):
         ivs = prop.intervals(val, margin_near=proposal.NO_NEAR_CLIP, margin_far=mf)
         for name, ms in by_schedule(lambda: fwd_bwd(val, val_ups, ivs), n=2).items():
             choices[(mf, name, "off")] = ms
@@ -906,7 +906,8 @@ def main():
     schedules = {}
     if use_cache:
         cur = (tuned or {}).get("split", args.split_forward), (tuned or {}).get("collect", args.collect_queries or 1)
-        for sname, split, collect in (("fused", False, 1), ("split_first", True, 1), ("split_all", True, 0)):
+        for sname, split, collect in (("fused", False, 1), ("split_first", True, 1), ("split_two", True, 2),
+                                      ("split_all", True, 0)):
             tr.set_split_forward(split)
             tr.set_collect_queries(collect)
             step()  # first launches of this schedule's kernels, untimed
