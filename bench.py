@@ -594,15 +594,18 @@ def secondary_leg(dev, steps=3, seed=0):
     tr.set_sort_secondary(False)
     ms_unsorted, _ = timed()
     tr.set_sort_secondary(True)
+    tr.set_split_forward(False)
+    ms_fused, _ = timed()
+    tr.set_split_forward(True)
     ms, st = timed()
     tr.device_status()
     R = 1600 * 800
     return {"workload": "500k triangles, 20% dielectric, env 512x1024, 2 views 800x800, 2 bounces",
             "pixels_per_step": R, "rays_per_step": st["rays"] / steps, "ms_per_step": ms,
             "primary_mrays": R / ms / 1e3, "all_rays_mrays": st["rays"] / steps / ms / 1e3,
-            "ms_per_step_spawn_order": ms_unsorted,
-            "step": "forward (3 trace levels, spawned levels sorted by direction octant and origin, + 3 resolves) "
-                    "+ adjoint (all levels, one launch)"}
+            "ms_per_step_spawn_order": ms_unsorted, "ms_per_step_without_split": ms_fused,
+            "step": "forward (3 trace levels, spawned levels sorted by direction octant and origin and traced "
+                    "as a traversal-only pass plus a shading pass, + 3 resolves) + adjoint (all levels, one launch)"}
 
 
 def views_leg(dev, name, steps, warmup=3, no_autotune=False, world=1, local=0, sample_clocks=False):

@@ -1897,13 +1897,14 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
       uint32_t* rec_link = &p.sec.rec[sh.ridx].cache_link;
       if (replay && first && !main_part) next = __ldcg(rec_link);
       if (replay && (main_part || cache_has<K>(p, next, cur.key_min))) {
+        if (p.cache_mode == kCacheFill) link = cache_link_of<K>(p, main_part, sh.ridx, next);
         t_drop = cache_get<K>(p, main_part, sh.ridx, next, sm, next);
         ++cnt.replays;
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
         query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
-        if (p.cache_mode == kCacheWrite) {
+        if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (main_part) {
             link = cache_put_first<K>(p, sh.ridx, sm, t_drop);
           } else {
@@ -2172,12 +2173,66 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_sec_primary(const
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
-// Levels >= 1: spawned rays, incoherent: one ray per lane.
-__global__ void __launch_bounds__(kTraceThreads, 4) k_sec_trace(const __grid_constant__ TraceParams p) {
+// Levels >= 1: spawned rays, incoherent: one ray per lane, with a
+// kSecStack-entry stack in shared memory per lane (continued in local
+// memory) and kSecBlocks blocks per SM.
+#ifndef TT_SEC_STACK
+#define TT_SEC_STACK 32
+#endif
+#ifndef TT_SEC_BLOCKS
+#define TT_SEC_BLOCKS 4
+#endif
+constexpr int kSecStack = TT_SEC_STACK, kSecBlocks = TT_SEC_BLOCKS;
+constexpr size_t sec_trace_smem() { return (size_t)kTraceThreads * (kSecStack * 8 + kChunk * 8); }
+
+__global__ void __launch_bounds__(kTraceThreads, kSecBlocks) k_sec_trace(const __grid_constant__ TraceParams p) {
   Counters cnt;
   SecShader sh(p);
-  drive_items<32>(p, thread_smem<32>(), sh, cnt, sec_level_size(p, p.sec.level));
+  drive_items<kSecStack>(p, thread_smem<kSecStack>(), sh, cnt, sec_level_size(p, p.sec.level));
+  cnt.queries += cnt.replays;  // replayed from the traversal pass (split schedule): used by the march all the same
+  cnt.replays = 0;
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
+}
+
+// Traversal pass of a spawned level (split schedule): the level's rays, in
+// the same order, with a shader that shades and spawns nothing, storing every
+// query in the ray tree's hit cache (the chain starts at the ray's record);
+// k_sec_trace then replays them in fill mode. Like k_collect for primary
+// rays: without the shading and spawning code the pass needs fewer
+// registers, and with a shorter shared-memory stack per lane (continued in
+// local memory) more blocks fit an SM.
+#ifndef TT_SEC_COLLECT_STACK
+#define TT_SEC_COLLECT_STACK 16
+#endif
+#ifndef TT_SEC_COLLECT_BLOCKS
+#define TT_SEC_COLLECT_BLOCKS 6
+#endif
+constexpr int kSecCollectStack = TT_SEC_COLLECT_STACK, kSecCollectBlocks = TT_SEC_COLLECT_BLOCKS;
+constexpr size_t sec_collect_smem() { return (size_t)kTraceThreads * (kSecCollectStack * 8 + kChunk * 8); }
+
+struct SecMarchShader {
+  static constexpr bool kStopsAtClip = true;
+  const TraceParams& p;
+  int ridx = 0;
+  __device__ explicit SecMarchShader(const TraceParams& params) : p(params) {}
+  __device__ __forceinline__ void begin_item(int i, float3& ro, float3& rd) {
+    const SecParams& s = p.sec;
+    ridx = s.base[s.level] + (s.order ? (int)__ldg(s.order + i) : i);
+    const SecRecord* r = s.rec + ridx;
+    ro = make_float3(r->o[0], r->o[1], r->o[2]);
+    rd = make_float3(r->d[0], r->d[1], r->d[2]);
+  }
+  __device__ __forceinline__ void prepare() {}
+  __device__ __forceinline__ bool visit(uint32_t, float) { return false; }
+  __device__ __forceinline__ void end() {}
+};
+
+__global__ void __launch_bounds__(kTraceThreads, kSecCollectBlocks) k_sec_collect(const __grid_constant__ TraceParams p) {
+  Counters cnt;
+  SecMarchShader sh(p);
+  drive_items<kSecCollectStack>(p, thread_smem<kSecCollectStack>(), sh, cnt, sec_level_size(p, p.sec.level));
+  cnt.queries = 0;  // counted by the shading pass (k_sec_trace), like k_collect
+  add_stats(p.stats, 0u, 0u, 0u, cnt);
 }
 
 // Sort keys of the spawned rays of level p.sec.level: the octant of the
@@ -2588,14 +2643,22 @@ cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s) {
 int sec_blocks_per_sm(int which) {
   int n = 0;
   const void* fn = which == 0 ? (const void*)k_sec_trace
-                              : (which == 1 ? (const void*)k_sec_backward : (const void*)k_sec_primary);
-  const size_t smem = which == 2 ? smem_bytes_for<kCfgPackets16>() : smem_bytes_for<kCfgLanes32>();
+                              : (which == 1 ? (const void*)k_sec_backward
+                                            : (which == 2 ? (const void*)k_sec_primary : (const void*)k_sec_collect));
+  const size_t smem = which == 2 ? smem_bytes_for<kCfgPackets16>()
+                                 : (which == 0 ? sec_trace_smem()
+                                               : (which == 3 ? sec_collect_smem() : smem_bytes_for<kCfgLanes32>()));
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTraceThreads, smem) != cudaSuccess) n = 1;
   return n > 0 ? n : 1;
 }
 
 cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s) {
-  k_sec_trace<<<grid, kTraceThreads, smem_bytes_for<kCfgLanes32>(), s>>>(p);
+  k_sec_trace<<<grid, kTraceThreads, sec_trace_smem(), s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sec_collect(const TraceParams& p, int grid, cudaStream_t s) {
+  k_sec_collect<<<grid, kTraceThreads, sec_collect_smem(), s>>>(p);
   return cudaGetLastError();
 }
 

@@ -185,9 +185,11 @@ cudaError_t launch_backward(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_hit_stream(const HitStreamParams& p, cudaStream_t s);
 // Secondary-ray passes (views[0] only): trace level p.sec.level, resolve it,
 // or run the adjoint of every ray of every level.
-int sec_blocks_per_sm(int which /*0 trace (levels >= 1), 1 adjoint, 2 primary level*/);
+int sec_blocks_per_sm(int which /*0 trace (levels >= 1), 1 adjoint, 2 primary level, 3 collecting pass*/);
 cudaError_t launch_sec_trace(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_primary(const TraceParams& p, int grid, cudaStream_t s);
+// Traversal-only pass over a spawned level (fills the ray tree's hit cache).
+cudaError_t launch_sec_collect(const TraceParams& p, int grid, cudaStream_t s);
 cudaError_t launch_sec_resolve(const TraceParams& p, cudaStream_t s);
 // Sort keys of the records of level p.sec.level (cap of them; the unused
 // slots get 0xFFFFFFFF and sort last) and their indices, for sort_pairs.
