@@ -32,7 +32,7 @@ struct tt_tracer {
   tt::DevBuf sec_cache;        // hit cache of that ray tree (tt_forward_secondary writes, the adjoint replays)
   size_t sec_cache_bytes = 0;  // its size for the last tree
   int sec_R = 0, sec_depth = -1;  // the ray tree the last tt_forward_secondary left
-  int sec_trace_grid = 0, sec_bwd_grid = 0, sec_primary_grid = 0, sec_collect_grid = 0;
+  int sec_trace_grid = 0, sec_bwd_grid = 0, sec_primary_grid = 0, sec_collect_grid = 0, sec_collect0_grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_mid = nullptr;
   float pass_ms[2] = {0.f, 0.f};  // last debug forward: collecting pass, shading pass (ms)
   unsigned long long trace_launches = 0;  // trace kernels enqueued
@@ -152,6 +152,7 @@ int tt_create(const tt_config* cfg, tt_tracer** out) {
   h->sec_primary_grid = h->num_sms * tt::sec_blocks_per_sm(2);
   h->sec_bwd_grid = h->num_sms * tt::sec_blocks_per_sm(1);
   h->sec_collect_grid = h->num_sms * tt::sec_blocks_per_sm(3);
+  h->sec_collect0_grid = h->num_sms * tt::trace_blocks_per_sm(3, tt::kCfgPackets16);
   if (tt_set_traversal(h, h->cfg.traversal, h->cfg.k, h->cfg.stack_depth) != TT_OK) {
     delete h;
     return TT_ERR_INVALID;
@@ -845,10 +846,19 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
       h->trace_launches += 1 + 3 * 4;
     }
     p.cache_mode = tt::kCacheWrite;
-    if (level > 0 && h->split_forward) {
-      // traversal-only pass over the level, then the shading pass replays it
+    if (h->split_forward) {
+      // traversal-only pass over the level (the primary rays as warp
+      // packets of 16-hit queries, like k_sec_primary; spawned rays lane by
+      // lane), then the shading pass replays it
       TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
-      TT_CUDA(h, tt::launch_sec_collect(p, h->sec_collect_grid, s));
+      if (level == 0) {
+        tt::TraceParams q = p;
+        q.cfg = tt::kCfgPackets16;
+        q.collect_queries = h->collect_queries;
+        TT_CUDA(h, tt::launch_collect(q, h->sec_collect0_grid, s));
+      } else {
+        TT_CUDA(h, tt::launch_sec_collect(p, h->sec_collect_grid, s));
+      }
       ++h->trace_launches;
       p.cache_mode = tt::kCacheFill;
     }
