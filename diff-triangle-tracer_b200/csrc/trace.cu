@@ -2170,6 +2170,8 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_sec_primary(const
   unsigned char* rest;
   const Smem sm = packet_smem<kChunk>(rest);
   drive_packets<kChunk>(p, sm, warp_stack(rest), sh, cnt);
+  cnt.queries += cnt.replays;  // replayed from the traversal pass (split schedule): used by the march all the same
+  cnt.replays = 0;
   add_stats(p.stats, sh.n_rays, sh.n_eval, sh.n_blend, cnt);
 }
 
