@@ -76,6 +76,20 @@ struct Counters {
   unsigned nodes = 0, tris = 0, queries = 0, warp_nodes = 0;
   unsigned cont = 0, restart = 0;  // proposed intervals left by continuation / re-trace
   unsigned replays = 0;            // queries taken from the hit cache (adjoint)
+  __device__ __forceinline__ void add_cont() { ++cont; }
+  __device__ __forceinline__ void add_restart() { ++restart; }
+};
+
+// The packet drivers keep their counters in per-warp shared-memory words
+// instead (warp-uniform updates by lane 0, shared atomics for the rare
+// per-lane events), so the traversal carries no counter registers; they are
+// folded into the thread's Counters when the warp is done.
+constexpr int kWNodes = 0, kWTris = 1, kWWarpNodes = 2, kWQueries = 3, kWReplays = 4, kWCont = 5, kWRestart = 6,
+              kWCounters = 8;
+struct WarpCounters {
+  unsigned* w;
+  __device__ __forceinline__ void add_cont() { atomicAdd(w + kWCont, 1u); }
+  __device__ __forceinline__ void add_restart() { atomicAdd(w + kWRestart, 1u); }
 };
 
 // Three-input FP32 min / max (one instruction on sm_100); min and max are
@@ -250,12 +264,13 @@ struct WarpStack {
   uint32_t* ref;
   unsigned* mask;
   float* tmin;
+  unsigned* cnt;  // kWCounters words: the warp's traversal counters
 };
 
 template <int K>
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
                                              unsigned long long key_min, float t_hi, unsigned long long* kb, int kstride,
-                                             WarpStack ws, float& t_drop, int* status, Counters& cnt) {
+                                             WarpStack ws, float& t_drop, int* status) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -264,7 +279,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
   t_drop = INFINITY;
   const unsigned act = __ballot_sync(full, want);
   if (act == 0 || !bvh.has_root) return;
-  if (want) ++cnt.queries;
+  if (lane == 0) ws.cnt[kWQueries] += __popc(act);
   const float t_lo = want ? key_t(key_min) : 0.f;
   float tmax = want ? t_hi : -1.0f;  // a lane without a query never passes a test
   const int nx = r.ix >= 0.f ? 0 : 2, ny = r.iy >= 0.f ? 4 : 6, nz = r.iz >= 0.f ? 8 : 10;
@@ -294,8 +309,10 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     if (m == 0) continue;
     if (!TT_IN_BOUNDS(status, ref < (uint32_t)bvh.wide_cap)) continue;  // ref is the same in every lane
     const bool on = (m >> lane) & 1u;
-    if (on) ++cnt.nodes;
-    if (lane == 0) ++cnt.warp_nodes;
+    if (lane == 0) {
+      ws.cnt[kWNodes] += __popc(m);
+      ws.cnt[kWWarpNodes] += 1u;
+    }
     const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
     // lane c (c < 8) will push child c: fetch its reference with the boxes
     const uint32_t my_ref = lane < 8 ? __ldg(reinterpret_cast<const uint32_t*>(nd + 12) + lane) : kEmptyRef;
@@ -321,10 +338,11 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     for (unsigned lb = __ballot_sync(full, my_leaf); lb != 0u; lb &= lb - 1u) {
       const int lc = __ffs(lb) - 1;
       const uint32_t lref = __shfl_sync(full, my_ref, lc);
-      const bool lon = (__shfl_sync(full, mymask, lc) >> lane) & 1u;
+      const unsigned lm = __shfl_sync(full, mymask, lc);  // lanes entering the leaf
+      const bool lon = (lm >> lane) & 1u;
       const uint32_t first = leaf_first(lref), ntri = leaf_count(lref);
       if (!TT_IN_BOUNDS(status, first + ntri <= (uint32_t)bvh.P)) continue;  // the same in every lane
-      if (lon) cnt.tris += ntri;
+      if (lane == 0) ws.cnt[kWTris] += __popc(lm) * ntri;
       with_perm(wperm, r, [&](const auto& pm) {
         for (uint32_t j = 0; j < ntri; ++j) {
           const float4* tr = bvh.tris + 3 * (size_t)(first + j);
@@ -785,9 +803,9 @@ __device__ __forceinline__ void clip_cursor(Cursor& c, const float* interval, in
 // in cnt.cont), or, if the interval held no hit at all, from the start of the
 // ray (a plain re-trace, cnt.restart). Either way every hit at or beyond
 // t_near is visited in the plain order.
-template <int K, class Shader>
+template <int K, class Shader, class Cnt>
 __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Cursor& cur, int tmin_inclusive,
-                                              int* status, Shader& sh, Counters& cnt) {
+                                              int* status, Shader& sh, Cnt& cnt) {
   const bool truncated = t_drop < INFINITY;
   auto trusted = [&](unsigned long long key) {
     return key != kEmptyKey && !(truncated && key_t(key) >= t_drop);
@@ -802,10 +820,10 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
     cur.t_hi = kFar;
     if (!any && cur.chunks == 0) {
       cur.key_min = first_key(tmin_inclusive);
-      ++cnt.restart;
+      cnt.add_restart();
     } else {
       cur.key_min = next;
-      ++cnt.cont;
+      cnt.add_cont();
     }
     return false;
   };
@@ -1074,6 +1092,7 @@ __device__ __forceinline__ WarpStack warp_stack(unsigned char* base) {
   ws.ref = reinterpret_cast<uint32_t*>(base) + w * kWarpStack;
   ws.mask = reinterpret_cast<unsigned*>(base + (size_t)(blockDim.x / 32) * kWarpStack * 4) + w * kWarpStack;
   ws.tmin = reinterpret_cast<float*>(base + (size_t)(blockDim.x / 32) * kWarpStack * 8) + w * kWarpStack;
+  ws.cnt = reinterpret_cast<unsigned*>(base + (size_t)(blockDim.x / 32) * kWarpStack * 12) + w * kWCounters;
   return ws;
 }
 
@@ -1083,6 +1102,9 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const bool replay = cache_replays<K>(p);
+  if (lane < kWCounters) ws.cnt[lane] = 0u;
+  __syncwarp();
+  WarpCounters wc{ws.cnt};
   for (;;) {
     int tile = 0;
     if (lane == 0) tile = atomicAdd(p.work, 1);
@@ -1112,11 +1134,12 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       const bool rep = replay && active && (first || cache_has<K>(p, next, cur.key_min));
       const bool trav = active && !rep;
       if (__any_sync(full, trav))
-        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status, cnt);
+        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status);
+      const unsigned nrep = __popc(__ballot_sync(full, rep));
+      if (lane == 0) ws.cnt[kWReplays] += nrep;
       if (rep) {
         if (p.cache_mode == kCacheFill) link = cache_link_of<K>(p, first, g, next);
         t_drop = cache_get<K>(p, first, g, next, sm, next);
-        ++cnt.replays;
       } else {
         next = kNoEntry;
       }
@@ -1130,7 +1153,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
         }
       }
       if (active) {
-        bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, cnt);
+        bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, wc);
         if (!done && ++cur.chunks >= kMaxChunks) {
           atomicOr(p.status, kStatusTimeout);
           done = true;
@@ -1143,6 +1166,17 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
         }
       }
     }
+  }
+  // the warp's counters into lane 0's Counters (summed over the warp later)
+  __syncwarp();
+  if (lane == 0) {
+    cnt.nodes += ws.cnt[kWNodes];
+    cnt.tris += ws.cnt[kWTris];
+    cnt.warp_nodes += ws.cnt[kWWarpNodes];
+    cnt.queries += ws.cnt[kWQueries];
+    cnt.replays += ws.cnt[kWReplays];
+    cnt.cont += ws.cnt[kWCont];
+    cnt.restart += ws.cnt[kWRestart];
   }
 }
 
@@ -1188,7 +1222,7 @@ struct TraversalCfg<kCfgLanes24> {
 template <int CFG>
 constexpr size_t smem_bytes_for() {
   using C = TraversalCfg<CFG>;
-  return C::packets ? (size_t)kTraceThreads * C::K * 8 + (size_t)(kTraceThreads / 32) * kWarpStack * 12
+  return C::packets ? (size_t)kTraceThreads * C::K * 8 + (size_t)(kTraceThreads / 32) * (kWarpStack * 12 + kWCounters * 4)
                     : (size_t)kTraceThreads * (C::SD * 8 + kChunk * 8);
 }
 

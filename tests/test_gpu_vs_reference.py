@@ -23,8 +23,9 @@ rays as the GPU:
     digits, so the reference itself is that far from the FP64 answer.
 `scaling` is written by the first ray that blends a triangle (a race in the
 reference too); it is compared for the one-camera cases, where every such
-ray starts at the same origin. Rays whose FP32 threshold decisions (alpha vs 1/255, T(1 - alpha) vs 1e-4)
-lie within 1e-5 (relative) of flipping are left out of the per-pixel checks,
+ray starts at the same origin. Rays whose FP32 threshold decisions (alpha
+vs 1/255, T(1 - alpha) vs 1e-4) lie within 1e-5 (relative) of flipping are
+left out of the per-pixel checks,
 and their upstream gradients are zero.
 
 Cases: the dense 3k-triangle scene, the random 20k-triangle scene, and a
@@ -102,9 +103,7 @@ def test_queries_equal_the_references(reference, c2, which, incl):
 
 
 def decisions_ok(oracle, sc, ro, rd, incl=True):
-    """`scaling` is written by the first ray that blends a triangle (a race in the
-reference too); it is compared for the one-camera cases, where every such
-ray starts at the same origin. Rays whose FP32 threshold decisions are clear of flipping (the FP32
+    """Rays whose FP32 threshold decisions are clear of flipping (the FP32
     oracle is bit-identical to the reference's code)."""
     H, W = ro.shape[:2]
     r = oracle.forward(sc, ro, rd, bg=BG, precision=32, tmin_inclusive=incl, record=256, nthreads=8)
