@@ -1405,12 +1405,15 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __g
 // no shading state or code the pass needs far fewer registers than the fused
 // kernel, so more warps per SM hide the latency of the node and triangle
 // loads, which is what bounds the traversal.
-// 5 blocks of 128 threads (96 registers, no spills): 20 warps per SM
-// against the fused kernel's 16. At 6 blocks (80 registers) ~170 bytes a
-// thread spill and the pass is slower (1M triangles, 4 x 800^2 rays:
-// split forward 18.3 ms at 6 blocks, 16.0 at 5; fused 18.3).
+// 6 blocks of 128 threads (80 registers, ~60 bytes of spills a thread since
+// the packet drivers keep their counters in shared memory): 24 warps per SM
+// against the fused kernel's 16. Measured on 1M triangles, 4 x 800^2 rays,
+// split forward storing two queries a ray: 15.4 ms at 6 blocks, 16.5 at 5
+// (95 registers, no spills), fused 19.0 (one run, same box). With the
+// counters in registers the 6-block build spilled ~170 bytes and was no
+// faster than 5 blocks.
 #ifndef TT_COLLECT_BLOCKS
-#define TT_COLLECT_BLOCKS 5
+#define TT_COLLECT_BLOCKS 6
 #endif
 constexpr int kCollectBlocks = TT_COLLECT_BLOCKS;
 
