@@ -81,7 +81,7 @@ struct RayW {
   float dx, dy, dz;
   float ix, iy, iz;      // 1/d (components clamped away from 0)
   float oix, oiy, oiz;   // o * (1/d)
-  int kx, ky, kz;        // watertight permutation
+  int perm;              // watertight permutation: kx | ky << 2 | kz << 4
   float Sx, Sy, Sz;      // watertight shear
 };
 
@@ -105,7 +105,7 @@ __device__ __forceinline__ RayW make_ray(float3 o, float3 d) {
     kx = ky;
     ky = tmp;
   }
-  r.kx = kx; r.ky = ky; r.kz = kz;
+  r.perm = kx | (ky << 2) | (kz << 4);
   r.Sx = __fdiv_rn(sel3(d.x, d.y, d.z, kx), dkz);
   r.Sy = __fdiv_rn(sel3(d.x, d.y, d.z, ky), dkz);
   r.Sz = __fdiv_rn(1.0f, dkz);
@@ -122,6 +122,7 @@ __device__ __forceinline__ RayW make_ray(float3 o, float3 d) {
 // at run time ...
 struct PermRt {
   int kx, ky, kz;
+  __device__ __forceinline__ explicit PermRt(int pack) : kx(pack & 3), ky((pack >> 2) & 3), kz((pack >> 4) & 3) {}
   __device__ __forceinline__ float x(float a, float b, float c) const { return sel3(a, b, c, kx); }
   __device__ __forceinline__ float y(float a, float b, float c) const { return sel3(a, b, c, ky); }
   __device__ __forceinline__ float z(float a, float b, float c) const { return sel3(a, b, c, kz); }
@@ -181,13 +182,13 @@ __device__ __forceinline__ bool isect_tri_p(const RayW& r, const Perm& pm, float
 }
 
 __device__ __forceinline__ bool isect_tri(const RayW& r, float4 a, float4 b, float4 c, float& t) {
-  return isect_tri_p(r, PermRt{r.kx, r.ky, r.kz}, a, b, c, t);
+  return isect_tri_p(r, PermRt(r.perm), a, b, c, t);
 }
 
 // Packed permutation: kx | ky << 2 | kz << 4. The six values the watertight
 // set-up produces (kz = dominant axis; kx, ky the other two, swapped when the
 // direction along kz is negative).
-__device__ __forceinline__ int perm_pack(const RayW& r) { return r.kx | (r.ky << 2) | (r.kz << 4); }
+__device__ __forceinline__ int perm_pack(const RayW& r) { return r.perm; }
 constexpr int kPerm12_0 = 1 | (2 << 2) | (0 << 4), kPerm21_0 = 2 | (1 << 2) | (0 << 4);
 constexpr int kPerm20_1 = 2 | (0 << 2) | (1 << 4), kPerm02_1 = 0 | (2 << 2) | (1 << 4);
 constexpr int kPerm01_2 = 0 | (1 << 2) | (2 << 4), kPerm10_2 = 1 | (0 << 2) | (2 << 4);
@@ -203,7 +204,7 @@ __device__ __forceinline__ void with_perm(int pack, const RayW& r, Fn&& fn) {
     case kPerm02_1: fn(PermCt<0, 2, 1>{}); break;
     case kPerm01_2: fn(PermCt<0, 1, 2>{}); break;
     case kPerm10_2: fn(PermCt<1, 0, 2>{}); break;
-    default: fn(PermRt{r.kx, r.ky, r.kz}); break;
+    default: fn(PermRt(r.perm)); break;
   }
 }
 
