@@ -157,9 +157,29 @@ def test_learned_intervals_on_tracer_records():
                                          2, intervals=intervals)
         return torch.stack([c for c, _ in outs]).cpu().numpy()
 
+    def work(st):  # traversal work per ray: node visits and triangle tests
+        return (st["node_visits"] + st["triangle_tests"]) / st["rays"]
+
     tr.reset_stats()
     plain = render(None)
     st_plain = tr.stats()
+    # what the clip can save at best: the plain tracer's own first / last hits
+    recs = [torch.empty((3, 96, 96), device=DEV) for _ in held]
+    tr.trace_forward_views(held, s["verts"], s["sigma"], s["npts"], s["cums"], sc.P, s["shs"], 3, s["opac"],
+                           torch.zeros(sc.P, device=DEV), torch.zeros(sc.P, device=DEV), bg, 2, records=recs)
+    perfect = [torch.stack([torch.zeros_like(r[0]), torch.where(r[2] > 0.5, r[1], torch.full_like(r[1], float("inf")))])
+               for r in recs]
+    tr.reset_stats()
+    np.testing.assert_array_equal(render(perfect), plain)
+    w_perfect = work(tr.stats())
+    tr.reset_stats()
+    render(p.intervals(held, margin_far=0.2))
+    w_learned = work(tr.stats())
+    print(f"traversal work per ray: plain {work(st_plain):.1f}, learned far clip {w_learned:.1f}, "
+          f"perfect far clip {w_perfect:.1f}")
+    # the trained network's far clip cuts the traversal work, and stays within
+    # reach of the perfect clip
+    assert w_perfect < w_learned < 0.97 * work(st_plain)
     for mf in (0.05, 0.2):
         tr.reset_stats()
         clipped = render(p.intervals(held, margin_far=mf))
