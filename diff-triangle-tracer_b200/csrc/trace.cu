@@ -55,12 +55,14 @@ struct Stack {
 };
 
 // Sorted insert into the lane's k-buffer in shared memory (hits are rare
-// next to box tests, so the buffer need not occupy 32 registers); kb_last
-// mirrors the largest key.
+// next to box tests, so the buffer need not occupy 32 registers). `n` counts
+// the valid keys (the slots from n on hold kEmptyKey): the insert shifts only
+// the valid keys above the new one, not the empty tail, and once the buffer
+// is full the largest key drops out. Returns true when the buffer is full
+// after the insert (its last key then bounds the query).
 template <int K>
-__device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key,
-                                               unsigned long long& kb_last) {
-  int i = K - 1;
+__device__ __forceinline__ bool kb_insert_smem(unsigned long long* kb, int stride, unsigned long long key, int& n) {
+  int i = n < K ? n : K - 1;
   while (i > 0) {
     const unsigned long long prev = kb[(i - 1) * stride];
     if (prev <= key) break;
@@ -68,7 +70,15 @@ __device__ __forceinline__ void kb_insert_smem(unsigned long long* kb, int strid
     --i;
   }
   kb[i * stride] = key;
-  kb_last = kb[(K - 1) * stride];
+  if (n < K) ++n;
+  return n == K;
+}
+
+// A candidate key enters a k-buffer holding n valid keys iff the buffer has
+// room or the key is below its largest key.
+template <int K>
+__device__ __forceinline__ bool kb_accepts(const unsigned long long* kb, int stride, unsigned long long key, int n) {
+  return n < K || key < kb[(K - 1) * stride];
 }
 
 
@@ -156,7 +166,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
   ++cnt.queries;
 #pragma unroll
   for (int i = 0; i < kChunk; ++i) kb[i * kstride] = kEmptyKey;
-  unsigned long long kb_last = kEmptyKey;
+  int kb_n = 0;
   t_drop = INFINITY;
   if (!bvh.has_root) return;
   const float t_lo = key_t(key_min);
@@ -196,9 +206,8 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
         if (!isect_tri(r, a, b, c, t)) continue;
         if (!(t >= t_lo) || !(t <= tmax)) continue;
         const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-        if (key >= key_min && key < kb_last) {
-          kb_insert_smem<kChunk>(kb, kstride, key, kb_last);
-          if (kb_last != kEmptyKey) tmax = key_t(kb_last);
+        if (key >= key_min && kb_accepts<kChunk>(kb, kstride, key, kb_n)) {
+          if (kb_insert_smem<kChunk>(kb, kstride, key, kb_n)) tmax = key_t(kb[(kChunk - 1) * kstride]);
         }
       }
       continue;
@@ -275,7 +284,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int i = 0; i < K; ++i) kb[i * kstride] = kEmptyKey;
-  unsigned long long kb_last = kEmptyKey;
+  int kb_n = 0;
   t_drop = INFINITY;
   const unsigned act = __ballot_sync(full, want);
   if (act == 0 || !bvh.has_root) return;
@@ -351,9 +360,8 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
           if (!lon || !isect_tri_p(r, pm, a, b, c, t)) continue;
           if (!(t >= t_lo) || !(t <= tmax)) continue;
           const unsigned long long key = hit_key(t, (uint32_t)__float_as_int(a.w));
-          if (key >= key_min && key < kb_last) {
-            kb_insert_smem<K>(kb, kstride, key, kb_last);
-            if (kb_last != kEmptyKey) tmax = key_t(kb_last);
+          if (key >= key_min && kb_accepts<K>(kb, kstride, key, kb_n)) {
+            if (kb_insert_smem<K>(kb, kstride, key, kb_n)) tmax = key_t(kb[(K - 1) * kstride]);
           }
         }
       });
