@@ -901,6 +901,14 @@ def main():
             dist.barrier()
         value_retrace = world * R * args.steps / (slowest_rank_ms(t0.elapsed_time(t1), world, dev) / 1e3) / 1e6
 
+    # traversal work of one step, counted outside the timed region (the
+    # counters cost the traversal a few per cent, so they are off while timing)
+    tr.set_work_counters(True)
+    tr.reset_stats()
+    step()
+    st_work = tr.stats()
+    tr.set_work_counters(False)
+
     # ---------------- roofline of the dominant kernel (adjoint)
     fwd_ms, bwd_ms = timed_kernels(3)
     fwd_plain_ms, bwd_retrace_ms = timed_kernels(2, cached=False) if use_cache else (fwd_ms, bwd_ms)
@@ -1076,7 +1084,7 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "traversal": ({k: tuned.get(k) for k in ("traversal", "k", "stack_depth", "split", "collect")} if tuned else "default"),
                    "hits_per_ray": {"evaluated": evals / max(rays_step, 1), "blended": blends / max(rays_step, 1)},
-                   "traversal_per_ray": {k: st[k] / max(st["rays"], 1)
+                   "traversal_per_ray": {k: st_work[k] / max(st_work["rays"], 1)
                                          for k in ("queries", "node_visits", "triangle_tests",
                                                    "packet_node_visits")}},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

@@ -21,6 +21,7 @@ struct tt_tracer {
   int fwd_grid = 0, bwd_grid = 0, collect_grid = 0;
   bool split_forward = true;  // plain forward with a hit cache: collecting pass + shading pass
   int collect_queries = 1;    // queries a ray's collecting pass stores at most (0 = all)
+  bool count_work = false;    // node visits and triangle tests counted into the stats
   bool sort_secondary = true; // secondary passes: spawned rays traced in sorted order
   tt::DevBuf sec_sort;        // their sort keys / indices (2 x 2 x 4R words) and the sort's histogram
   int cfg_id = tt::kCfgPackets16;
@@ -191,6 +192,7 @@ int tt_set_option(tt_tracer* h, int option, int value) {
   switch (option) {
     case TT_OPT_SPLIT_FORWARD: h->split_forward = value != 0; return TT_OK;
     case TT_OPT_SORT_SECONDARY: h->sort_secondary = value != 0; return TT_OK;
+    case TT_OPT_WORK_COUNTERS: h->count_work = value != 0; return TT_OK;
     case TT_OPT_COLLECT_QUERIES:
       TT_REQUIRE(h, value >= 0, "collect_queries must be >= 0");
       h->collect_queries = value;
@@ -270,6 +272,7 @@ static tt::TraceParams base_params(tt_tracer* h) {
   p.mode = h->cfg.exact_adjoint ? tt::kShadeExact : (h->cfg.reference_arithmetic ? tt::kShadeRefArith : tt::kShadeRef);
   p.variant = h->cfg.variant;
   p.cfg = h->cfg_id;
+  p.count_work = h->count_work ? 1 : 0;
   p.work = h->scratch.as<int>();
   p.status = h->scratch.as<int>() + 1;
   p.stats = reinterpret_cast<unsigned long long*>(h->scratch.as<char>() + 16);
@@ -843,7 +846,7 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
       TT_CUDA(h, tt::launch_sec_sort_keys(p, keys, vals, s));
       TT_CUDA(h, tt::sort_pairs(keys, vals, keys2, vals2, hist, p.sec.cap[level], 32, &second, s));
       p.sec.order = second ? vals2 : vals;
-      h->trace_launches += 1 + 3 * 4;
+      h->trace_launches += 1 + tt::sort_pairs_launches(p.sec.cap[level], 32);
     }
     p.cache_mode = tt::kCacheWrite;
     if (h->split_forward) {

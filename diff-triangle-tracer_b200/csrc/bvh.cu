@@ -161,53 +161,107 @@ __global__ void k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift,
   hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of n counters in one block (digit-major histogram).
-__global__ void k_scan_excl(uint32_t* __restrict__ a, int n) {
-  constexpr int T = 1024, K = 8;
+// Exclusive scan of the histogram (digit-major: all tiles' counts of digit
+// 0, then of digit 1, ...), giving each tile's first output position per
+// digit. A 1024-thread block scans chunks of kScanChunk counters (8 a
+// thread): one block walks them all for a small histogram; a large one is
+// scanned as chunks in parallel, then the chunk totals, then each chunk gets
+// its total's prefix added.
+constexpr int kScanThreads = 1024, kScanPer = 8, kScanChunk = kScanThreads * kScanPer;
+
+// Scans a[base, base + kScanChunk) (bounded by n) exclusively, starting from
+// `carry`; returns carry + the chunk's total (to every thread).
+__device__ __forceinline__ uint32_t scan_chunk(uint32_t* __restrict__ a, int n, int base, uint32_t carry) {
   __shared__ uint32_t warp_sum[32];
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
+  __shared__ uint32_t total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int base = 0; base < n; base += T * K) {
-    uint32_t v[K];
-    uint32_t s = 0;
+  uint32_t v[kScanPer];
+  uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int idx = base + threadIdx.x * K + k;
-      v[k] = idx < n ? a[idx] : 0u;
-      s += v[k];
-    }
-    uint32_t incl = s;
+  for (int k = 0; k < kScanPer; ++k) {
+    const int idx = base + threadIdx.x * kScanPer + k;
+    v[k] = idx < n ? a[idx] : 0u;
+    s += v[k];
+  }
+  uint32_t incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = warp_sum[lane];
+    uint32_t wi = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += y;
     }
-    if (lane == 31) warp_sum[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t w = warp_sum[lane];
-      uint32_t wi = w;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-        if (lane >= o) wi += y;
-      }
-      warp_sum[lane] = wi - w;  // exclusive prefix of warp totals
-    }
-    __syncthreads();
-    uint32_t run = carry + warp_sum[warp] + (incl - s);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int idx = base + threadIdx.x * K + k;
-      if (idx < n) a[idx] = run;
-      run += v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == T - 1) carry = run;
-    __syncthreads();
+    warp_sum[lane] = wi - w;  // exclusive prefix of warp totals
+    if (lane == 31) total = wi;
   }
+  __syncthreads();
+  uint32_t run = carry + warp_sum[warp] + (incl - s);
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int idx = base + threadIdx.x * kScanPer + k;
+    if (idx < n) a[idx] = run;
+    run += v[k];
+  }
+  const uint32_t out = carry + total;
+  __syncthreads();  // warp_sum and total are reused by the next chunk
+  return out;
+}
+
+// One block over all of a[0, n).
+__global__ void __launch_bounds__(kScanThreads) k_scan_excl(uint32_t* __restrict__ a, int n) {
+  uint32_t carry = 0;
+  for (int base = 0; base < n; base += kScanChunk) carry = scan_chunk(a, n, base, carry);
+}
+
+// Block b scans chunk b on its own and leaves the chunk's total in sums[b].
+__global__ void __launch_bounds__(kScanThreads) k_scan_chunks(uint32_t* __restrict__ a, int n,
+                                                              uint32_t* __restrict__ sums) {
+  const uint32_t t = scan_chunk(a, n, blockIdx.x * kScanChunk, 0u);
+  if (threadIdx.x == 0) sums[blockIdx.x] = t;
+}
+
+// Adds the exclusive prefix of the chunk totals (scanned sums) to chunk b.
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(uint32_t* __restrict__ a, int n,
+                                                           const uint32_t* __restrict__ sums) {
+  const uint32_t add = sums[blockIdx.x];
+  const int base = blockIdx.x * kScanChunk;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int idx = base + k * kScanThreads + threadIdx.x;
+    if (idx < n) a[idx] += add;
+  }
+}
+
+// Words of histogram storage for `tiles` sort tiles: 256 counters a tile and
+// the chunk totals of the parallel scan.
+size_t hist_words_for_tiles(size_t tiles) {
+  const size_t n = 256 * tiles;
+  return n + (n + kScanChunk - 1) / kScanChunk;
+}
+
+// Launches of one histogram scan.
+int scan_launches(int tiles) { return 256 * tiles <= kScanChunk ? 1 : 3; }
+
+// The exclusive scan of hist[0, 256 * tiles); the chunk totals go after it.
+void scan_hist(uint32_t* hist, int tiles, cudaStream_t s) {
+  const int n = 256 * tiles;
+  if (n <= kScanChunk) {
+    k_scan_excl<<<1, kScanThreads, 0, s>>>(hist, n);
+    return;
+  }
+  const int chunks = (n + kScanChunk - 1) / kScanChunk;
+  uint32_t* sums = hist + n;
+  k_scan_chunks<<<chunks, kScanThreads, 0, s>>>(hist, n, sums);
+  k_scan_excl<<<1, kScanThreads, 0, s>>>(sums, chunks);
+  k_scan_add<<<chunks, kScanThreads, 0, s>>>(hist, n, sums);
 }
 
 // Stable scatter of one tile: keys are visited in index order (16 rounds of
@@ -564,7 +618,7 @@ cudaError_t Bvh::reserve(int P) {
   TT_RES(vals_, n * 4);
   TT_RES(keys2_, n * 4);
   TT_RES(vals2_, n * 4);
-  TT_RES(hist_, 256 * tiles * 4);
+  TT_RES(hist_, hist_words_for_tiles(tiles) * 4);
   TT_RES(bnode_, (n > 1 ? n - 1 : 1) * sizeof(BinNode));
   TT_RES(bparent_, (n > 1 ? n - 1 : 1) * 4);
   TT_RES(lparent_, n * 4);
@@ -618,17 +672,17 @@ cudaError_t Bvh::build(const float* verts, const int* cumsum, int P, cudaStream_
   if (e != cudaSuccess) return e;
   if ((e = prep(verts, cumsum, P, true, s)) != cudaSuccess) return e;
   // morton + 4 x (hist, scan, scatter) + records + karras + bottom-up + collapse init/levels/total + boxes
-  launches_ += 1 + 12 + 1 + (P >= 2 ? 2 : 0) + 1 + (2 + collapse_big_launches(P)) + 1 + 1;
+  const int tiles = (P + kSortTile - 1) / kSortTile;
+  launches_ += 1 + 4 * (2 + scan_launches(tiles)) + 1 + (P >= 2 ? 2 : 0) + 1 + (2 + collapse_big_launches(P)) + 1 + 1;
   k_morton<<<blocks_for(P), kBlock, 0, s>>>(centroid_.as<float4>(), bounds_.as<int>(), P, keys_.as<uint32_t>(),
                                             vals_.as<uint32_t>());
   // 30-bit keys: four 8-bit passes, ending back in keys_/vals_
-  const int tiles = (P + kSortTile - 1) / kSortTile;
   uint32_t *ka = keys_.as<uint32_t>(), *va = vals_.as<uint32_t>();
   uint32_t *kb = keys2_.as<uint32_t>(), *vb = vals2_.as<uint32_t>();
   for (int pass = 0; pass < 4; ++pass) {
     const int shift = 8 * pass;
     k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, P, shift, hist_.as<uint32_t>(), tiles);
-    k_scan_excl<<<1, 1024, 0, s>>>(hist_.as<uint32_t>(), 256 * tiles);
+    scan_hist(hist_.as<uint32_t>(), tiles, s);
     k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, P, shift, hist_.as<uint32_t>(), tiles);
     uint32_t* t;
     t = ka; ka = kb; kb = t;
@@ -903,7 +957,7 @@ BvhStorage carve(char* base, int P, size_t* total) {
   st.vals = c.take<uint32_t>(n);
   st.keys2 = c.take<uint32_t>(n);
   st.vals2 = c.take<uint32_t>(n);
-  st.hist = c.take<uint32_t>(256 * tiles);
+  st.hist = c.take<uint32_t>(hist_words_for_tiles(tiles));
   st.bnode = c.take<BinNode>(inner);
   st.bparent = c.take<int>(inner);
   st.lparent = c.take<int>(n);
@@ -937,7 +991,7 @@ cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* 
   uint32_t *ka = st.keys, *va = st.vals, *kb = st.keys2, *vb = st.vals2;
   for (int pass = 0; pass < 4; ++pass) {
     k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, P, 8 * pass, st.hist, tiles);
-    k_scan_excl<<<1, 1024, 0, s>>>(st.hist, 256 * tiles);
+    scan_hist(st.hist, tiles, s);
     k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, P, 8 * pass, st.hist, tiles);
     uint32_t* t;
     t = ka; ka = kb; kb = t;
@@ -958,7 +1012,12 @@ cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* 
   return cudaGetLastError();
 }
 
-size_t sort_pairs_hist_words(int n) { return (size_t)256 * (size_t)((n + kSortTile - 1) / kSortTile); }
+size_t sort_pairs_hist_words(int n) { return hist_words_for_tiles((size_t)((n + kSortTile - 1) / kSortTile)); }
+
+int sort_pairs_launches(int n, int bits) {
+  if (n <= 0) return 0;
+  return ((bits + 7) / 8) * (2 + scan_launches((n + kSortTile - 1) / kSortTile));
+}
 
 cudaError_t sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2, uint32_t* hist, int n,
                        int bits, bool* in_second, cudaStream_t s) {
@@ -968,7 +1027,7 @@ cudaError_t sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t
   uint32_t *ka = keys, *va = vals, *kb = keys2, *vb = vals2;
   for (int shift = 0; shift < bits; shift += 8) {
     k_sort_hist<<<tiles, kBlock, 0, s>>>(ka, n, shift, hist, tiles);
-    k_scan_excl<<<1, 1024, 0, s>>>(hist, 256 * tiles);
+    scan_hist(hist, tiles, s);
     k_sort_scatter<<<tiles, kBlock, 0, s>>>(ka, va, kb, vb, n, shift, hist, tiles);
     uint32_t* t;
     t = ka; ka = kb; kb = t;

@@ -88,11 +88,14 @@ cudaError_t bvh_build_into(const BvhStorage& st, const float* verts, const int* 
 BvhView bvh_storage_view(const BvhStorage& st, int P);
 
 // Stable LSD radix sort of n (key, value) pairs by the low `bits` bits of the
-// keys, 8 bits a pass, with the builder's kernels: 3 launches a pass, nothing
+// keys, 8 bits a pass, with the builder's kernels (a histogram, a scan of 1
+// or 3 launches and a scatter a pass, sort_pairs_launches in all); nothing
 // synchronises. The sorted pairs end in (keys, vals) after an even number of
 // passes and in (keys2, vals2) after an odd one (*in_second). hist holds
 // sort_pairs_hist_words(n) words.
 size_t sort_pairs_hist_words(int n);
+// Kernel launches of one sort_pairs call.
+int sort_pairs_launches(int n, int bits);
 cudaError_t sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2, uint32_t* hist, int n,
                        int bits, bool* in_second, cudaStream_t s);
 

@@ -162,7 +162,7 @@ __device__ __forceinline__ void slab8(const float4* __restrict__ nd, int nx, int
 template <int SD>
 __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigned long long key_min, float t_hi,
                                       unsigned long long* kb, int kstride, Stack st, float& t_drop, int* status,
-                                      Counters& cnt) {
+                                      Counters& cnt, int count_work) {
   ++cnt.queries;
 #pragma unroll
   for (int i = 0; i < kChunk; ++i) kb[i * kstride] = kEmptyKey;
@@ -198,7 +198,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
     if (ref_is_leaf(ref)) {
       const uint32_t first = leaf_first(ref), ntri = leaf_count(ref);
       if (!TT_IN_BOUNDS(status, first + ntri <= (uint32_t)bvh.P)) continue;
-      cnt.tris += ntri;
+      if (count_work) cnt.tris += ntri;
       for (uint32_t j = 0; j < ntri; ++j) {
         const float4* tr = bvh.tris + 3 * (size_t)(first + j);
         const float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
@@ -213,7 +213,7 @@ __device__ __forceinline__ void query(const BvhView& bvh, const RayW& r, unsigne
       continue;
     }
     if (!TT_IN_BOUNDS(status, ref < (uint32_t)bvh.wide_cap)) continue;
-    ++cnt.nodes;
+    if (count_work) ++cnt.nodes;
     const float4* nd = bvh.nodes + (size_t)ref * kNodeF4;
     float tn[8], tf[8];
     bool hit[8];
@@ -279,7 +279,7 @@ struct WarpStack {
 template <int K>
 __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, bool want,
                                              unsigned long long key_min, float t_hi, unsigned long long* kb, int kstride,
-                                             WarpStack ws, float& t_drop, int* status) {
+                                             WarpStack ws, float& t_drop, int* status, int count_work) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -318,7 +318,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
     if (m == 0) continue;
     if (!TT_IN_BOUNDS(status, ref < (uint32_t)bvh.wide_cap)) continue;  // ref is the same in every lane
     const bool on = (m >> lane) & 1u;
-    if (lane == 0) {
+    if (count_work && lane == 0) {
       ws.cnt[kWNodes] += __popc(m);
       ws.cnt[kWWarpNodes] += 1u;
     }
@@ -351,7 +351,7 @@ __device__ __forceinline__ void packet_query(const BvhView& bvh, const RayW& r, 
       const bool lon = (lm >> lane) & 1u;
       const uint32_t first = leaf_first(lref), ntri = leaf_count(lref);
       if (!TT_IN_BOUNDS(status, first + ntri <= (uint32_t)bvh.P)) continue;  // the same in every lane
-      if (lane == 0) ws.cnt[kWTris] += __popc(lm) * ntri;
+      if (count_work && lane == 0) ws.cnt[kWTris] += __popc(lm) * ntri;
       with_perm(wperm, r, [&](const auto& pm) {
         for (uint32_t j = 0; j < ntri; ++j) {
           const float4* tr = bvh.tris + 3 * (size_t)(first + j);
@@ -1059,7 +1059,7 @@ __device__ __forceinline__ void drive(const TraceParams& p, const Smem& sm, Shad
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
-        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt, p.count_work);
         if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (first) {
             link = cache_put_first<K>(p, g, sm, t_drop);
@@ -1142,7 +1142,8 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       const bool rep = replay && active && (first || cache_has<K>(p, next, cur.key_min));
       const bool trav = active && !rep;
       if (__any_sync(full, trav))
-        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status);
+        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status,
+                        p.count_work);
       const unsigned nrep = __popc(__ballot_sync(full, rep));
       if (lane == 0) ws.cnt[kWReplays] += nrep;
       if (rep) {
@@ -1948,7 +1949,7 @@ __device__ __forceinline__ void drive_items(const TraceParams& p, const Smem& sm
       } else {
         next = kNoEntry;
         const RayW r = make_ray(o, d);
-        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
+        query<SD>(p.bvh, r, cur.key_min, cur.t_hi, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt, p.count_work);
         if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
           if (main_part) {
             link = cache_put_first<K>(p, sh.ridx, sm, t_drop);
@@ -2551,7 +2552,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_hit_stream(HitStreamParams p)
   for (int chunk = 0; chunk < kMaxChunks; ++chunk) {
     float t_drop;
     Counters cnt;
-    query<kStackDepth>(p.bvh, r, key_min, kFar, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt);
+    query<kStackDepth>(p.bvh, r, key_min, kFar, sm.keys, sm.stride, sm.st, t_drop, p.status, cnt, 0);
     int consumed = 0;
     unsigned long long last = 0;
 #pragma unroll

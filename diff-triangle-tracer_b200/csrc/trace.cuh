@@ -134,6 +134,7 @@ struct TraceParams {
   int mode;     // kShade*: how the plain forward / adjoint shade a hit
   int cfg;      // traversal configuration, kCfg*
   int collect_queries;  // collecting pass: queries stored per ray at most (0 = all the march makes)
+  int count_work;       // count node visits and triangle tests (tt_stats), off by default
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)

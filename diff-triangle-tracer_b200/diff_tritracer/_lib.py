@@ -30,6 +30,7 @@ TT_VARIANT_ENVLIGHT = 3
 TT_OPT_SPLIT_FORWARD = 1
 TT_OPT_SORT_SECONDARY = 2
 TT_OPT_COLLECT_QUERIES = 3
+TT_OPT_WORK_COUNTERS = 4
 
 TT_TRAVERSAL_AUTO = 0
 TT_TRAVERSAL_PACKETS = 1

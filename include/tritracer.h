@@ -257,7 +257,12 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  *   pool entries both passes asked for: with a cap of 1 the later queries of
  *   the shading pass's march; otherwise also those the traversal-only pass
  *   made past a ray's cut-off, and a query it was refused counts again when
- *   the shading pass asks for it. */
+ *   the shading pass asks for it.
+ * TT_OPT_WORK_COUNTERS, 0 (default): 1 makes the traversal kernels count
+ *   their node visits and triangle tests into tt_stats (node_visits,
+ *   triangle_tests, packet_node_visits; they stay 0 otherwise). The counts
+ *   cost the packet traversal a shared-memory update per node visit, about
+ *   4 % of its time, so they are off unless asked for. */
 /* Device time of the two passes of the last forward on the handle that ran
  * with `debug` (events, as gpu_time_ms): the traversal-only pass (0 for a
  * fused forward) and the shading pass. No reference counterpart. */
@@ -266,6 +271,7 @@ int tt_forward_pass_times(tt_tracer* h, float* collect_ms, float* shade_ms);
 #define TT_OPT_SPLIT_FORWARD 1
 #define TT_OPT_SORT_SECONDARY 2
 #define TT_OPT_COLLECT_QUERIES 3
+#define TT_OPT_WORK_COUNTERS 4
 int tt_set_option(tt_tracer* h, int option, int value);
 
 /* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the
@@ -327,7 +333,8 @@ int tt_device_status(tt_tracer* h, void* stream);
  * reference counterpart; the reference reports only gpu_time). Evaluated hits
  * are hits at or beyond the near plane whose window function was computed;
  * blended hits are those composited; node visits (per ray), triangle tests and
- * queries (k-closest traversals) describe the traversal work. kernel_launches counts
+ * queries (k-closest traversals) describe the traversal work (node visits and
+ * triangle tests only with TT_OPT_WORK_COUNTERS on). kernel_launches counts
  * every kernel this handle enqueued (BVH steps included). */
 typedef struct tt_stats {
   unsigned long long rays;

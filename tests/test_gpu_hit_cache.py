@@ -284,3 +284,28 @@ def test_split_forward_equals_fused(setup, mode, k, sd, incl, collect):
         assert_grads_equal(b[2], a[2])
         assert b[3] > 0
     tr.set_split_forward(True)
+
+
+@pytest.mark.parametrize("mode,k", [("packets", 32), ("lanes", 16)])
+def test_work_counters_are_opt_in(setup, mode, k):
+    """Node visits and triangle tests are counted only with the option on,
+    and counting changes no output."""
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal=mode)
+    tr.set_traversal(mode, k=k, stack_depth=32)
+    outs = {}
+    for on in (False, True):
+        tr.set_work_counters(on)
+        cache = tr.new_hit_cache(H * W, pool=4 * H * W)
+        col, oth = forward(tr, sc, s, ro, rd, cache)
+        st = tr.stats()
+        tr.device_status()
+        outs[on] = (col.cpu().numpy(), oth.cpu().numpy())
+        assert st["queries"] > 0 and st["rays"] == H * W
+        if on:
+            assert st["node_visits"] > st["rays"] and st["triangle_tests"] > st["rays"]
+            assert (st["packet_node_visits"] > 0) == (mode == "packets")
+        else:
+            assert st["node_visits"] == 0 and st["triangle_tests"] == 0 and st["packet_node_visits"] == 0
+    np.testing.assert_array_equal(outs[False][0], outs[True][0])
+    np.testing.assert_array_equal(outs[False][1], outs[True][1])

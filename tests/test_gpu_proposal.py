@@ -132,6 +132,7 @@ def test_learned_intervals_on_tracer_records():
     sc = scenes.make_scene(20000, seed=11, center_std=0.25, edge_range=(0.06, 0.25))
     s = scene_dict(sc)
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+    tr.set_work_counters(True)  # node visits and triangle tests, for the work comparison below
     tr.build_tri_accel(s["verts"], s["cums"], sc.P, True)
     cams = scenes.sphere_cameras(40, 96, 96, seed=4, fov_deg=20.0)
     views = [tuple(T(a) for a in scenes.camera_rays(c)) for c in cams]
