@@ -20,7 +20,7 @@ struct tt_tracer {
   int num_sms = 148;
   int fwd_grid = 0, bwd_grid = 0, collect_grid = 0;
   bool split_forward = true;  // plain forward with a hit cache: collecting pass + shading pass
-  int collect_queries = 1;    // queries a ray's collecting pass stores at most (0 = all)
+  int collect_queries = 2;    // queries a ray's collecting pass stores at most (0 = all)
   bool count_work = false;    // node visits and triangle tests counted into the stats
   bool sort_secondary = true; // secondary passes: spawned rays traced in sorted order
   tt::DevBuf sec_sort;        // their sort keys / indices (2 x 2 x 4R words) and the sort's histogram

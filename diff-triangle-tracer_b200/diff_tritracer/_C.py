@@ -406,7 +406,7 @@ class OptixTracer:
         check(self._h, lib.tt_forward_pass_times(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
-    def set_collect_queries(self, n: int = 1):
+    def set_collect_queries(self, n: int = 2):
         """Queries per ray the split forward's traversal-only pass stores at
         most (0: all of the march's); the shading pass traverses the rest."""
         check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_COLLECT_QUERIES, int(n)))

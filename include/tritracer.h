@@ -249,7 +249,7 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  *   level of spawned rays in order of direction octant and origin (Morton
  *   code), after a radix sort of the level, so the rays of a warp cross
  *   nearly the same BVH nodes. 0: in the order they were spawned.
- * TT_OPT_COLLECT_QUERIES, n >= 0 (default 1): the traversal-only pass of the
+ * TT_OPT_COLLECT_QUERIES, n >= 0 (default 2): the traversal-only pass of the
  *   split forward stores at most n k-closest queries per ray (0: every query
  *   of the march, also those past the point where the ray's transmittance
  *   would end it, which that pass cannot know); the shading pass traverses

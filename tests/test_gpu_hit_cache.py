@@ -192,6 +192,7 @@ def test_usage_reports_pool_capacity_and_demand(setup):
     sc, s, ro, rd, g, go = setup
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal="packets")
     tr.set_traversal("packets", k=16)
+    tr.set_collect_queries(1)  # the traversal-only pass asks for no query past a ray's cut-off
     R = H * W
     with pytest.raises(RuntimeError, match="not written by a forward"):
         tr.hit_cache_usage(torch.zeros(tr.new_hit_cache(R).numel(), dtype=torch.uint8, device=DEV))
