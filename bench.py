@@ -545,7 +545,7 @@ def widened_leg(dev, d, P, cams, cfg, steps=3):
     return res
 
 
-def secondary_leg(dev, steps=3, seed=0):
+def secondary_leg(dev, steps=3, seed=0, default_only=False):
     """Secondary-ray passes on their benchmark configuration: 500k
     triangles, 20 % dielectric (IOR ~ U[1.3, 1.6]), a 512x1024 lat-long
     environment map (U[0, 1] noise box-filtered 9x9), 2 views of 800x800
@@ -591,12 +591,14 @@ def secondary_leg(dev, steps=3, seed=0):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps, tr.stats()
 
-    tr.set_sort_secondary(False)
-    ms_unsorted, _ = timed()
-    tr.set_sort_secondary(True)
-    tr.set_split_forward(False)
-    ms_fused, _ = timed()
-    tr.set_split_forward(True)
+    ms_unsorted = ms_fused = None
+    if not default_only:  # the schedule's two parts, each switched off once
+        tr.set_sort_secondary(False)
+        ms_unsorted, _ = timed()
+        tr.set_sort_secondary(True)
+        tr.set_split_forward(False)
+        ms_fused, _ = timed()
+        tr.set_split_forward(True)
     ms, st = timed()
     tr.device_status()
     R = 1600 * 800
@@ -761,6 +763,8 @@ def main():
     ap.add_argument("--no-proposal", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--proposal-small", action="store_true", help="learned-proposal leg at profiling size")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary-ray leg")
+    ap.add_argument("--secondary-only", action="store_true",
+                    help="run only the secondary-ray leg, in its default schedule, for --steps steps (profiling)")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the leg timing the exact adjoint, precomputed colours, BVH files and camera rays")
     ap.add_argument("--no-c4", action="store_true", help="skip the batched 3M-triangle, 16-view leg")
@@ -795,6 +799,10 @@ def main():
     import diff_tritracer
     from diff_tritracer import _C
     from diff_tritracer.autotune import autotune
+
+    if args.secondary_only:
+        print(json.dumps({"secondary": secondary_leg(dev, steps=args.steps, default_only=True)}), flush=True)
+        return
 
     name = args.workload
     if name.startswith("c4"):
