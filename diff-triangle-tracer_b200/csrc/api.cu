@@ -758,6 +758,8 @@ static void sec_layout(tt::SecParams& sp, const tt_secondary* sec, tt::SecRecord
   sp.max_depth = sec->max_depth;
   sp.rec = rec;
   sp.count = count;
+  sp.d_env = nullptr;  // the adjoint sets its optional material gradients itself
+  sp.d_ior = nullptr;
   for (int l = 0; l <= tt::kMaxSecDepth; ++l) {
     sp.base[l] = R * ((1 << l) - 1);
     sp.cap[l] = R << l;
@@ -957,6 +959,14 @@ int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary
   p.d_sh = a->dL_dsh;
   int* count = reinterpret_cast<int*>(h->scratch.as<char>() + kSecCountOffset);
   sec_layout(p.sec, sec, h->sec_rec.as<tt::SecRecord>(), h->sec_R, count);
+  if (sec->dL_denv) {
+    p.sec.d_env = sec->dL_denv;
+    TT_CUDA(h, cudaMemsetAsync(sec->dL_denv, 0, (size_t)sec->env_h * sec->env_w * 3 * sizeof(float), s));
+  }
+  if (sec->dL_dior && a->P > 0) {
+    p.sec.d_ior = sec->dL_dior;
+    TT_CUDA(h, cudaMemsetAsync(sec->dL_dior, 0, (size_t)a->P * sizeof(float), s));
+  }
   if (h->sec_cache_bytes > 0) {  // replayed where its header matches (same BVH generation)
     p.hit_cache = h->sec_cache.p;
     p.cache_mode = tt::kCacheRead;

@@ -2049,7 +2049,14 @@ __device__ __noinline__ SpawnDev spawn_rays(float4 a4, float4 b4, float4 c4, flo
 
 // Lat-long lookup: longitude atan2(d.z, d.x) over the columns (wrapping),
 // colatitude acos(d.y) over the rows (clamped), bilinear between texel centres.
-__device__ __forceinline__ float3 env_lookup(const SecParams& s, float3 d) {
+// env_texels gives the four texels (word offsets of their RGB) and the
+// bilinear fractions; the adjoint scatters into the same four.
+struct EnvTexels {
+  size_t t00, t01, t10, t11;
+  float ax, ay;
+};
+
+__device__ __forceinline__ EnvTexels env_texels(const SecParams& s, float3 d) {
   const float kPi = 3.14159265358979f;
   const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
   const float u = atan2f(d.z, d.x) * (0.5f / kPi) + 0.5f;
@@ -2058,19 +2065,56 @@ __device__ __forceinline__ float3 env_lookup(const SecParams& s, float3 d) {
   if (!(fabsf(fx) <= (float)s.env_w)) fx = 0.f;  // NaN direction: any texel, never out of bounds
   if (!(fabsf(fy) <= (float)s.env_h)) fy = 0.f;
   const float x0f = floorf(fx), y0f = floorf(fy);
-  const float ax = fx - x0f, ay = fy - y0f;
   const int W = s.env_w, H = s.env_h;
   const int x0 = (((int)x0f % W) + W) % W, x1 = (x0 + 1) % W;
   const int y0 = max(0, min(H - 1, (int)y0f)), y1 = max(0, min(H - 1, (int)y0f + 1));
+  EnvTexels t;
+  t.ax = fx - x0f;
+  t.ay = fy - y0f;
+  t.t00 = ((size_t)y0 * W + x0) * 3;
+  t.t01 = ((size_t)y0 * W + x1) * 3;
+  t.t10 = ((size_t)y1 * W + x0) * 3;
+  t.t11 = ((size_t)y1 * W + x1) * 3;
+  return t;
+}
+
+__device__ __forceinline__ float3 env_lookup(const SecParams& s, float3 d) {
+  const EnvTexels t = env_texels(s, d);
+  const float ax = t.ax, ay = t.ay;
   const float* e = s.env;
   float out[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float t00 = __ldg(e + ((size_t)y0 * W + x0) * 3 + c), t01 = __ldg(e + ((size_t)y0 * W + x1) * 3 + c);
-    const float t10 = __ldg(e + ((size_t)y1 * W + x0) * 3 + c), t11 = __ldg(e + ((size_t)y1 * W + x1) * 3 + c);
+    const float t00 = __ldg(e + t.t00 + c), t01 = __ldg(e + t.t01 + c);
+    const float t10 = __ldg(e + t.t10 + c), t11 = __ldg(e + t.t11 + c);
     out[c] = (1.f - ay) * ((1.f - ax) * t00 + ax * t01) + ay * ((1.f - ax) * t10 + ax * t11);
   }
   return make_float3(out[0], out[1], out[2]);
+}
+
+// Adjoint of T env(d) in a ray's radiance: dL/d(texel) += g T (bilinear weight).
+__device__ __forceinline__ void env_lookup_bwd(const SecParams& s, float3 d, float T, float g0, float g1, float g2) {
+  const EnvTexels t = env_texels(s, d);
+  const float ax = t.ax, ay = t.ay;
+  const float wt[4] = {(1.f - ay) * (1.f - ax), (1.f - ay) * ax, ay * (1.f - ax), ay * ax};
+  const size_t at[4] = {t.t00, t.t01, t.t10, t.t11};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float f = T * wt[k];
+    red_add(s.d_env + at[k] + 0, g0 * f);
+    red_add(s.d_env + at[k] + 1, g1 * f);
+    red_add(s.d_env + at[k] + 2, g2 * f);
+  }
+}
+
+// d F / d ior of Schlick's reflected share F at a refracting hit:
+// F = r0 + (1 - r0) (1 - cos)^5 with r0 = ((ior - 1) / (ior + 1))^2 (either
+// side of the interface), so dF/dior = dr0/dior (1 - F) / (1 - r0) and
+// dr0/dior = 4 (ior - 1) / (ior + 1)^3.
+__device__ __forceinline__ float fresnel_dF_dior(float n, float F) {
+  const float q = (n - 1.f) / (n + 1.f);
+  const float n1 = n + 1.f;
+  return 4.f * (n - 1.f) / (n1 * n1 * n1) * (1.f - F) / (1.f - q * q);
 }
 
 // The rays of one level: trace, composite, spawn children into the next level.
@@ -2473,6 +2517,10 @@ struct SecBwdShader {
       c0 = F * lr[0] + (1.0f - F) * lt[0];
       c1 = F * lr[1] + (1.0f - F) * lt[1];
       c2 = F * lr[2] + (1.0f - F) * lt[2];
+      if (s.d_ior && r->child_t >= 0) {  // a refracting hit: the colour depends on ior through F
+        const float dL_dF = w * (g0 * (lr[0] - lt[0]) + g1 * (lr[1] - lt[1]) + g2 * (lr[2] - lt[2]));
+        red_add(s.d_ior + prim, dL_dF * fresnel_dF_dior(__ldg(s.ior + prim), F));
+      }
     } else {
       sh_basis(unit(d), p.sh_degree, B);
       const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
@@ -2526,7 +2574,10 @@ struct SecBwdShader {
     return false;
   }
 
-  __device__ __forceinline__ void end() {}
+  // the environment term T env(d) of the ray's radiance
+  __device__ __forceinline__ void end() {
+    if (p.sec.d_env) env_lookup_bwd(p.sec, d, T, g0, g1, g2);
+  }
 };
 
 __global__ void __launch_bounds__(kTraceThreads, 4) k_sec_backward(const __grid_constant__ TraceParams p) {

@@ -93,6 +93,10 @@ struct SecParams {
   // order. The spawned rays sorted by direction octant and origin (Morton
   // code), so that the rays of a warp cross nearly the same BVH nodes.
   const uint32_t* order;
+  // adjoint only, optional: gradients of the environment map and of the
+  // per-triangle IOR (through the Fresnel share), or nullptr
+  float* d_env;
+  float* d_ior;
 };
 
 // Shading modes of the plain forward and adjoint (tt_config): the

@@ -502,9 +502,12 @@ class OptixTracer:
 
     def trace_backward_secondary(self, ray_o, ray_d, triangles_points, sigma, num_points_per_triangle,
                                  cumsum_of_points_per_triangle, colors, others, number_of_points, shs, sh_degree,
-                                 opacities, dL_dpixels, dL_dothers, material, ior, env, max_depth=2):
+                                 opacities, dL_dpixels, dL_dothers, material, ior, env, max_depth=2,
+                                 material_grads=False):
         """Adjoint of the last trace_forward_secondary (same rays and scene):
-        (dL_dtriangle [V,3], dL_dsigma, dL_dopacity, dL_dsh [P,M,3])."""
+        (dL_dtriangle [V,3], dL_dsigma, dL_dopacity, dL_dsh [P,M,3]), and with
+        material_grads also dL_denv [env_h, env_w, 3] and dL_dior [P] (through
+        the Fresnel share; bent directions held constant)."""
         dev = self.device
         P = int(number_of_points)
         ro, rd = _f32(ray_o, "ray_o", dev), _f32(ray_d, "ray_d", dev)
@@ -536,6 +539,10 @@ class OptixTracer:
         a.dL_dtriangle, a.dL_dsigma, a.dL_dopacity, a.dL_dsh = [_ptr(x) for x in grads]
         a.gpu_time_ms = ctypes.cast(None, ctypes.POINTER(ctypes.c_float))
         sec, skeep = self._secondary(material, ior, env, max_depth)
+        if material_grads:
+            grads = grads + (torch.empty((sec.env_h, sec.env_w, 3), dtype=torch.float32, device=dev),
+                             torch.empty((P,), dtype=torch.float32, device=dev))
+            sec.dL_denv, sec.dL_dior = _ptr(grads[4]), _ptr(grads[5])
         check(self._h, lib.tt_backward_secondary(self._h, ctypes.byref(a), ctypes.byref(sec), _stream()))
         self._keep = (ro, rd, verts, sig, npts, cums, col, oth, sh, opac, g, go, bg) + skeep
         return grads

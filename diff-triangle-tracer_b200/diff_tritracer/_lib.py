@@ -120,7 +120,7 @@ class TtMlpStep(ctypes.Structure):
 
 class TtSecondary(ctypes.Structure):
     _fields_ = [("material", _vp), ("ior", _vp), ("env", _vp), ("env_h", ctypes.c_int), ("env_w", ctypes.c_int),
-                ("max_depth", ctypes.c_int)]
+                ("max_depth", ctypes.c_int), ("dL_denv", _vp), ("dL_dior", _vp)]
 
 
 EXPORTS = (

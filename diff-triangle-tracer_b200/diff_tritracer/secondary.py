@@ -33,18 +33,25 @@ class _Secondary(torch.autograd.Function):
          others) = ctx.saved_tensors
         g_color = torch.zeros_like(color) if g_color is None else g_color.contiguous()
         g_others = torch.zeros_like(others) if g_others is None else g_others.contiguous()
-        d_tri, d_sigma, d_opac, d_sh = ctx.tracer.trace_backward_secondary(
+        want_material = ctx.needs_input_grad[12] or ctx.needs_input_grad[13]
+        grads = ctx.tracer.trace_backward_secondary(
             ray_o, ray_d, verts, sigma, num_points, cumsum, color, others, ctx.P, shs, ctx.sh_degree, opacities,
-            g_color, g_others, material, ior, env, ctx.max_depth)
+            g_color, g_others, material, ior, env, ctx.max_depth, material_grads=want_material)
+        d_tri, d_sigma, d_opac, d_sh = grads[:4]
+        d_ior = grads[5].reshape(ior.shape) if want_material and ctx.needs_input_grad[12] else None
+        d_env = grads[4].reshape(env.shape) if want_material and ctx.needs_input_grad[13] else None
         return (None, None, None, d_tri.reshape(verts.shape), d_sigma.reshape(sigma.shape), None, None, None,
-                d_opac.reshape(opacities.shape), d_sh, None, None, None, None, None, None)
+                d_opac.reshape(opacities.shape), d_sh, None, None, d_ior, d_env, None, None)
 
 
 class SecondaryTracer(nn.Module):
     """forward(ray_o, ray_d, triangles_points, sigma, num_points, cumsum, P,
     opacities, shs, material, ior, env) -> (color, others, max_blending,
     scaling, density_factor); gradients flow to the vertices, sigma,
-    opacities and SH coefficients."""
+    opacities and SH coefficients, and, when they require it, to the
+    environment map and the IOR (through the Fresnel share of each
+    refracting hit; the bent directions are held constant, as the spawn
+    geometry is for every input)."""
 
     def __init__(self, sh_degree=3, max_depth=2):
         super().__init__()

@@ -470,6 +470,12 @@ typedef struct tt_secondary {
   const float* env;    /* [env_h][env_w][3] */
   int env_h, env_w;
   int max_depth;       /* 0..TT_MAX_BOUNCES */
+  /* tt_backward_secondary only, optional (NULL: not computed; the forward
+   * ignores both): dL/d(env) [env_h][env_w][3] and dL/d(ior) [P], overwritten.
+   * The IOR gradient goes through Schlick's Fresnel share F of each spawning
+   * hit; the bent directions are held constant, as for every other input. */
+  float* dL_denv;
+  float* dL_dior;
 } tt_secondary;
 int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary* s, void* stream);
 int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary* s, void* stream);

@@ -53,5 +53,11 @@ struct or_args {
   unsigned* chunk_ids;  // [H*W][max_chunks][16]
   float* chunk_tmin;    // [H*W][max_chunks]
   int* chunk_count;     // [H*W] queries made (may exceed max_chunks)
+  // secondary-ray adjoint, optional (precision of the call): gradients of the
+  // environment map [env_h][env_w][3] and of the IOR [P]; and the test hook
+  // SecInputs::ior_fresnel
+  void* denv;
+  void* dior;
+  const float* ior_fresnel;
 };
 }

@@ -134,6 +134,7 @@ static SecInputs to_sec(const or_args* a) {
   s.env_h = a->env_h;
   s.env_w = a->env_w;
   s.max_depth = a->max_depth;
+  s.ior_fresnel = a->ior_fresnel;
   return s;
 }
 
@@ -169,6 +170,8 @@ static int backward_sec_impl(void* scene, const or_args* a, R* dtri, R* dsigma, 
   const Opts opt = to_opts(a, sizeof(R) == 8);
   const R* others = static_cast<const R*>(a->others);
   BwdOut<R> bo{dtri, dsigma, dopac, dsh};
+  bo.denv = static_cast<R*>(a->denv);
+  bo.dior = static_cast<R*>(a->dior);
   const int HW = a->H * a->W;
   parallel_rows(a, [&](int pix) {
     const R gL[3] = {(R)a->dL_dpixels[pix], (R)a->dL_dpixels[HW + pix], (R)a->dL_dpixels[2 * HW + pix]};

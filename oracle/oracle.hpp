@@ -783,6 +783,8 @@ struct BwdOut {
   R* dopac;   // [P]
   R* dsh;     // [P, M, 3]
   R* dcolors = nullptr;  // [P, 3] with precomputed colours
+  R* denv = nullptr;     // secondary rays: [env_h, env_w, 3] environment map
+  R* dior = nullptr;     // secondary rays: [P] IOR (through the Fresnel share)
 };
 
 template <class R>
@@ -1087,6 +1089,10 @@ struct SecInputs {
   const float* env = nullptr;     // [env_h][env_w][3]
   int env_h = 0, env_w = 0;
   int max_depth = 2;
+  // test hook: per-triangle IOR used for the Fresnel share F only (the bent
+  // directions keep `ior`), so that finite differences over it measure the
+  // adjoint's IOR gradient, which holds the directions constant
+  const float* ior_fresnel = nullptr;
 };
 
 // Lat-long lookup: longitude atan2(d.z, d.x) over the columns (wrapping),
@@ -1113,16 +1119,43 @@ inline V3<R> env_lookup(const SecInputs& s, V3<R> d) {
   return V3<R>{(R)out[0], (R)out[1], (R)out[2]};
 }
 
+// Adjoint of T env(d): each of the four texels of the lookup gets
+// gL T (bilinear weight).
+template <class R>
+inline void env_lookup_bwd(const SecInputs& s, V3<R> d, R T, const R gL[3], R* denv, bool mt) {
+  const double kPi = 3.14159265358979323846;
+  const double dx = d.x, dy = d.y, dz = d.z;
+  const double len = std::sqrt(dx * dx + dy * dy + dz * dz);
+  const double u = std::atan2(dz, dx) / (2.0 * kPi) + 0.5;
+  const double v = std::acos(std::fmax(-1.0, std::fmin(1.0, dy / len))) / kPi;
+  const double fx = u * s.env_w - 0.5, fy = v * s.env_h - 0.5;
+  const double x0f = std::floor(fx), y0f = std::floor(fy);
+  const double ax = fx - x0f, ay = fy - y0f;
+  const int W = s.env_w, H = s.env_h;
+  const int x0 = (((int)x0f % W) + W) % W, x1 = (x0 + 1) % W;
+  const int y0 = std::max(0, std::min(H - 1, (int)y0f)), y1 = std::max(0, std::min(H - 1, (int)y0f + 1));
+  const int xs[4] = {x0, x1, x0, x1}, ys[4] = {y0, y0, y1, y1};
+  const double wt[4] = {(1 - ay) * (1 - ax), (1 - ay) * ax, ay * (1 - ax), ay * ax};
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c)
+      atomic_add(&denv[((size_t)ys[k] * W + xs[k]) * 3 + c], gL[c] * T * R(wt[k]), mt);
+}
+
+inline double fresnel_ior(const SecInputs& s, int prim) {
+  return (double)(s.ior_fresnel ? s.ior_fresnel[prim] : s.ior[prim]);
+}
+
 struct Spawn {
   float o[3];   // exact hit point
   float r[3];   // reflected direction
   float t[3];   // refracted direction (if refracts)
   bool refracts;
   double F;     // reflected share
+  double dF_dior;  // its derivative in the IOR, directions held constant
 };
 
 // Reflected / refracted rays at the hit of ray (of, df) on triangle prim.
-inline Spawn spawn_rays(const Inputs& in, int prim, const float* of, const float* df, double ior) {
+inline Spawn spawn_rays(const Inputs& in, int prim, const float* of, const float* df, double ior, double ior_F) {
   const int off = in.cumsum[prim];
   const V3<double> A = from_f<double>(in.verts + 3 * (size_t)off);
   const V3<double> B = from_f<double>(in.verts + 3 * (size_t)(off + 1));
@@ -1139,7 +1172,9 @@ inline Spawn spawn_rays(const Inputs& in, int prim, const float* of, const float
   const double c = entering ? -cosi : cosi;
   const double ei = entering ? 1.0 : ior, et = entering ? ior : 1.0;
   const double eta = ei / et;
-  const double r0 = ((ei - et) / (ei + et)) * ((ei - et) / (ei + et));
+  // Schlick's r0 is the same on both sides of the interface
+  const double qF = (ior_F - 1.0) / (ior_F + 1.0);
+  const double r0 = qF * qF;
   const double k = 1.0 - eta * eta * (1.0 - c * c);
   Spawn sp;
   const V3<double> r = du + (2.0 * c) * nf;
@@ -1149,9 +1184,12 @@ inline Spawn spawn_rays(const Inputs& in, int prim, const float* of, const float
     const double m = 1.0 - c;
     const double m2 = m * m;
     sp.F = r0 + (1.0 - r0) * (m2 * m2 * m);
+    // dr0/dior = 4 (ior - 1) / (ior + 1)^3; F moves by (1 - m^5) of it
+    sp.dF_dior = 4.0 * (ior_F - 1.0) / ((ior_F + 1.0) * (ior_F + 1.0) * (ior_F + 1.0)) * (1.0 - m2 * m2 * m);
     t = eta * du + (eta * c - std::sqrt(k)) * nf;
   } else {
     sp.F = 1.0;
+    sp.dF_dior = 0.0;
   }
   const double xs[3] = {x.x, x.y, x.z}, rs[3] = {r.x, r.y, r.z}, ts[3] = {t.x, t.y, t.z};
   for (int i = 0; i < 3; ++i) {
@@ -1193,7 +1231,7 @@ inline V3<R> sec_radiance(const Scene& sc, const Inputs& in, const SecInputs& s,
         V3<R> col;
         if (!spawned && depth < s.max_depth && s.material[prim] == 1) {
           spawned = true;
-          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim]);
+          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim], fresnel_ior(s, (int)prim));
           const V3<R> Lr = sec_radiance<R>(sc, in, s, sp.o, sp.r, depth + 1, opt, nullptr, pix, rec);
           const V3<R> Lt = sp.refracts ? sec_radiance<R>(sc, in, s, sp.o, sp.t, depth + 1, opt, nullptr, pix, rec)
                                        : mk<R>(0, 0, 0);
@@ -1260,7 +1298,7 @@ inline void sec_backward(const Scene& sc, const Inputs& in, const SecInputs& s, 
         bool spawn = false;
         if (!spawned && depth < s.max_depth && s.material[prim] == 1) {
           spawned = spawn = true;
-          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim]);
+          const Spawn sp = spawn_rays(in, (int)prim, of, df, (double)s.ior[prim], fresnel_ior(s, (int)prim));
           const V3<R> Lr = sec_radiance<R>(sc, in, s, sp.o, sp.r, depth + 1, opt, nullptr, 0, nullptr);
           V3<R> Lt = mk<R>(0, 0, 0);
           const R gr[3] = {gL[0] * bw * R(sp.F), gL[1] * bw * R(sp.F), gL[2] * bw * R(sp.F)};
@@ -1272,6 +1310,10 @@ inline void sec_backward(const Scene& sc, const Inputs& in, const SecInputs& s, 
             sec_backward<R>(sc, in, s, sp.o, sp.t, depth + 1, opt, gt, nullptr, nullptr, bo);
           }
           col = R(sp.F) * Lr + R(1.0 - sp.F) * Lt;
+          if (bo.dior && sp.refracts) {
+            const R dL_dF = bw * (gL[0] * (Lr.x - Lt.x) + gL[1] * (Lr.y - Lt.y) + gL[2] * (Lr.z - Lt.z));
+            atomic_add(&bo.dior[prim], dL_dF * R(sp.dF_dior), opt.mt);
+          }
         } else {
           col = sh_color(in, (int)prim, d, clamped);
         }
@@ -1300,6 +1342,7 @@ inline void sec_backward(const Scene& sc, const Inputs& in, const SecInputs& s, 
         return false;
       },
       [](const Hit&) {});
+  if (bo.denv) env_lookup_bwd<R>(s, d, T, gL, bo.denv, opt.mt);
 }
 
 }  // namespace tto

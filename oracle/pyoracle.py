@@ -44,6 +44,7 @@ class OrArgs(ctypes.Structure):
         ("precomp", _fp), ("dprecomp", ctypes.c_void_p),
         ("max_chunks", ctypes.c_int), ("chunk_ids", ctypes.POINTER(ctypes.c_uint32)), ("chunk_tmin", _fp),
         ("chunk_count", _ip),
+        ("denv", ctypes.c_void_p), ("dior", ctypes.c_void_p), ("ior_fresnel", _fp),
     ]
 
 
@@ -79,6 +80,8 @@ class BwdResult:
     dopac: np.ndarray
     dsh: np.ndarray
     dcolors: np.ndarray | None = None
+    denv: np.ndarray | None = None  # secondary rays: [env_h, env_w, 3]
+    dior: np.ndarray | None = None  # secondary rays: [P]
 
 
 class _Runner:
@@ -141,7 +144,9 @@ class _Runner:
 
     @staticmethod
     def _secondary(a, keep, secondary):
-        """Secondary-ray inputs: dict(material [P] int, ior [P], env [h, w, 3], max_depth)."""
+        """Secondary-ray inputs: dict(material [P] int, ior [P], env [h, w, 3],
+        max_depth; optional ior_fresnel [P]: the IOR of the Fresnel share
+        only, for finite differences of the IOR gradient)."""
         if secondary is None:
             return ""
         keep["material"] = _c(secondary["material"], np.int32)
@@ -150,6 +155,9 @@ class _Runner:
         a.material, a.ior, a.env = _ptr(keep["material"], _ip), _ptr(keep["ior"]), _ptr(keep["env"])
         a.env_h, a.env_w = keep["env"].shape[0], keep["env"].shape[1]
         a.max_depth = int(secondary.get("max_depth", 2))
+        if secondary.get("ior_fresnel") is not None:
+            keep["ior_fresnel"] = _c(secondary["ior_fresnel"], np.float32)
+            a.ior_fresnel = _ptr(keep["ior_fresnel"])
         return "secondary_"
 
     def forward(self, scene, ray_o, ray_d, bg=None, extra=None, variant=0, precision=32, tmin_inclusive=True,
@@ -228,6 +236,11 @@ class _Runner:
         dsigma = np.zeros(P, dt)
         dopac = np.zeros(P, dt)
         dsh = np.zeros((P, M, 3), dt)
+        denv = dior = None
+        if sec:
+            denv = np.zeros(keep["env"].shape, dt)
+            dior = np.zeros(P, dt)
+            a.denv, a.dior = denv.ctypes.data, dior.ctypes.data
         t = ctypes.POINTER(ctypes.c_float if precision == 32 else ctypes.c_double)
         if self.prefix == "ref":
             assert precision == 32
@@ -240,6 +253,7 @@ class _Runner:
             raise RuntimeError(f"{self.prefix} backward failed ({rc})")
         res = BwdResult(dtri, dsigma, dopac, dsh)
         res.dcolors = dcolors
+        res.denv, res.dior = denv, dior
         return res
 
     def close(self):

@@ -37,7 +37,7 @@ def setup():
     return sc, ro, rd, sec
 
 
-def gpu_secondary(tr, sc, ro, rd, sec, g=None, go=None, max_depth=2):
+def gpu_secondary(tr, sc, ro, rd, sec, g=None, go=None, max_depth=2, material_grads=False):
     color, others, maxb = tr.trace_forward_secondary(
         T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P, T(sc.shs), 3,
         T(sc.opacities), scaling := torch.zeros(sc.P, device=DEV), density := torch.zeros(sc.P, device=DEV),
@@ -47,7 +47,7 @@ def gpu_secondary(tr, sc, ro, rd, sec, g=None, go=None, max_depth=2):
         out["grads"] = tr.trace_backward_secondary(
             T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), color, others, sc.P,
             T(sc.shs), 3, T(sc.opacities), T(g), T(go), T(sec["material"]), T(sec["ior"]), T(sec["env"]),
-            max_depth)
+            max_depth, material_grads=material_grads)
     torch.cuda.synchronize()
     tr.device_status()
     return {k: (v.cpu().numpy() if torch.is_tensor(v) else [x.cpu().numpy() for x in v]) for k, v in out.items()}
@@ -64,7 +64,7 @@ def test_forward_and_adjoint_vs_fp64_oracle(oracle, setup, max_depth):
     ok = (ref.margin > MARGIN).reshape(H, W)
     assert ok.mean() > 0.95, ok.mean()
     g, go = g * ok[None], go * ok[None]
-    got = gpu_secondary(tr, sc, ro, rd, sec, g, go, max_depth)
+    got = gpu_secondary(tr, sc, ro, rd, sec, g, go, max_depth, material_grads=True)
     st = tr.stats()
     assert st["rays"] > H * W * 1.5  # the queue really held spawned rays
     for key in ("color", "others"):
@@ -79,7 +79,9 @@ def test_forward_and_adjoint_vs_fp64_oracle(oracle, setup, max_depth):
     np.testing.assert_allclose(got["max_blending"][~skip], ref.max_blending[~skip], rtol=RTOL, atol=ATOL)
     rb = oracle.backward(sc, ro, rd, ref.color, ref.others, g, go, precision=64, exact=True, canonical=True,
                          nthreads=8, secondary=sec)
-    for key, x in zip(("dtri", "dsigma", "dopac", "dsh"), got["grads"]):
+    # the environment map's and the IOR's gradients too (the oracle's FP64
+    # restatement is checked against central differences on the CPU)
+    for key, x in zip(("dtri", "dsigma", "dopac", "dsh", "denv", "dior"), got["grads"]):
         e = rel_norm(x, getattr(rb, key))
         print(f"depth {max_depth} {key}: rel L2 {e:.2e}")
         assert np.linalg.norm(getattr(rb, key)) > 0
@@ -122,6 +124,31 @@ def test_autograd_module_and_state(setup):
                                     T(sc.cumsum), color.detach(), others, sc.P, T(sc.shs), 3, T(sc.opacities),
                                     torch.zeros_like(color), torch.zeros_like(others), T(sec["material"]),
                                     T(sec["ior"]), T(sec["env"]), 2)
+
+
+def test_autograd_module_material_gradients(setup):
+    """With the environment map and the IOR requiring gradients, the module
+    returns the adjoint's material gradients for them (and the same
+    geometry gradients as without)."""
+    sc, ro, rd, sec = setup
+    g, go = scenes.upstream_grads(H, W, seed=13, others_std=0.0)
+    grads = {}
+    for want in (False, True):
+        mod = SecondaryTracer(max_depth=2)
+        opac = T(sc.opacities).requires_grad_(True)
+        env = T(sec["env"]).requires_grad_(want)
+        ior = T(sec["ior"]).requires_grad_(want)
+        color = mod(T(ro), T(rd), T(sc.verts.reshape(-1)), T(sc.sigma), T(sc.num_points), T(sc.cumsum), sc.P, opac,
+                    T(sc.shs), T(sec["material"]), ior, env)[0]
+        (color * T(g)).sum().backward()
+        torch.cuda.synchronize()
+        mod.tracer.device_status()
+        grads[want] = (opac.grad.cpu().numpy(), env.grad, ior.grad)
+    assert grads[False][1] is None and grads[False][2] is None
+    _, env_g, ior_g = grads[True]
+    assert env_g.shape == (32, 64, 3) and ior_g.shape == (sc.P,)
+    assert env_g.abs().sum() > 0 and ior_g.abs().sum() > 0
+    assert rel_norm(grads[True][0], grads[False][0]) < 1e-6
 
 
 def test_adjoint_replays_the_ray_tree_queries(setup):
