@@ -742,7 +742,6 @@ int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int 
 static int check_secondary(tt_tracer* h, const tt_secondary* sec, int P) {
   TT_REQUIRE(h, sec != nullptr, "null secondary-ray description");
   TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "secondary-ray passes need the plain program");
-  TT_REQUIRE(h, h->cfg.exact_adjoint == 0, "secondary-ray passes have the reference-style adjoint only");
   TT_REQUIRE(h, sec->max_depth >= 0 && sec->max_depth <= TT_MAX_BOUNCES, "max_depth must be in [0, 2]");
   TT_REQUIRE(h, sec->env && sec->env_h > 0 && sec->env_w > 0, "need an environment map [env_h][env_w][3]");
   TT_REQUIRE(h, P == 0 || (sec->material && sec->ior), "need material and ior per triangle");

@@ -2541,15 +2541,24 @@ struct SecBwdShader {
     const float inv1a = 1.0f / (1.0f - alpha);
     float dL_dalpha = g0 * (T * c0 - (Cf0 - C0) * inv1a) + g1 * (T * c1 - (Cf1 - C1) * inv1a) +
                       g2 * (T * c2 - (Cf2 - C2) * inv1a);
-    dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
+    // The exact adjoint differentiates the outputs the passes compute: the
+    // depth channel is 0 there (as in the reference), so it has no gradient,
+    // and a clamped alpha passes none; the reference-style adjoint keeps
+    // backward.cu's depth term and differentiates through the clamp.
+    const bool exact = p.mode == kShadeExact;
+    if (!exact) dL_dalpha += gD * (T * g.t - (Df - D) * inv1a);
     dL_dalpha += gN0 * (T * g.n.x - (Nf0 - N0) * inv1a) + gN1 * (T * g.n.y - (Nf1 - N1) * inv1a) +
                  gN2 * (T * g.n.z - (Nf2 - N2) * inv1a);
-    red_add(p.d_opac + prim, dL_dalpha * g.Cx);
-    const float dL_dC = opacity * dL_dalpha;
+    const bool live = !exact || opacity * g.Cx < kAlphaMax;
+    const float dL_dC = live ? opacity * dL_dalpha : 0.0f;
+    if (live) red_add(p.d_opac + prim, dL_dalpha * g.Cx);
     if (g.phi_final > 0.0f) red_add(p.d_sigma + prim, dL_dC * g.Cx * logf(g.phi_final));
     const float dL_dphi = sig / g.phi_max * dL_dC * g.Cx;
     float3 gv[3];
-    window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
+    if (exact)  // the full chain rule of the window function and the face normal; spawn geometry held constant
+      window_bwd_exact(g, d, dL_dphi, dL_dC * sig * g.Cx, make_float3(gN0 * w, gN1 * w, gN2 * w), 0.0f, gv);
+    else
+      window_bwd(g, dL_dphi, make_float3(gN0 * w, gN1 * w, gN2 * w), gv);
     float* dt = p.d_tri + 3 * (size_t)__ldg(p.cumsum + prim);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

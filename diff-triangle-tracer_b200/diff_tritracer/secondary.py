@@ -53,9 +53,12 @@ class SecondaryTracer(nn.Module):
     refracting hit; the bent directions are held constant, as the spawn
     geometry is for every input)."""
 
-    def __init__(self, sh_degree=3, max_depth=2):
+    def __init__(self, sh_degree=3, max_depth=2, exact_adjoint=False):
         super().__init__()
-        self.tracer = _C.OptixTracer("", "forward.ptx", "backward.ptx")
+        # exact_adjoint: the full chain rule of the window function (vertex
+        # gradients included) for every triangle; the spawn geometry stays
+        # constant
+        self.tracer = _C.OptixTracer("", "forward.ptx", "backward.ptx", exact_adjoint=exact_adjoint)
         self.sh_degree, self.max_depth = sh_degree, max_depth
         self._built = False
 

@@ -77,7 +77,8 @@ typedef struct tt_config {
                          (sum w t), middepth (t of the hit after which T <= 0.5) and
                          distortion (sum over hit pairs i < j of w_i w_j (t_i - t_j)^2), all
                          differentiated by the adjoint. No reference counterpart; plain
-                         program only */
+                         program only (the secondary-ray passes take it for their adjoint
+                         without the extra channels, see tt_forward_secondary) */
   int reference_arithmetic; /* 0 (default): each hit's point on its triangle comes from an
                          FP64 ray/plane solve and the window function is evaluated
                          relative to vertex A, which holds ~7 digits of the incircle; 1:
@@ -461,7 +462,12 @@ int tt_mlp_intervals(tt_tracer* h, const tt_mlp* net, const tt_view* views, int 
  * out_others, density_factor, scaling and max_blending come from the primary
  * rays only. The adjoint differentiates every ray of the tree with the spawn
  * geometry (directions, F) held constant, and uses the ray tree of the last
- * tt_forward_secondary on the handle (same rays, scene and max_depth).
+ * tt_forward_secondary on the handle (same rays, scene and max_depth). With
+ * tt_config.exact_adjoint it applies the full chain rule of the window
+ * function and face normal (no gradient through a clamped alpha) to the
+ * outputs the passes compute; depth, middepth and distortion stay 0 here,
+ * so their upstream gradients are ignored. Only the spawning triangles'
+ * vertex gradients then still hold the spawn geometry constant.
  * One view per call (H, W, rays and outputs of the argument block). */
 #define TT_MAX_BOUNCES 2
 typedef struct tt_secondary {

@@ -1329,14 +1329,23 @@ inline void sec_backward(const Scene& sc, const Inputs& in, const SecInputs& s, 
           dL_dalpha += gL[ch] * (T * c[ch] - (final_color[ch] - C[ch]) * inv_1_alpha);
         }
         if (g_others) {
-          dL_dalpha += gD * (T * hit_t - (final_depth - D) * inv_1_alpha);
+          // the exact adjoint differentiates the outputs the passes compute:
+          // depth is 0 there, so it has no gradient (the reference-style
+          // adjoint keeps backward.cu's depth term)
+          if (!opt.exact_adjoint) dL_dalpha += gD * (T * hit_t - (final_depth - D) * inv_1_alpha);
           dL_dalpha += sum3(vmul(gN, T * w.n - (final_normal - N) * inv_1_alpha));
         }
-        atomic_add(&bo.dopac[prim], dL_dalpha * w.Cx, opt.mt);
-        const R dL_dC = opacity * dL_dalpha;
+        const bool live = !opt.exact_adjoint || opacity * w.Cx < R(kAlphaMax);
+        const R dL_dC = live ? opacity * dL_dalpha : R(0);
+        if (live) atomic_add(&bo.dopac[prim], dL_dalpha * w.Cx, opt.mt);
         if (w.phi_final > R(0)) atomic_add(&bo.dsigma[prim], dL_dC * w.Cx * fast_log<R>(w.phi_final), opt.mt);
         const R dL_dphi_x = (R)in.sigma[prim] / w.phi_max * dL_dC * w.Cx;
-        window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, gN * bw, bo.dtri, opt.mt);
+        if (opt.exact_adjoint) {  // full chain rule; the spawn geometry stays constant
+          const R dL_ddist = -dL_dC * (R)in.sigma[prim] * w.Cx / w.dist;
+          window_bwd_exact(in, (int)prim, d, hp, w, dL_dphi_x, dL_ddist, gN * bw, R(0), bo.dtri, opt.mt);
+        } else {
+          window_bwd(in, (int)prim, hp, dL_dphi_x, w.phi_max, w.d, gN * bw, bo.dtri, opt.mt);
+        }
         if (!spawn) sh_color_bwd(in, (int)prim, d, clamped, dL_dcolor, bo.dsh, opt.mt);
         T = test_T;
         return false;
