@@ -484,6 +484,11 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
   }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));
+  // with a cache, the packet configurations run the adjoint as a pair: a
+  // replay-only build (no traversal code, for a complete cache) and the
+  // traversing one; each checks the cache on the device and one returns
+  p.bwd_pair = p.hit_cache && (p.cfg == tt::kCfgPackets16 || p.cfg == tt::kCfgPackets32) ? 1 : 0;
+  if (p.bwd_pair) ++h->trace_launches;
   TT_CUDA(h, tt::launch_backward(p, h->bwd_grid, s));
   ++h->trace_launches;
   if (a->debug) {
@@ -533,6 +538,8 @@ int tt_device_status(tt_tracer* h, void* stream) {
   if (st & tt::kStatusBounds) return fail(h, TT_ERR_BOUNDS, "a device index check failed (TT_BOUNDS_CHECK build)");
   if (st & tt::kStatusStack) return fail(h, TT_ERR_STACK, "traversal stack overflow made no progress on some ray");
   if (st & tt::kStatusTimeout) return fail(h, TT_ERR_TIMEOUT, "a bounded device loop gave up");
+  if (st & tt::kStatusCacheMiss)
+    return fail(h, TT_ERR_STATE, "the adjoint's hit cache lacked a query its forward had stored");
   return TT_OK;
 }
 

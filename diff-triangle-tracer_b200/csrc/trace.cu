@@ -915,6 +915,14 @@ __device__ __forceinline__ bool cache_replays(const TraceParams& p) {
          h->pool_cap == p.cache_pool_cap;
 }
 
+// The forward stored every query it made: no pool entry was refused (a
+// missing query always follows a refusal, and pool_used counts refused
+// requests too). The adjoint can then replay every query of every march.
+template <int K>
+__device__ __forceinline__ bool cache_complete(const TraceParams& p) {
+  return cache_replays<K>(p) && cache_header_ptr(p)->pool_used <= p.cache_pool_cap;
+}
+
 // Forward, first query of ray g. Returns where the entry of its next query
 // gets linked (the high half of row k).
 template <int K>
@@ -1104,7 +1112,11 @@ __device__ __forceinline__ WarpStack warp_stack(unsigned char* base) {
   return ws;
 }
 
-template <int K, class Shader>
+// kReplayOnly: every query comes from the hit cache (the adjoint given a
+// complete cache); the build carries no traversal code, which leaves the
+// shading arithmetic more registers. A query the cache lacks (which a
+// complete cache never does) ends that ray and sets kStatusCacheMiss.
+template <int K, class Shader, bool kReplayOnly = false>
 __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& sm, WarpStack ws, Shader& sh,
                                               Counters& cnt) {
   const unsigned full = 0xFFFFFFFFu;
@@ -1141,9 +1153,16 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       // lanes whose query the forward stored replay it; the others traverse
       const bool rep = replay && active && (first || cache_has<K>(p, next, cur.key_min));
       const bool trav = active && !rep;
-      if (__any_sync(full, trav))
-        packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status,
-                        p.count_work);
+      if constexpr (kReplayOnly) {
+        if (trav) {
+          atomicOr(p.status, kStatusCacheMiss);
+          active = false;
+        }
+      } else {
+        if (__any_sync(full, trav))
+          packet_query<K>(p.bvh, r, trav, cur.key_min, cur.t_hi, sm.keys, sm.stride, ws, t_drop, p.status,
+                          p.count_work);
+      }
       const unsigned nrep = __popc(__ballot_sync(full, rep));
       if (lane == 0) ws.cnt[kWReplays] += nrep;
       if (rep) {
@@ -1240,13 +1259,13 @@ constexpr size_t smem_bytes_for() {
 constexpr int kXD = 0, kXWsum = 1, kXWt2 = 2, kXMid = 3, kXDist2 = 4, kXMidSet = 5, kExactSlots = 6;
 constexpr size_t kExactSmemBytes = (size_t)kTraceThreads * kExactSlots * 4;
 
-template <int CFG, class Shader>
+template <int CFG, class Shader, bool kReplayOnly = false>
 __device__ __forceinline__ void run(const TraceParams& p, Shader& sh, Counters& cnt) {
   using C = TraversalCfg<CFG>;
   if constexpr (C::packets) {
     unsigned char* rest;
     const Smem sm = packet_smem<C::K>(rest);
-    drive_packets<C::K>(p, sm, warp_stack(rest), sh, cnt);
+    drive_packets<C::K, Shader, kReplayOnly>(p, sm, warp_stack(rest), sh, cnt);
   } else {
     drive<C::SD>(p, thread_smem<C::SD>(), sh, cnt);
   }
@@ -1872,11 +1891,17 @@ struct BwdShader {
   __device__ __forceinline__ void end() {}
 };
 
-template <int CFG, int MODE>
+// The adjoint. REPLAY: the replay-only build (packet configurations), which
+// needs a complete hit cache. Given a cache, the host launches the two builds
+// back to back (p.bwd_pair): the replay-only one works when the cache is
+// complete, the traversing one otherwise, and the other returns at once;
+// the choice is read on the device, so nothing synchronises.
+template <int CFG, int MODE, bool REPLAY = false>
 __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
+  if (p.bwd_pair && cache_complete<TraversalCfg<CFG>::K>(p) != REPLAY) return;
   Counters cnt;
   BwdShader<MODE> sh(p);
-  run<CFG>(p, sh, cnt);
+  run<CFG, BwdShader<MODE>, REPLAY>(p, sh, cnt);
   const unsigned s = __reduce_add_sync(0xFFFFFFFFu, cnt.replays);
   if ((threadIdx.x & 31) == 0 && s != 0u) atomicAdd(p.stats + kStatReplays, (unsigned long long)s);
 }
@@ -2709,6 +2734,12 @@ cudaError_t launch_forward_t(const TraceParams& p, int grid, cudaStream_t s) {
 
 template <int MODE>
 cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
+  if (p.bwd_pair) {
+    if (p.cfg == kCfgPackets16)
+      k_backward<kCfgPackets16, MODE, true><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p);
+    else
+      k_backward<kCfgPackets32, MODE, true><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p);
+  }
   switch (p.cfg) {
     case kCfgPackets16: k_backward<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;
     case kCfgPackets32: k_backward<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p); break;

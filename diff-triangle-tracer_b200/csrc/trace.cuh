@@ -139,6 +139,7 @@ struct TraceParams {
   int cfg;      // traversal configuration, kCfg*
   int collect_queries;  // collecting pass: queries stored per ray at most (0 = all the march makes)
   int count_work;       // count node visits and triangle tests (tt_stats), off by default
+  int bwd_pair;         // adjoint launched as a replay-only / traversing pair: one of the two works
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)

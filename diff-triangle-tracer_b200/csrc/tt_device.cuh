@@ -30,6 +30,7 @@ constexpr int kMaxWideLevels = 72;  // > 64-bit key depth of the binary tree
 constexpr int kStatusTimeout = 1;
 constexpr int kStatusStack = 2;
 constexpr int kStatusBounds = 4;
+constexpr int kStatusCacheMiss = 8;  // the replay-only adjoint met a query its cache did not hold
 
 // Debug builds (-DTT_BOUNDS_CHECK, `make bounds`): device index checks that
 // record a violation in the status word and let the caller skip the access,
