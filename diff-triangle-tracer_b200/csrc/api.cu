@@ -379,6 +379,14 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
     TT_CUDA(h, tt::launch_collect(p, h->collect_grid, s));
     ++h->trace_launches;
     p.cache_mode = tt::kCacheFill;
+    // When the first pass stores every query of every march (no cap, no
+    // proposed interval stopping it early), the shading pass runs as a pair:
+    // a replay-only build for a complete cache, the traversing one otherwise
+    bool clipped = false;
+    for (int i = 0; i < p.nviews; ++i) clipped = clipped || p.views[i].interval != nullptr;
+    p.fwd_pair = h->collect_queries == 0 && !clipped &&
+                         (p.cfg == tt::kCfgPackets16 || p.cfg == tt::kCfgPackets32) ? 1 : 0;
+    if (p.fwd_pair) ++h->trace_launches;
   }
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev_mid, s));
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));

@@ -1409,12 +1409,24 @@ struct FwdShader {
   }
 };
 
-template <int CFG, int MODE>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
+// Blocks per SM the replay-only builds are compiled for (shading pass and
+// adjoint): 4, as the traversing builds; at 5 the adjoint spilled 240 bytes
+// a thread and took 5.4 ms instead of 5.0 on C2.
+#ifndef TT_REPLAY_BLOCKS
+#define TT_REPLAY_BLOCKS 4
+#endif
+constexpr int kReplayBlocks = TT_REPLAY_BLOCKS;
+
+// REPLAY: the replay-only build for the shading pass of a split forward
+// whose traversal-only pass stored every query of every march; launched as a
+// pair with the traversing build (p.fwd_pair), like the adjoint.
+template <int CFG, int MODE, bool REPLAY = false>
+__global__ void __launch_bounds__(kTraceThreads, REPLAY ? kReplayBlocks : kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
+  if (p.fwd_pair && cache_complete<TraversalCfg<CFG>::K>(p) != REPLAY) return;
   cache_header<TraversalCfg<CFG>::K>(p);
   Counters cnt;
   FwdShader<MODE> sh(p, smem_bytes_for<CFG>());
-  run<CFG>(p, sh, cnt);
+  run<CFG, FwdShader<MODE>, REPLAY>(p, sh, cnt);
   // queries = those the march used, traversed here or replayed from the
   // collecting pass; hit_cache_replays counts the adjoint's replays only
   cnt.queries += cnt.replays;
@@ -1897,7 +1909,7 @@ struct BwdShader {
 // complete, the traversing one otherwise, and the other returns at once;
 // the choice is read on the device, so nothing synchronises.
 template <int CFG, int MODE, bool REPLAY = false>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
+__global__ void __launch_bounds__(kTraceThreads, REPLAY ? kReplayBlocks : kMinBlocks) k_backward(const __grid_constant__ TraceParams p) {
   if (p.bwd_pair && cache_complete<TraversalCfg<CFG>::K>(p) != REPLAY) return;
   Counters cnt;
   BwdShader<MODE> sh(p);
@@ -2715,14 +2727,26 @@ cudaError_t trace_init() {
   };
   opt_in((const void*)k_forward<kCfgPackets16, kShadeExact>, smem_bytes_for<kCfgPackets16>() + kExactSmemBytes);
   opt_in((const void*)k_forward<kCfgPackets32, kShadeExact>, smem_bytes_for<kCfgPackets32>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgPackets16, kShadeExact, true>, smem_bytes_for<kCfgPackets16>() + kExactSmemBytes);
+  opt_in((const void*)k_forward<kCfgPackets32, kShadeExact, true>, smem_bytes_for<kCfgPackets32>() + kExactSmemBytes);
   opt_in((const void*)k_forward<kCfgLanes24, kShadeExact>, smem_bytes_for<kCfgLanes24>() + kExactSmemBytes);
   opt_in((const void*)k_forward<kCfgLanes32, kShadeExact>, smem_bytes_for<kCfgLanes32>() + kExactSmemBytes);
   return e;
 }
 
+// Grid of a replay-only build: the traversing build's grid (SMs x its blocks
+// per SM) at the replay build's blocks per SM.
+inline int replay_grid(int grid) { return grid / kMinBlocks * kReplayBlocks; }
+
 template <int MODE>
 cudaError_t launch_forward_t(const TraceParams& p, int grid, cudaStream_t s) {
   const size_t extra = MODE == kShadeExact ? kExactSmemBytes : 0;
+  if (p.fwd_pair) {
+    if (p.cfg == kCfgPackets16)
+      k_forward<kCfgPackets16, MODE, true><<<replay_grid(grid), kTraceThreads, smem_bytes_for<kCfgPackets16>() + extra, s>>>(p);
+    else
+      k_forward<kCfgPackets32, MODE, true><<<replay_grid(grid), kTraceThreads, smem_bytes_for<kCfgPackets32>() + extra, s>>>(p);
+  }
   switch (p.cfg) {
     case kCfgPackets16: k_forward<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>() + extra, s>>>(p); break;
     case kCfgPackets32: k_forward<kCfgPackets32, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>() + extra, s>>>(p); break;
@@ -2736,9 +2760,9 @@ template <int MODE>
 cudaError_t launch_backward_t(const TraceParams& p, int grid, cudaStream_t s) {
   if (p.bwd_pair) {
     if (p.cfg == kCfgPackets16)
-      k_backward<kCfgPackets16, MODE, true><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p);
+      k_backward<kCfgPackets16, MODE, true><<<replay_grid(grid), kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p);
     else
-      k_backward<kCfgPackets32, MODE, true><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p);
+      k_backward<kCfgPackets32, MODE, true><<<replay_grid(grid), kTraceThreads, smem_bytes_for<kCfgPackets32>(), s>>>(p);
   }
   switch (p.cfg) {
     case kCfgPackets16: k_backward<kCfgPackets16, MODE><<<grid, kTraceThreads, smem_bytes_for<kCfgPackets16>(), s>>>(p); break;

@@ -140,6 +140,7 @@ struct TraceParams {
   int collect_queries;  // collecting pass: queries stored per ray at most (0 = all the march makes)
   int count_work;       // count node visits and triangle tests (tt_stats), off by default
   int bwd_pair;         // adjoint launched as a replay-only / traversing pair: one of the two works
+  int fwd_pair;         // shading pass of the split forward launched as such a pair
   int* work;    // tile counter, zero at launch
   int* status;  // kStatus* bits
   unsigned long long* stats;  // forward counters, kNumStats of them (add_stats in trace.cu)
