@@ -325,8 +325,10 @@ int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream
 const char* tt_last_error(const tt_tracer* h);
 
 /* Synchronises `stream` and returns the device-side status word of the
- * handle's kernels since the last call (TT_OK, TT_ERR_TIMEOUT, TT_ERR_STACK
- * or, in a TT_BOUNDS_CHECK build, TT_ERR_BOUNDS), then clears it. No reference counterpart: the reference's
+ * handle's kernels since the last call (TT_OK, TT_ERR_TIMEOUT, TT_ERR_STACK,
+ * TT_ERR_STATE when an adjoint that found its hit cache complete still met a
+ * query missing from it, or, in a TT_BOUNDS_CHECK build, TT_ERR_BOUNDS),
+ * then clears it. No reference counterpart: the reference's
  * device code has no bounded loops to report on. */
 int tt_device_status(tt_tracer* h, void* stream);
 

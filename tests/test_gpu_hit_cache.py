@@ -310,3 +310,32 @@ def test_work_counters_are_opt_in(setup, mode, k):
             assert st["node_visits"] == 0 and st["triangle_tests"] == 0 and st["packet_node_visits"] == 0
     np.testing.assert_array_equal(outs[False][0], outs[True][0])
     np.testing.assert_array_equal(outs[False][1], outs[True][1])
+
+
+@pytest.mark.parametrize("k", [32, 16])
+def test_replay_only_builds_and_their_fallback(setup, k):
+    """With the first pass storing every query, the shading pass and the
+    adjoint run as pairs of a replay-only build and the traversing one, and
+    the device picks the traversing one when the cache is incomplete (here:
+    no pool at all, so every later query was refused). Either way the image
+    equals the fused forward's bit for bit and the gradients equal the
+    re-traversing adjoint's."""
+    sc, s, ro, rd, g, go = setup
+    tr = _C.OptixTracer("", "forward.ptx", "backward.ptx", traversal="packets")
+    tr.set_traversal("packets", k=k)
+    R = H * W
+    tr.set_split_forward(False)
+    col0, oth0 = forward(tr, sc, s, ro, rd, None)
+    traced, _ = backward(tr, sc, s, ro, rd, col0, oth0, g, go, None)
+    tr.set_split_forward(True)
+    tr.set_collect_queries(0)
+    for pool in (4 * R, 0):
+        cache = tr.new_hit_cache(R, pool=pool)
+        col, oth = forward(tr, sc, s, ro, rd, cache, rebuild=2)
+        queries = tr.stats()["queries"]
+        assert torch.equal(col, col0) and torch.equal(oth, oth0), pool
+        use = tr.hit_cache_usage(cache)
+        assert (use["pool_used"] <= use["pool_cap"]) == (pool > 0), use
+        grads, n = backward(tr, sc, s, ro, rd, col, oth, g, go, cache)
+        assert n == (queries if pool > 0 else R), (pool, n, queries)
+        assert_grads_equal(grads, traced)
