@@ -606,7 +606,7 @@ def secondary_leg(dev, steps=3, seed=0, default_only=False):
             "pixels_per_step": R, "rays_per_step": st["rays"] / steps, "ms_per_step": ms,
             "primary_mrays": R / ms / 1e3, "all_rays_mrays": st["rays"] / steps / ms / 1e3,
             "ms_per_step_spawn_order": ms_unsorted, "ms_per_step_without_split": ms_fused,
-            "step": "forward (3 trace levels, spawned levels sorted by direction octant and origin and traced "
+            "step": "forward (3 trace levels, spawned levels sorted by direction and origin and traced "
                     "as a traversal-only pass plus a shading pass, + 3 resolves) + adjoint (all levels, one launch)"}
 
 

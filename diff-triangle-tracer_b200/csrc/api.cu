@@ -857,7 +857,7 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
     p.sec.level = level;
     p.sec.order = nullptr;
     if (level > 0 && keys) {
-      // trace the spawned rays in (direction octant, origin Morton code) order
+      // trace the spawned rays in (direction bin, origin Morton code) order
       bool second = false;
       TT_CUDA(h, tt::launch_sec_sort_keys(p, keys, vals, s));
       TT_CUDA(h, tt::sort_pairs(keys, vals, keys2, vals2, hist, p.sec.cap[level], 32, &second, s));

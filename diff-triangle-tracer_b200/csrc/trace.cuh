@@ -90,7 +90,7 @@ struct SecParams {
   int* count;                      // [kMaxSecDepth + 1] records per level, levels >= 1 (device)
   // Order in which k_sec_trace takes the records of the level it traces
   // (levels >= 1): item i is record base[level] + order[i]; nullptr = queue
-  // order. The spawned rays sorted by direction octant and origin (Morton
+  // order. The spawned rays sorted by direction and origin (Morton
   // code), so that the rays of a warp cross nearly the same BVH nodes.
   const uint32_t* order;
   // adjoint only, optional: gradients of the environment map and of the

@@ -418,7 +418,7 @@ class OptixTracer:
 
     def set_sort_secondary(self, on: bool = True):
         """Trace each level of spawned secondary rays sorted by direction
-        octant and origin (default) or in spawn order (False). The results
+        (octahedral bins) and origin (default) or in spawn order (False). The results
         are the same."""
         check(self._h, lib.tt_set_option(self._h, _lib.TT_OPT_SORT_SECONDARY, 1 if on else 0))
 

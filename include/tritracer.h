@@ -247,7 +247,7 @@ int tt_set_traversal(tt_tracer* h, int traversal, int k, int stack_depth);
  *   the latency of the node and triangle loads. 0: one fused kernel that
  *   traverses and shades.
  * TT_OPT_SORT_SECONDARY, 1 (default): the secondary-ray passes trace each
- *   level of spawned rays in order of direction octant and origin (Morton
+ *   level of spawned rays in order of direction (octahedral bins) and origin (Morton
  *   code), after a radix sort of the level, so the rays of a warp cross
  *   nearly the same BVH nodes. 0: in the order they were spawned.
  * TT_OPT_COLLECT_QUERIES, n >= 0 (default 2): the traversal-only pass of the
