@@ -24,6 +24,8 @@ struct tt_tracer {
   bool count_work = false;    // node visits and triangle tests counted into the stats
   bool sort_secondary = true; // secondary passes: spawned rays traced in sorted order
   tt::DevBuf sec_sort;        // their sort keys / indices (2 x 2 x 4R words) and the sort's histogram
+  tt::DevBuf sec_order;       // each spawned level's trace order, kept for the adjoint
+  bool sec_sorted = false;    // the last secondary forward sorted its spawned levels
   int cfg_id = tt::kCfgPackets16;
   std::string err;
   tt::Bvh bvh;
@@ -774,6 +776,7 @@ static void sec_layout(tt::SecParams& sp, const tt_secondary* sec, tt::SecRecord
   sp.count = count;
   sp.d_env = nullptr;  // the adjoint sets its optional material gradients itself
   sp.d_ior = nullptr;
+  for (int l = 0; l <= tt::kMaxSecDepth; ++l) sp.bwd_order[l] = nullptr;
   for (int l = 0; l <= tt::kMaxSecDepth; ++l) {
     sp.base[l] = R * ((1 << l) - 1);
     sp.cap[l] = R << l;
@@ -846,6 +849,7 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
     const long long cap = R << sec->max_depth;  // the deepest level's capacity
     const size_t hw = tt::sort_pairs_hist_words((int)cap);
     TT_CUDA(h, h->sec_sort.reserve((size_t)(4 * cap) * 4 + hw * 4));
+    TT_CUDA(h, h->sec_order.reserve((size_t)((2ll << sec->max_depth) - 2) * R * 4));  // levels 1..max_depth
     keys = h->sec_sort.as<uint32_t>();
     vals = keys + cap;
     keys2 = vals + cap;
@@ -863,6 +867,9 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
       TT_CUDA(h, tt::sort_pairs(keys, vals, keys2, vals2, hist, p.sec.cap[level], 32, &second, s));
       p.sec.order = second ? vals2 : vals;
       h->trace_launches += 1 + tt::sort_pairs_launches(p.sec.cap[level], 32);
+      // the adjoint takes the level's rays in the same order
+      TT_CUDA(h, cudaMemcpyAsync(h->sec_order.as<uint32_t>() + (size_t)(p.sec.base[level] - R), p.sec.order,
+                                 (size_t)p.sec.cap[level] * 4, cudaMemcpyDeviceToDevice, s));
     }
     p.cache_mode = tt::kCacheWrite;
     if (h->split_forward) {
@@ -900,6 +907,7 @@ int tt_forward_secondary(tt_tracer* h, const tt_fwd_args* a, const tt_secondary*
   }
   h->sec_R = (int)R;
   h->sec_depth = sec->max_depth;
+  h->sec_sorted = keys != nullptr;
   return TT_OK;
 }
 
@@ -973,6 +981,9 @@ int tt_backward_secondary(tt_tracer* h, const tt_bwd_args* a, const tt_secondary
   p.d_sh = a->dL_dsh;
   int* count = reinterpret_cast<int*>(h->scratch.as<char>() + kSecCountOffset);
   sec_layout(p.sec, sec, h->sec_rec.as<tt::SecRecord>(), h->sec_R, count);
+  if (h->sec_sorted)  // the spawned levels in the order the forward traced them
+    for (int l = 1; l <= sec->max_depth; ++l)
+      p.sec.bwd_order[l] = h->sec_order.as<uint32_t>() + (size_t)(p.sec.base[l] - h->sec_R);
   if (sec->dL_denv) {
     p.sec.d_env = sec->dL_denv;
     TT_CUDA(h, cudaMemsetAsync(sec->dL_denv, 0, (size_t)sec->env_h * sec->env_w * 3 * sizeof(float), s));

@@ -2493,7 +2493,10 @@ struct SecBwdShader {
       i -= sec_level_size(p, level);
       ++level;
     }
-    ridx = s.base[level] + i;
+    // spawned levels in the order the forward traced them (neighbouring
+    // items then gather the same triangles)
+    const uint32_t* ord = level > 0 ? s.bwd_order[level] : nullptr;
+    ridx = s.base[level] + (ord ? (int)__ldg(ord + i) : i);
     const SecRecord* r = s.rec + ridx;
     const int HW = v->H * v->W;
     float tau;

@@ -97,6 +97,9 @@ struct SecParams {
   // per-triangle IOR (through the Fresnel share), or nullptr
   float* d_env;
   float* d_ior;
+  // adjoint only: the order each spawned level was traced in (item i of
+  // level l is record base[l] + bwd_order[l][i]), or nullptr for queue order
+  const uint32_t* bwd_order[kMaxSecDepth + 1];
 };
 
 // Shading modes of the plain forward and adjoint (tt_config): the
