@@ -756,7 +756,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_1M_4x800", choices=sorted(WORKLOADS))
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20,
+                    help="steps of the end-to-end leg (the same count as the device-timed steps by default)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-budget", type=float, default=3.0, help="seconds of CPU work per reference step")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default traversal configuration")
