@@ -112,6 +112,21 @@ long long cache_pool_cap(int k, long long rays, size_t bytes) {
   return (long long)(cap < 0xFFFFFFF0ull ? cap : 0xFFFFFFF0ull);
 }
 
+// The same for the plain forward / adjoint's cache, whose entries also hold
+// their hits' colours (tt::hit_cache_bytes_pool).
+long long cache_pool_cap_colors(int k, long long rays, size_t bytes) {
+  const size_t main = tt::hit_cache_main_bytes(k, rays) + tt::hit_cache_color_bytes(k, rays);
+  if (bytes < main) return -1;
+  const unsigned long long cap = (bytes - main) / ((size_t)(k + 2) * 8 + (size_t)12 * k);
+  return (long long)(cap < 0xFFFFFFF0ull ? cap : 0xFFFFFFF0ull);
+}
+
+// Colour rows of a plain cache with `cap` pool entries (after the pool's keys).
+float* cache_colors_of(void* cache, int k, long long rays, long long cap) {
+  return reinterpret_cast<float*>(static_cast<char*>(cache) + tt::hit_cache_main_bytes(k, rays) +
+                                  (size_t)(k + 2) * 8 * (size_t)cap);
+}
+
 int check_sh(tt_tracer* h, const float* shs, int deg, int M, int P, const float* cols = nullptr) {
   if (cols && !shs) return TT_OK;  // precomputed colours in place of SH
   TT_REQUIRE(h, deg >= 0 && deg <= 3, "sh_degree must be in [0, 3]");
@@ -210,8 +225,7 @@ size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays) {
 
 size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long pool_queries) {
   if (!h || rays < 0 || pool_queries < 0) return 0;
-  const int k = h->k();
-  return tt::hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)pool_queries;
+  return tt::hit_cache_bytes_pool(h->k(), rays, pool_queries);
 }
 
 int tt_camera_rays(tt_tracer* h, const tt_camera* cams, int n_cams, void* stream) {
@@ -238,7 +252,7 @@ int tt_hit_cache_usage(tt_tracer* h, const void* hit_cache, void* stream, int* k
   TT_CUDA(h, cudaMemcpyAsync(&hd, hit_cache, sizeof(hd), cudaMemcpyDeviceToHost, s));
   TT_CUDA(h, cudaStreamSynchronize(s));
   TT_REQUIRE(h, hd.magic == tt::kHitCacheMagic, "hit_cache was not written by a forward");
-  if (k) *k = (int)hd.k;
+  if (k) *k = (int)(hd.k & ~tt::kCacheColorsFlag);
   if (pool_cap) *pool_cap = hd.pool_cap;
   if (pool_used) *pool_used = hd.pool_used;
   return TT_OK;
@@ -343,12 +357,13 @@ static int forward_impl(tt_tracer* h, const tt_fwd_args* a, const tt_view* views
   if (a->hit_cache) {
     TT_REQUIRE(h, h->cfg.variant == TT_VARIANT_PLAIN, "the hit cache is for the plain program only");
     TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
-    const long long cap = cache_pool_cap(h->k(), p.cache_rays, a->hit_cache_bytes);
+    const long long cap = cache_pool_cap_colors(h->k(), p.cache_rays, a->hit_cache_bytes);
     TT_REQUIRE(h, cap >= 0, "hit_cache is too small for these rays (tt_hit_cache_bytes)");
     p.hit_cache = a->hit_cache;
     p.cache_mode = tt::kCacheWrite;
     p.cache_gen = h->bvh_gen;
     p.cache_pool_cap = (uint32_t)cap;
+    p.cache_colors = cache_colors_of(a->hit_cache, h->k(), p.cache_rays, cap);
     TT_CUDA(h, cudaMemsetAsync(a->hit_cache, 0, sizeof(tt::HitCacheHeader), s));
   }
   p.bvh = h->bvh.view();
@@ -484,13 +499,14 @@ static int backward_impl(tt_tracer* h, const tt_bwd_args* a, const tt_view* view
   p.d_sh = a->dL_dsh;
   // a cache written for another k, ray count or pool size (or too small for
   // this k) fails the kernels' header check or is not passed at all: they re-trace
-  const long long cap = a->hit_cache ? cache_pool_cap(h->k(), p.cache_rays, a->hit_cache_bytes) : -1;
+  const long long cap = a->hit_cache ? cache_pool_cap_colors(h->k(), p.cache_rays, a->hit_cache_bytes) : -1;
   if (cap >= 0) {
     TT_REQUIRE(h, (reinterpret_cast<uintptr_t>(a->hit_cache) & 15u) == 0, "hit_cache must be 16-byte aligned");
     p.hit_cache = const_cast<void*>(a->hit_cache);
     p.cache_mode = tt::kCacheRead;
     p.cache_gen = h->bvh_gen;
     p.cache_pool_cap = (uint32_t)cap;
+    p.cache_colors = cache_colors_of(const_cast<void*>(a->hit_cache), h->k(), p.cache_rays, cap);
   }
   TT_CUDA(h, cudaMemsetAsync(p.work, 0, sizeof(int), s));
   if (a->debug) TT_CUDA(h, cudaEventRecord(h->ev0, s));

@@ -848,7 +848,7 @@ __device__ __forceinline__ bool consume_chunk(const Smem& sm, float t_drop, Curs
     cur.last_hit_t = fmaxf(__double2float_rn(__dadd_rn((double)cur.last_hit_t, kStepEps)), t);
     ++cur.ref_pos;
     if (!TT_IN_BOUNDS(status, key_prim(key) < (uint32_t)sh.p.bvh.P)) return true;
-    if (t >= kNear && sh.visit(key_prim(key), t)) return true;
+    if (t >= kNear && visit_slot(sh, key_prim(key), t, i, 0)) return true;
     if (cur.ref_pos == kChunk) {
       // the reference's next optixTrace starts at last_hit_t
       cur.ref_pos = 0;
@@ -911,8 +911,8 @@ template <int K>
 __device__ __forceinline__ bool cache_replays(const TraceParams& p) {
   if (p.cache_mode != kCacheRead && p.cache_mode != kCacheFill) return false;
   const HitCacheHeader* h = cache_header_ptr(p);
-  return h->magic == kHitCacheMagic && h->k == (uint32_t)K && h->rays == p.cache_rays && h->gen == p.cache_gen &&
-         h->pool_cap == p.cache_pool_cap;
+  return h->magic == kHitCacheMagic && (h->k & ~kCacheColorsFlag) == (uint32_t)K && h->rays == p.cache_rays &&
+         h->gen == p.cache_gen && h->pool_cap == p.cache_pool_cap;
 }
 
 // The forward stored every query it made: no pool entry was refused (a
@@ -921,6 +921,43 @@ __device__ __forceinline__ bool cache_replays(const TraceParams& p) {
 template <int K>
 __device__ __forceinline__ bool cache_complete(const TraceParams& p) {
   return cache_replays<K>(p) && cache_header_ptr(p)->pool_used <= p.cache_pool_cap;
+}
+
+// Hit colours beside the queries (plain forward / adjoint of the packet
+// drivers): the forward's shading kernels store them, the adjoint reads them
+// when the header says they were written.
+__device__ __forceinline__ bool cache_colors_on(const TraceParams& p) {
+  if (!p.cache_colors || p.cols) return false;
+  return p.cache_mode != kCacheRead || (cache_header_ptr(p)->k & kCacheColorsFlag) != 0u;
+}
+// Colour rows of the main-part entry of ray g or of pool entry e (row 3i + c
+// holds channel c of slot i; `stride` floats between rows).
+template <int K>
+__device__ __forceinline__ float* cache_color_rows(const TraceParams& p, bool main_part, long long g, uint32_t e,
+                                                   int& stride) {
+  if (main_part) {
+    stride = (int)p.cache_rays;
+    return p.cache_colors + g;
+  }
+  stride = (int)p.cache_pool_cap;
+  return p.cache_colors + (size_t)3 * K * p.cache_rays + e;
+}
+
+// Shaders that use the colour rows take them and the hit's slot; the others
+// ignore both.
+template <class S>
+__device__ __forceinline__ auto set_color_rows(S& sh, float* rows, int stride, int) -> decltype(sh.set_colors(rows, stride)) {
+  sh.set_colors(rows, stride);
+}
+template <class S>
+__device__ __forceinline__ void set_color_rows(S&, float*, int, long) {}
+template <class S>
+__device__ __forceinline__ auto visit_slot(S& sh, uint32_t prim, float t, int slot, int) -> decltype(sh.visit(prim, t, slot)) {
+  return sh.visit(prim, t, slot);
+}
+template <class S>
+__device__ __forceinline__ bool visit_slot(S& sh, uint32_t prim, float t, int, long) {
+  return sh.visit(prim, t);
 }
 
 // Forward, first query of ray g. Returns where the entry of its next query
@@ -992,11 +1029,11 @@ __device__ __forceinline__ bool cache_has(const TraceParams& p, uint32_t e, unsi
 }
 
 template <int K>
-__device__ __forceinline__ void cache_header(const TraceParams& p) {
+__device__ __forceinline__ void cache_header(const TraceParams& p, bool colors = false) {
   if (p.cache_mode == kCacheWrite && blockIdx.x == 0 && threadIdx.x == 0) {
     HitCacheHeader* h = cache_header_ptr(p);  // pool_used was zeroed by the host
     h->magic = kHitCacheMagic;
-    h->k = K;
+    h->k = K | (colors ? kCacheColorsFlag : 0u);  // colours: the shading kernels store them
     h->rays = p.cache_rays;
     h->gen = p.cache_gen;
     h->pool_cap = p.cache_pool_cap;
@@ -1122,6 +1159,7 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const bool replay = cache_replays<K>(p);
+  const bool colors = cache_colors_on(p);
   if (lane < kWCounters) ws.cnt[lane] = 0u;
   __syncwarp();
   WarpCounters wc{ws.cnt};
@@ -1165,7 +1203,12 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       }
       const unsigned nrep = __popc(__ballot_sync(full, rep));
       if (lane == 0) ws.cnt[kWReplays] += nrep;
+      // the cache entry holding this query, if any: its colour rows
+      bool in_main = false;
+      uint32_t entry = kNoEntry;
       if (rep) {
+        in_main = first;
+        entry = next;
         if (p.cache_mode == kCacheFill) link = cache_link_of<K>(p, first, g, next);
         t_drop = cache_get<K>(p, first, g, next, sm, next);
       } else {
@@ -1173,12 +1216,23 @@ __device__ __forceinline__ void drive_packets(const TraceParams& p, const Smem& 
       }
       if (p.cache_mode == kCacheWrite || p.cache_mode == kCacheFill) {
         if (first) {
-          if (trav) link = cache_put_first<K>(p, g, sm, t_drop);
+          if (trav) {
+            link = cache_put_first<K>(p, g, sm, t_drop);
+            in_main = true;
+          }
         } else {
           const bool more = trav && link != nullptr;
           const uint32_t e = cache_alloc(p, more);
-          if (more) link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
+          if (more) {
+            link = e < p.cache_pool_cap ? cache_put_more<K>(p, e, cur.key_min, sm, t_drop, link) : nullptr;
+            if (e < p.cache_pool_cap) entry = e;
+          }
         }
+      }
+      if (colors) {
+        int stride = 0;
+        float* rows = (in_main || entry != kNoEntry) ? cache_color_rows<K>(p, in_main, g, entry, stride) : nullptr;
+        set_color_rows(sh, rows, stride, 0);
       }
       if (active) {
         bool done = consume_chunk<K>(sm, t_drop, cur, p.tmin_inclusive, p.status, sh, wc);
@@ -1300,6 +1354,10 @@ struct FwdShader {
   // per-thread shared-memory slot (kExactSlots words, stride blockDim.x), so
   // the traversal between two shading passes does not carry them in registers
   float* xs = nullptr;
+  // colour rows of the current query's hit-cache entry (raw colour of the
+  // hit in slot i at rows 3i..3i+2, `cstride` floats apart), or nullptr
+  float* crow = nullptr;
+  int cstride = 0;
   unsigned n_rays = 0, n_eval = 0, n_blend = 0;
   unsigned first_eval = 0;  // value of n_eval at the ray's first hit (record only)
 
@@ -1338,7 +1396,15 @@ struct FwdShader {
 
   __device__ __forceinline__ void prepare() {}
 
-  __device__ __forceinline__ bool visit(uint32_t prim, float t) {
+  __device__ __forceinline__ void set_colors(float* rows, int stride) {
+    crow = rows;
+    cstride = stride;
+  }
+
+  __device__ __forceinline__ bool visit(uint32_t prim, float t) { return visit(prim, t, -1); }
+
+  // `slot`: the hit's position in its query (colour rows), -1 if unknown
+  __device__ __forceinline__ bool visit(uint32_t prim, float t, int slot) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const Geom g = shade_geom<MODE>(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, t, __ldg(p.sigma + prim));
     ++n_eval;
@@ -1386,6 +1452,11 @@ struct FwdShader {
       sh_basis(unit(d), p.sh_degree, B);
       const float3 raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
       c = make_float3(fmaxf(raw.x, 0.f), fmaxf(raw.y, 0.f), fmaxf(raw.z, 0.f));
+      if (crow && slot >= 0) {  // for the adjoint, which then reads it instead of the SH
+        crow[(size_t)(3 * slot) * cstride] = raw.x;
+        crow[(size_t)(3 * slot + 1) * cstride] = raw.y;
+        crow[(size_t)(3 * slot + 2) * cstride] = raw.z;
+      }
     }
     C0 += c.x * w;
     C1 += c.y * w;
@@ -1423,7 +1494,7 @@ constexpr int kReplayBlocks = TT_REPLAY_BLOCKS;
 template <int CFG, int MODE, bool REPLAY = false>
 __global__ void __launch_bounds__(kTraceThreads, REPLAY ? kReplayBlocks : kMinBlocks) k_forward(const __grid_constant__ TraceParams p) {
   if (p.fwd_pair && cache_complete<TraversalCfg<CFG>::K>(p) != REPLAY) return;
-  cache_header<TraversalCfg<CFG>::K>(p);
+  cache_header<TraversalCfg<CFG>::K>(p, TraversalCfg<CFG>::packets && p.cache_colors != nullptr);
   Counters cnt;
   FwdShader<MODE> sh(p, smem_bytes_for<CFG>());
   run<CFG, FwdShader<MODE>, REPLAY>(p, sh, cnt);
@@ -1470,7 +1541,7 @@ struct MarchShader {
 
 template <int CFG>
 __global__ void __launch_bounds__(kTraceThreads, kCollectBlocks) k_collect(const __grid_constant__ TraceParams p) {
-  cache_header<TraversalCfg<CFG>::K>(p);
+  cache_header<TraversalCfg<CFG>::K>(p, TraversalCfg<CFG>::packets && p.cache_colors != nullptr);
   Counters cnt;
   MarchShader sh(p);
   run<CFG>(p, sh, cnt);
@@ -1799,7 +1870,18 @@ struct BwdShader {
     }
   }
 
-  __device__ __forceinline__ bool visit(uint32_t prim, float t) {
+  // colour rows of the current query's hit-cache entry (the forward's raw
+  // colour of each blended hit), or nullptr: then the SH are evaluated
+  float* crow = nullptr;
+  int cstride = 0;
+  __device__ __forceinline__ void set_colors(float* rows, int stride) {
+    crow = rows;
+    cstride = stride;
+  }
+
+  __device__ __forceinline__ bool visit(uint32_t prim, float t) { return visit(prim, t, -1); }
+
+  __device__ __forceinline__ bool visit(uint32_t prim, float t, int slot) {
     const float4* tr = p.bvh.tri_prim + 3 * (size_t)prim;
     const float sig = __ldg(p.sigma + prim);
     const Geom g = shade_geom<MODE>(__ldg(tr), __ldg(tr + 1), __ldg(tr + 2), o, d, t, sig);
@@ -1815,7 +1897,11 @@ struct BwdShader {
       raw = make_float3(__ldg(p.cols + 3 * prim), __ldg(p.cols + 3 * prim + 1), __ldg(p.cols + 3 * prim + 2));
     } else {
       sh_basis(unit(d), p.sh_degree, B);
-      raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
+      if (crow && slot >= 0)
+        raw = make_float3(crow[(size_t)(3 * slot) * cstride], crow[(size_t)(3 * slot + 1) * cstride],
+                          crow[(size_t)(3 * slot + 2) * cstride]);
+      else
+        raw = sh_raw(p.shs, p.M, (int)prim, p.sh_degree, B);
     }
     const float c0 = p.cols ? raw.x : fmaxf(raw.x, 0.f), c1 = p.cols ? raw.y : fmaxf(raw.y, 0.f),
                 c2 = p.cols ? raw.z : fmaxf(raw.z, 0.f);

@@ -51,9 +51,23 @@ constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
 __host__ __device__ inline size_t hit_cache_main_bytes(int k, long long rays) {
   return sizeof(HitCacheHeader) + (size_t)(k + 1) * 8 * (size_t)rays;
 }
+// The plain forward / adjoint's cache also holds each stored query's hit
+// colours after the pool: per entry (main part, then pool) 3k float rows,
+// the raw (unclamped) colour of the hit in slot i in rows 3i, 3i + 1, 3i + 2.
+// The shading pass writes the colour of every hit it blends and the adjoint
+// reads it instead of evaluating the hit's SH again. Header k carries
+// kCacheColorsFlag when the colours were written.
+constexpr uint32_t kCacheColorsFlag = 0x10000u;
+__host__ __device__ inline size_t hit_cache_color_bytes(int k, long long entries) {
+  return (size_t)12 * k * (size_t)entries;
+}
+// keys and colours of `rays` first queries and `pool` later ones
+__host__ __device__ inline size_t hit_cache_bytes_pool(int k, long long rays, long long pool) {
+  return hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)pool + hit_cache_color_bytes(k, rays + pool);
+}
 // default pool: later queries of a quarter of the rays
 __host__ __device__ inline size_t hit_cache_bytes(int k, long long rays) {
-  return hit_cache_main_bytes(k, rays) + (size_t)(k + 2) * 8 * (size_t)((rays + 3) / 4);
+  return hit_cache_bytes_pool(k, rays, (rays + 3) / 4);
 }
 // Cache modes: off; write (the forward stores its queries); read (the
 // adjoint replays them); fill (the shading pass of the split forward replays
@@ -154,6 +168,7 @@ struct TraceParams {
   long long cache_rays;       // rays of all views of the launch
   unsigned long long cache_gen;
   uint32_t cache_pool_cap;    // pool entries the buffer holds
+  float* cache_colors;        // plain forward / adjoint: the cache's colour rows (main part), or nullptr
 };
 
 struct HitStreamParams {

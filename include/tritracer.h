@@ -125,12 +125,14 @@ typedef struct tt_fwd_args {
   /* Optional hit cache (plain program; NULL = none; no reference counterpart):
    * 16-byte aligned device memory, rays = H * W (the sum over the views of a
    * batched call). The forward stores every ray's k-closest queries in it:
-   * the first ones in a main part of 32 + (k + 1) * 8 * rays bytes (the
-   * minimum size), later ones in a pool filling the rest, (k + 2) * 8 bytes a
-   * query, while it lasts. tt_hit_cache_bytes(h, rays) sizes the pool for a
-   * quarter of the rays. A tt_backward given the same cache replays the
-   * stored queries instead of traversing the BVH again. tt_forward_noalloc
-   * ignores it. */
+   * the first ones in a main part, later ones in a pool while it lasts; each
+   * stored query takes (k + 1) * 8 bytes of keys (k + 2 in the pool) and 12 * k
+   * bytes for its hits' colours, which the warp-packet traversals store and
+   * the adjoint reads instead of evaluating the SH again. The minimum size is
+   * the main part, 32 + ((k + 1) * 8 + 12 * k) * rays bytes; the pool fills
+   * the rest. tt_hit_cache_bytes(h, rays) sizes the pool for a quarter of the
+   * rays. A tt_backward given the same cache replays the stored queries
+   * instead of traversing the BVH again. tt_forward_noalloc ignores it. */
   void* hit_cache;
   size_t hit_cache_bytes;
 } tt_fwd_args;
@@ -277,13 +279,13 @@ int tt_set_option(tt_tracer* h, int option, int value);
 
 /* Bytes of a hit cache (tt_fwd_args.hit_cache) for `rays` rays under the
  * handle's current traversal configuration, with a pool for later queries of
- * a quarter of the rays: 32 + (k + 1) * 8 * rays + (k + 2) * 8 * ceil(rays / 4).
+ * a quarter of the rays: tt_hit_cache_bytes_pool(h, rays, ceil(rays / 4)).
  * No reference counterpart. */
 size_t tt_hit_cache_bytes(const tt_tracer* h, long long rays);
 
 /* Bytes of a hit cache for `rays` rays whose pool holds `pool_queries` later
  * queries under the handle's current traversal configuration:
- * 32 + (k + 1) * 8 * rays + (k + 2) * 8 * pool_queries. No reference
+ * 32 + ((k + 1) * 8 + 12 * k) * rays + ((k + 2) * 8 + 12 * k) * pool_queries. No reference
  * counterpart. */
 size_t tt_hit_cache_bytes_pool(const tt_tracer* h, long long rays, long long pool_queries);
 

@@ -28,6 +28,12 @@ from diff_tritracer import _C, scenes  # noqa: E402
 from gpu_helpers import DEV, T, rel_norm, settings  # noqa: E402
 from scenes_for_tests import dense_scene, dense_view  # noqa: E402
 
+
+def cache_bytes(k, rays, pool):
+    """Hit cache layout: 32-byte header, k + 1 rows of keys a ray, k + 2 a
+    pool entry, then 3k float rows of hit colours for every entry."""
+    return 32 + (k + 1) * 8 * rays + (k + 2) * 8 * pool + 12 * k * (rays + pool)
+
 H, W = 48, 64
 GRAD_RTOL = 1e-6  # same hits in the same order: only the atomic summation order differs
 
@@ -74,7 +80,7 @@ def test_replay_equals_retrace(setup, mode, k):
     tr.set_traversal(mode, k=k)
     R = H * W
     cache = tr.new_hit_cache(R)
-    assert cache.numel() == 32 + (k + 1) * 8 * R + (k + 2) * 8 * ((R + 3) // 4)
+    assert cache.numel() == cache_bytes(k, R, (R + 3) // 4)
     col, oth = forward(tr, sc, s, ro, rd, cache)
     # the cache does not change the forward
     col0, oth0 = forward(tr, sc, s, ro, rd, None, rebuild=2)
@@ -89,13 +95,13 @@ def test_replay_equals_retrace(setup, mode, k):
     assert R <= n <= queries
     assert_grads_equal(replayed, traced)
     # a pool for every later query: the adjoint replays exactly the forward's queries
-    big = torch.empty(32 + (k + 1) * 8 * R + (k + 2) * 8 * 8 * R, dtype=torch.uint8, device=DEV)
+    big = torch.empty(cache_bytes(k, R, 8 * R), dtype=torch.uint8, device=DEV)
     forward(tr, sc, s, ro, rd, big, rebuild=2)
     replayed, n = backward(tr, sc, s, ro, rd, col, oth, g, go, big)
     assert n == queries
     assert_grads_equal(replayed, traced)
     # no pool at all (the main part only): the first queries
-    small = big[:32 + (k + 1) * 8 * R]
+    small = big[:cache_bytes(k, R, 0)]
     forward(tr, sc, s, ro, rd, small, rebuild=2)
     replayed, n = backward(tr, sc, s, ro, rd, col, oth, g, go, small)
     assert n == R
@@ -168,7 +174,7 @@ def test_autograd_module_with_and_without_cache(setup):
 def test_small_cache_rejected(setup):
     sc, s, ro, rd, g, go = setup
     tr = _C.OptixTracer("", "forward.ptx", "backward.ptx")  # k = 16
-    small = torch.empty(32 + 17 * 8 * H * W - 8, dtype=torch.uint8, device=DEV)
+    small = torch.empty(cache_bytes(16, H * W, 0) - 8, dtype=torch.uint8, device=DEV)
     with pytest.raises(RuntimeError, match="hit_cache"):
         forward(tr, sc, s, ro, rd, small)
 
@@ -198,7 +204,7 @@ def test_usage_reports_pool_capacity_and_demand(setup):
         tr.hit_cache_usage(torch.zeros(tr.new_hit_cache(R).numel(), dtype=torch.uint8, device=DEV))
     # a pool for every later query: the demand is exact (queries after each ray's first)
     big = tr.new_hit_cache(R, pool=8 * R)
-    assert big.numel() == 32 + 17 * 8 * R + 18 * 8 * 8 * R
+    assert big.numel() == cache_bytes(16, R, 8 * R)
     forward(tr, sc, s, ro, rd, big)
     queries = tr.stats()["queries"]
     use = tr.hit_cache_usage(big)
