@@ -277,15 +277,18 @@ def reference_arm(args, rank):
     }), flush=True)
 
 
-def algorithmic_bytes(rays, evals, blends, cache_k=0):
+def algorithmic_bytes(rays, evals, blends, cache_k=0, colors=False):
     """Per launch, from the per-ray figures: forward 24 + 40 + 48 h_e + 204 h_b;
     adjoint 24 + 40 + 28 + 48 h_e + (192 + 2*236) h_b (h_e/h_b = evaluated /
     blended hits, counted by the forward kernel); with a hit cache of k-hit
     queries, (k + 1) * 8 bytes per ray more: written by the forward, read by
-    the adjoint."""
+    the adjoint. With the hit colours in the cache (warp-packet traversals),
+    the forward writes 12 bytes a blended hit and the adjoint reads those 12
+    instead of its 192 bytes of SH."""
     c = (cache_k + 1) * 8 if cache_k else 0
-    fwd = rays * (24 + 40 + c) + 48 * evals + 204 * blends
-    bwd = rays * (24 + 40 + 28 + c) + 48 * evals + (192 + 2 * 236) * blends
+    col = 12 if (cache_k and colors) else 0
+    fwd = rays * (24 + 40 + c) + 48 * evals + (204 + col) * blends
+    bwd = rays * (24 + 40 + 28 + c) + 48 * evals + ((12 if col else 192) + 2 * 236) * blends
     return fwd, bwd
 
 
@@ -946,7 +949,9 @@ def main():
     evals = st["evaluated_hits"] / args.steps
     blends = st["blended_hits"] / args.steps
     k_cache = int(tuned["k"]) if tuned else 16
-    fwd_b, bwd_b = algorithmic_bytes(rays_step, evals, blends, cache_k=k_cache if use_cache else 0)
+    packets = (tuned or {}).get("traversal", "packets") == "packets"
+    fwd_b, bwd_b = algorithmic_bytes(rays_step, evals, blends, cache_k=k_cache if use_cache else 0,
+                                     colors=packets)
     peak, peak_kind = peaks()
     dominant = "adjoint" if bwd_ms >= fwd_ms else "forward"
     dom_bytes, dom_ms = (bwd_b, bwd_ms) if dominant == "adjoint" else (fwd_b, fwd_ms)
