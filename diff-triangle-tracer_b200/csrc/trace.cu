@@ -931,7 +931,8 @@ __device__ __forceinline__ bool cache_colors_on(const TraceParams& p) {
   return p.cache_mode != kCacheRead || (cache_header_ptr(p)->k & kCacheColorsFlag) != 0u;
 }
 // Colour rows of the main-part entry of ray g or of pool entry e (row 3i + c
-// holds channel c of slot i; `stride` floats between rows).
+// holds channel c of slot i; `stride` floats between rows). Both counts fit
+// an int: every entry takes over 400 bytes of the buffer.
 template <int K>
 __device__ __forceinline__ float* cache_color_rows(const TraceParams& p, bool main_part, long long g, uint32_t e,
                                                    int& stride) {
